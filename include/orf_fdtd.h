@@ -1,0 +1,266 @@
+/*
+ * orf_fdtd.h -- C ABI of the B200 Yee-FDTD engine (liborf_fdtd.so).
+ *
+ * Drop-in for the time loop behind OpticRCWAFDTD's orf.fdtd2D / orf.fdtd2DTE /
+ * orf.fdtd3D.  Every struct is plain data: pointers, sizes, doubles.  A MATLAB
+ * MEX gateway (mex/orf_fdtd_mex.c), Python ctypes, or any C caller binds the
+ * same symbols.
+ *
+ * Conventions (toolbox/+orf/fdtd2D.m:1-7, fdtd3D.m:1-9, docs/CONVENTIONS.md:17):
+ *   - real fields, H~ = eta0*H, time as c0*t in micrometres;
+ *   - arrays are column-major with x fastest (MATLAB ndgrid layout);
+ *   - every index in these structs is 0-based (the MEX gateway and the Python
+ *     mirror subtract 1 from MATLAB's 1-based indices);
+ *   - complex outputs are interleaved (re, im) doubles, MATLAB's
+ *     interleaved-complex layout (R2018a+).
+ *
+ * Ownership: input arrays are borrowed for the duration of the call.  Output
+ * arrays are allocated by the caller; orf_out2d_sizes / orf_out3d_sizes give
+ * their element counts.  Device memory is owned by an orf_ctx.
+ */
+#ifndef ORF_FDTD_H
+#define ORF_FDTD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ORF_ABI_VERSION 1
+
+#if defined(_WIN32)
+#define ORF_API __declspec(dllexport)
+#else
+#define ORF_API __attribute__((visibility("default")))
+#endif
+
+/* Status codes.  The MEX gateway maps them to MATLAB error identifiers
+ * (ORF_ECANCELLED -> 'orf:cancelled', tests/TestGUISupport.m:39-43). */
+typedef enum orf_status {
+    ORF_OK = 0,
+    ORF_EINVAL = 1,            /* malformed sim struct / out-of-range index   */
+    ORF_ENOMEM_DEVICE = 2,     /* not enough free device memory                */
+    ORF_ECANCELLED = 3,        /* progress callback asked to stop              */
+    ORF_ETIMEOUT_DEVICE = 4,   /* a bounded device-side wait ran out           */
+    ORF_ECUDA = 5,             /* CUDA runtime error (message in orf_last_error)*/
+    ORF_ENODEV = 6,            /* no CUDA device / library built without one   */
+    ORF_EBUSY = 7,             /* serving queue full / ticket not finished     */
+    ORF_ETOOLARGE = 8          /* request exceeds a documented size limit      */
+} orf_status;
+
+enum { ORF_TE = 0, ORF_TM = 1 };                 /* sim.pol        */
+enum { ORF_DOUBLE = 0, ORF_SINGLE = 1 };         /* sim.precision  */
+
+/* Progress callback, invoked on the calling thread every 50 simulated steps
+ * (fdtd2D.m:18-20).  frac follows orf.fdtdProgress (fdtdProgress.m:1-13).
+ * Return non-zero to cancel the run: the call then returns ORF_ECANCELLED. */
+typedef int (*orf_progress_fn)(double frac, const char* msg, void* user);
+
+/* ---------------------------------------------------------------- 2D ---- */
+/* Mirrors the sim struct of orf.fdtd2D / orf.fdtd2DTE
+ * (fdtd2D.m:9-23, fdtd2DTE.m:7-25). */
+typedef struct orf_sim2d {
+    int32_t pol;               /* ORF_TE (P=Ey,A=Hx,B=Hz) or ORF_TM (P=Hy,A=-Ex,B=-Ez) */
+    int32_t nx, nz;            /* numel(sim.x), numel(sim.z)                          */
+    double x0, z0, dx;         /* sim.x(1), sim.z(1), uniform spacing                 */
+    const double* eps;         /* TE: nx*nz eps at P                                   */
+    const double* eps_x;       /* TM: nx*(nz-1) (nx*nz if periodic_z) eps at A        */
+    const double* eps_z;       /* TM: (nx-1)*nz eps at B                               */
+    int32_t npml_x, npml_z;    /* sim.npml = [nx nz] CPML cells per end               */
+    int32_t periodic_z;        /* sim.periodicZ                                        */
+    int32_t src_ix;            /* sim.source.ix (0-based P column)                    */
+    const double* src_profile; /* sim.source.profile, nz values                       */
+    double src_neff, src_lambda0, src_bw;
+    int32_t n_mon;             /* sim.monitors: P columns of x = const lines          */
+    const int32_t* monitors;
+    int32_t n_monz;            /* sim.monitorsZ: P rows of z = const lines            */
+    const int32_t* monitors_z;
+    int32_t n_lambda;          /* sim.lambdas [um]                                     */
+    const double* lambdas;
+    double max_time;           /* sim.maxTime (c0*t, um), default 1e4                 */
+    double shutoff;            /* sim.shutoff, default 1e-10                           */
+    double courant;            /* sim.courant, default 0.99/sqrt(2)                   */
+    int32_t precision;         /* ORF_DOUBLE or ORF_SINGLE                             */
+    int32_t flags;             /* reserved, 0                                          */
+} orf_sim2d;
+
+/* Mirrors the out struct (fdtd2D.m:25-29, fdtd2DTE.m:27-32).  Any pointer may
+ * be NULL to skip that output. */
+typedef struct orf_out2d {
+    double* flux;      /* n_mon  x n_lambda, column-major                        */
+    double* flux_z;    /* n_monz x n_lambda                                      */
+    double* P;         /* complex nz x n_lambda x n_mon  (out.P, TE Ey / TM Hy)  */
+    double* B;         /* complex nz x n_lambda x n_mon  (out.B, TE Hz / TM -Ez) */
+    double* PZ;        /* complex nx x n_lambda x n_monz (out.PZ)                */
+    double* AZ;        /* complex nx x n_lambda x n_monz (out.AZ, TE Hx / TM -Ex)*/
+    int32_t converged; /* 0: maxTime reached (fdtd2D:notConverged)               */
+    int32_t _pad;
+    int64_t steps;
+    double time;       /* steps * courant * dx                                   */
+    double wall_time;  /* seconds                                                */
+} orf_out2d;
+
+/* ---------------------------------------------------------------- 3D ---- */
+/* Mirrors the sim struct of orf.fdtd3D (fdtd3D.m:11-24). */
+typedef struct orf_sim3d {
+    int32_t nx, ny, nz;
+    int32_t _pad0;
+    double x0, y0, z0, d;
+    const double* eps_x;       /* sim.eps.x, nx*ny*nz at Ex (x+d/2, y, z)   */
+    const double* eps_y;       /* sim.eps.y at Ey                            */
+    const double* eps_z;       /* sim.eps.z at Ez                            */
+    int32_t npml[3];           /* sim.npml                                   */
+    int32_t periodic[3];       /* sim.periodic                               */
+    int32_t src_axis;          /* sim.source.axis - 1  (0 = x, 1 = y, 2 = z) */
+    int32_t src_index;         /* sim.source.index - 1                       */
+    const double* src_Ea;      /* Na*Nb profiles, a = axis+1, b = axis+2     */
+    const double* src_Eb;
+    const double* src_Ha;
+    const double* src_Hb;
+    double src_neff, src_lambda0, src_bw;
+    int32_t n_mon;
+    int32_t _pad1;
+    const int32_t* mon_axis;   /* sim.monitors(q).axis - 1                   */
+    const int32_t* mon_index;  /* sim.monitors(q).index - 1                  */
+    int32_t n_lambda;
+    int32_t _pad2;
+    const double* lambdas;
+    double max_time, shutoff, courant;   /* courant default 0.99/sqrt(3)     */
+    int32_t precision;
+    int32_t flags;
+} orf_sim3d;
+
+typedef struct orf_out3d {
+    double* flux;              /* n_mon x n_lambda                                  */
+    double* const* mon_Ea;     /* n_mon pointers, each complex Na x Nb x n_lambda   */
+    double* const* mon_Eb;
+    double* const* mon_Ha;     /* H averaged onto the E plane (fdtd3D.m:27-28)      */
+    double* const* mon_Hb;
+    int32_t converged;
+    int32_t _pad;
+    int64_t steps;
+    double time;
+    double wall_time;
+} orf_out3d;
+
+/* ------------------------------------------------------------ context --- */
+typedef struct orf_ctx orf_ctx;
+
+/* Tuning knobs of the 2D/3D step kernels; zero fields mean "autotuned". */
+typedef struct orf_tuning {
+    int32_t tsteps;            /* time steps fused per launch (temporal block depth) */
+    int32_t variant;           /* kernel tile variant id, 0 = autotune               */
+    int32_t use_graph;         /* 1: capture the time loop in CUDA graphs            */
+    int32_t _pad;
+} orf_tuning;
+
+/* Per-kernel timing, collected when orf_ctx_set_timing(ctx, 1). */
+typedef struct orf_kernel_stats {
+    double step_ms;            /* summed CUDA-event time of the step kernels        */
+    int64_t step_launches;
+    int64_t cell_updates;      /* cells x steps advanced by those launches          */
+    double flush_ms;           /* DFT flush + check kernels                         */
+    int64_t flush_launches;
+} orf_kernel_stats;
+
+ORF_API int32_t     orf_abi_version(void);
+ORF_API const char* orf_status_string(int32_t status);
+/* Copies the last error message of this thread (NUL-terminated). */
+ORF_API int32_t     orf_last_error(char* buf, size_t len);
+ORF_API int32_t     orf_device_count(void);
+
+/* Creates a context on `device`.  `stream` is a cudaStream_t or NULL (the
+ * context then creates its own non-blocking stream). */
+ORF_API int32_t orf_ctx_create(int32_t device, void* stream, orf_ctx** out);
+ORF_API int32_t orf_ctx_destroy(orf_ctx* ctx);
+ORF_API int32_t orf_ctx_set_tuning(orf_ctx* ctx, const orf_tuning* t);
+ORF_API int32_t orf_ctx_set_timing(orf_ctx* ctx, int32_t on);
+ORF_API int32_t orf_ctx_get_stats(orf_ctx* ctx, orf_kernel_stats* st);
+ORF_API int32_t orf_ctx_reset_stats(orf_ctx* ctx);
+
+/* ------------------------------------------------------------ 2D runs --- */
+/* Element counts of the caller-allocated out arrays (complex counts are in
+ * complex elements; allocate twice as many doubles). */
+ORF_API int32_t orf_out2d_sizes(const orf_sim2d* sim, int64_t* n_flux, int64_t* n_flux_z,
+                        int64_t* n_P, int64_t* n_PZ);
+
+/* One orf.fdtd2D(sim) call: host arrays in, host arrays out.
+ * Replaces toolbox/+orf/fdtd2D.m:1-29 (and fdtd2DTE.m:33-34 with pol = TE). */
+ORF_API int32_t orf_fdtd2d_run(const orf_sim2d* sim, orf_out2d* out,
+                       orf_progress_fn progress, void* user);
+ORF_API int32_t orf_fdtd2d_run_ctx(orf_ctx* ctx, const orf_sim2d* sim, orf_out2d* out,
+                           orf_progress_fn progress, void* user);
+
+/* Device-resident form of the same run, for benchmarks and callers that keep
+ * fields on the GPU: create (uploads + allocates), advance (enqueues steps,
+ * asynchronous), finish (flux + copy-out, synchronous). */
+typedef struct orf_job orf_job;
+ORF_API int32_t orf_job2d_create(orf_ctx* ctx, const orf_sim2d* sim, orf_job** job);
+ORF_API int32_t orf_job3d_create(orf_ctx* ctx, const orf_sim3d* sim, orf_job** job);
+ORF_API int32_t orf_job_advance(orf_job* job, int64_t nsteps);
+ORF_API int32_t orf_job_sync(orf_job* job);
+ORF_API int32_t orf_job_reset(orf_job* job);       /* fields, DFT sums, step counter -> 0 */
+ORF_API int64_t orf_job_steps_done(orf_job* job);
+ORF_API int64_t orf_job_cells(orf_job* job);
+ORF_API int32_t orf_job2d_finish(orf_job* job, orf_out2d* out);
+ORF_API int32_t orf_job3d_finish(orf_job* job, orf_out3d* out);
+/* Copies the current fields to host: 2D fills P, A, B with nx*nz, nx*nzA,
+ * (nx-1)*nz doubles; 3D fills the six components (nx*ny*nz each, order
+ * Ex Ey Ez Hx Hy Hz).  For parity tests. */
+ORF_API int32_t orf_job_get_fields(orf_job* job, double* const* fields, int32_t nfields);
+ORF_API int32_t orf_job_destroy(orf_job* job);
+
+/* ------------------------------------------------------------ 3D runs --- */
+/* Plane sizes Na, Nb of each monitor (arrays of n_mon). */
+ORF_API int32_t orf_out3d_sizes(const orf_sim3d* sim, int32_t* na, int32_t* nb);
+/* One orf.fdtd3D(sim) call.  Replaces toolbox/+orf/fdtd3D.m:1-29. */
+ORF_API int32_t orf_fdtd3d_run(const orf_sim3d* sim, orf_out3d* out,
+                       orf_progress_fn progress, void* user);
+ORF_API int32_t orf_fdtd3d_run_ctx(orf_ctx* ctx, const orf_sim3d* sim, orf_out3d* out,
+                           orf_progress_fn progress, void* user);
+
+/* ------------------------------------------------------------ batches --- */
+/* Many independent 2D runs advanced together by one persistent kernel per
+ * launch, the time loop captured in CUDA graphs.  All sims of one call must
+ * share pol and precision.  Replaces the sequential orf.fdtd2D calls of the
+ * sweeps (examples/cpo_box_scan.m:23-31, optimizeGratingCoupler.m:1-12). */
+ORF_API int32_t orf_batch2d_run(orf_ctx* ctx, int32_t n, const orf_sim2d* sims,
+                        orf_out2d* outs, orf_progress_fn progress, void* user);
+
+/* ------------------------------------------------------------ serving --- */
+typedef struct orf_server orf_server;
+typedef struct orf_serve_cfg {
+    int64_t max_device_bytes;   /* admission budget; 0 = 90% of free memory   */
+    int32_t max_jobs;           /* slot count; 0 = 1024                        */
+    int32_t macro_steps;        /* steps advanced between admissions; 0 = 200  */
+} orf_serve_cfg;
+typedef struct orf_serve_job_info {
+    double t_submit, t_admit, t_done;   /* seconds on the server's clock       */
+    int64_t steps;
+    int64_t cells;
+    int32_t status;
+    int32_t dims;
+} orf_serve_job_info;
+
+ORF_API int32_t orf_serve_open(orf_ctx* ctx, const orf_serve_cfg* cfg, orf_server** srv);
+/* The sim and its arrays are copied at submit; out arrays must stay valid
+ * until the ticket completes. */
+ORF_API int32_t orf_serve_submit2d(orf_server* srv, const orf_sim2d* sim, orf_out2d* out,
+                           int64_t* ticket);
+ORF_API int32_t orf_serve_submit3d(orf_server* srv, const orf_sim3d* sim, orf_out3d* out,
+                           int64_t* ticket);
+/* Runs one scheduling round: admits queued jobs that fit, advances every
+ * resident job by up to macro_steps, retires finished jobs. */
+ORF_API int32_t orf_serve_step(orf_server* srv);
+/* ORF_OK when the ticket is done (info filled), ORF_EBUSY otherwise. */
+ORF_API int32_t orf_serve_poll(orf_server* srv, int64_t ticket, orf_serve_job_info* info);
+ORF_API int32_t orf_serve_pending(orf_server* srv, int32_t* queued, int32_t* resident);
+ORF_API double  orf_serve_clock(orf_server* srv);
+ORF_API int32_t orf_serve_close(orf_server* srv);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ORF_FDTD_H */

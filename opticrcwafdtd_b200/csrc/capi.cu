@@ -1,0 +1,225 @@
+// capi.cu -- the extern "C" entry points of liborf_fdtd.so (include/orf_fdtd.h).
+#include "engine.cuh"
+
+using namespace orf;
+
+namespace orf {
+
+orf_ctx* default_ctx(int* status) {
+    static thread_local orf_ctx* ctxs[64] = {nullptr};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        set_error("no CUDA device: %s", cudaGetErrorString(e));
+        *status = ORF_ENODEV;
+        return nullptr;
+    }
+    if (dev >= 64) { *status = ORF_ENODEV; return nullptr; }
+    if (!ctxs[dev]) {
+        orf_ctx* c = nullptr;
+        int st = orf_ctx_create(dev, nullptr, &c);
+        if (st != ORF_OK) { *status = st; return nullptr; }
+        ctxs[dev] = c;
+    }
+    *status = ORF_OK;
+    return ctxs[dev];
+}
+
+}  // namespace orf
+
+extern "C" {
+
+int32_t orf_abi_version(void) { return ORF_ABI_VERSION; }
+
+const char* orf_status_string(int32_t s) {
+    switch (s) {
+        case ORF_OK: return "ORF_OK";
+        case ORF_EINVAL: return "ORF_EINVAL";
+        case ORF_ENOMEM_DEVICE: return "ORF_ENOMEM_DEVICE";
+        case ORF_ECANCELLED: return "ORF_ECANCELLED";
+        case ORF_ETIMEOUT_DEVICE: return "ORF_ETIMEOUT_DEVICE";
+        case ORF_ECUDA: return "ORF_ECUDA";
+        case ORF_ENODEV: return "ORF_ENODEV";
+        case ORF_EBUSY: return "ORF_EBUSY";
+        case ORF_ETOOLARGE: return "ORF_ETOOLARGE";
+    }
+    return "ORF_UNKNOWN";
+}
+
+int32_t orf_last_error(char* buf, size_t len) {
+    if (!buf || len == 0) return ORF_EINVAL;
+    std::snprintf(buf, len, "%s", last_error());
+    return ORF_OK;
+}
+
+int32_t orf_device_count(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+int32_t orf_ctx_create(int32_t device, void* stream, orf_ctx** out) {
+    if (!out) return ORF_EINVAL;
+    *out = nullptr;
+    int n = orf_device_count();
+    if (n <= 0) { set_error("no CUDA device available"); return ORF_ENODEV; }
+    if (device < 0 || device >= n) { set_error("device %d outside 0..%d", device, n - 1); return ORF_EINVAL; }
+    ORF_CUDA(cudaSetDevice(device));
+    auto c = new orf_ctx();
+    c->device = device;
+    cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
+    if (stream) {
+        c->stream = static_cast<cudaStream_t>(stream);
+    } else {
+        cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) { delete c; set_error("stream: %s", cudaGetErrorString(e)); return ORF_ECUDA; }
+        c->own_stream = true;
+    }
+    c->tuning.use_graph = 1;
+    *out = c;
+    return ORF_OK;
+}
+
+int32_t orf_ctx_destroy(orf_ctx* c) {
+    if (!c) return ORF_EINVAL;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return ORF_OK;
+}
+
+int32_t orf_ctx_set_tuning(orf_ctx* c, const orf_tuning* t) {
+    if (!c || !t) return ORF_EINVAL;
+    if (t->tsteps < 0 || t->tsteps > kMaxSub) { set_error("tsteps must be 0..%d", kMaxSub); return ORF_EINVAL; }
+    c->tuning = *t;
+    return ORF_OK;
+}
+
+int32_t orf_ctx_set_timing(orf_ctx* c, int32_t on) {
+    if (!c) return ORF_EINVAL;
+    c->timing = on != 0;
+    return ORF_OK;
+}
+
+int32_t orf_ctx_get_stats(orf_ctx* c, orf_kernel_stats* st) {
+    if (!c || !st) return ORF_EINVAL;
+    *st = c->stats;
+    return ORF_OK;
+}
+
+int32_t orf_ctx_reset_stats(orf_ctx* c) {
+    if (!c) return ORF_EINVAL;
+    c->stats = orf_kernel_stats{};
+    return ORF_OK;
+}
+
+int32_t orf_out2d_sizes(const orf_sim2d* s, int64_t* n_flux, int64_t* n_flux_z, int64_t* n_P, int64_t* n_PZ) {
+    if (!s) return ORF_EINVAL;
+    if (n_flux) *n_flux = (int64_t)s->n_mon * s->n_lambda;
+    if (n_flux_z) *n_flux_z = (int64_t)s->n_monz * s->n_lambda;
+    if (n_P) *n_P = (int64_t)s->nz * s->n_lambda * s->n_mon;
+    if (n_PZ) *n_PZ = (int64_t)s->nx * s->n_lambda * s->n_monz;
+    return ORF_OK;
+}
+
+int32_t orf_fdtd2d_run_ctx(orf_ctx* ctx, const orf_sim2d* sim, orf_out2d* out, orf_progress_fn progress,
+                           void* user) {
+    if (!ctx || !sim || !out) { set_error("NULL argument"); return ORF_EINVAL; }
+    const double t0 = now_s();
+    orf_job* job = nullptr;
+    ORF_TRY(make_job2d(ctx, sim, &job));
+    std::unique_ptr<orf_job> guard(job);
+    ORF_TRY(job->advance(job->step_budget(), progress, user));
+    ORF_TRY(job->finish2d(out));
+    out->wall_time = now_s() - t0;
+    return ORF_OK;
+}
+
+int32_t orf_fdtd2d_run(const orf_sim2d* sim, orf_out2d* out, orf_progress_fn progress, void* user) {
+    if (!out) { set_error("out is NULL"); return ORF_EINVAL; }
+    ORF_TRY(validate2d(sim));
+    int st = ORF_OK;
+    orf_ctx* c = default_ctx(&st);
+    if (!c) return st;
+    return orf_fdtd2d_run_ctx(c, sim, out, progress, user);
+}
+
+int32_t orf_job2d_create(orf_ctx* ctx, const orf_sim2d* sim, orf_job** job) {
+    if (!ctx || !job) return ORF_EINVAL;
+    return make_job2d(ctx, sim, job);
+}
+
+int32_t orf_job3d_create(orf_ctx* ctx, const orf_sim3d* sim, orf_job** job) {
+    if (!ctx || !job) return ORF_EINVAL;
+    return make_job3d(ctx, sim, job);
+}
+
+int32_t orf_job_advance(orf_job* job, int64_t nsteps) {
+    if (!job || nsteps < 0) return ORF_EINVAL;
+    return job->advance(nsteps, nullptr, nullptr);
+}
+
+int32_t orf_job_sync(orf_job* job) {
+    if (!job) return ORF_EINVAL;
+    ORF_CUDA(cudaStreamSynchronize(job->ctx->stream));
+    return ORF_OK;
+}
+
+int32_t orf_job_reset(orf_job* job) { return job ? job->reset() : ORF_EINVAL; }
+int64_t orf_job_steps_done(orf_job* job) { return job ? job->steps_done() : -1; }
+int64_t orf_job_cells(orf_job* job) { return job ? job->cells() : -1; }
+int32_t orf_job2d_finish(orf_job* job, orf_out2d* out) { return (job && out) ? job->finish2d(out) : ORF_EINVAL; }
+int32_t orf_job3d_finish(orf_job* job, orf_out3d* out) { return (job && out) ? job->finish3d(out) : ORF_EINVAL; }
+int32_t orf_job_get_fields(orf_job* job, double* const* f, int32_t nf) {
+    return (job && f) ? job->get_fields(f, nf) : ORF_EINVAL;
+}
+int32_t orf_job_destroy(orf_job* job) {
+    delete job;
+    return ORF_OK;
+}
+
+int32_t orf_out3d_sizes(const orf_sim3d* s, int32_t* na, int32_t* nb) {
+    if (!s) return ORF_EINVAL;
+    const int n[3] = {s->nx, s->ny, s->nz};
+    for (int m = 0; m < s->n_mon; ++m) {
+        const int q = s->mon_axis[m];
+        if (q < 0 || q > 2) { set_error("monitors(%d).axis must be 1..3", m + 1); return ORF_EINVAL; }
+        if (na) na[m] = n[(q + 1) % 3];
+        if (nb) nb[m] = n[(q + 2) % 3];
+    }
+    return ORF_OK;
+}
+
+int32_t orf_fdtd3d_run_ctx(orf_ctx* ctx, const orf_sim3d* sim, orf_out3d* out, orf_progress_fn progress,
+                           void* user) {
+    if (!ctx || !sim || !out) { set_error("NULL argument"); return ORF_EINVAL; }
+    const double t0 = now_s();
+    orf_job* job = nullptr;
+    ORF_TRY(make_job3d(ctx, sim, &job));
+    std::unique_ptr<orf_job> guard(job);
+    ORF_TRY(job->advance(job->step_budget(), progress, user));
+    ORF_TRY(job->finish3d(out));
+    out->wall_time = now_s() - t0;
+    return ORF_OK;
+}
+
+int32_t orf_fdtd3d_run(const orf_sim3d* sim, orf_out3d* out, orf_progress_fn progress, void* user) {
+    if (!out) { set_error("out is NULL"); return ORF_EINVAL; }
+    ORF_TRY(validate3d(sim));
+    int st = ORF_OK;
+    orf_ctx* c = default_ctx(&st);
+    if (!c) return st;
+    return orf_fdtd3d_run_ctx(c, sim, out, progress, user);
+}
+
+int32_t orf_batch2d_run(orf_ctx* ctx, int32_t n, const orf_sim2d* sims, orf_out2d* outs, orf_progress_fn progress,
+                        void* user) {
+    if (!ctx || n < 0 || (n > 0 && (!sims || !outs))) { set_error("NULL argument"); return ORF_EINVAL; }
+    return batch2d_run(ctx, n, sims, outs, progress, user);
+}
+
+}  // extern "C"

@@ -1,0 +1,69 @@
+// engine.cuh -- the chunked time loop shared by 2D, 3D and batched runs.
+//
+// One chunk = kChunk time steps = ceil(kChunk / T) step-kernel launches
+// (each fusing up to T steps), one DFT flush launch and one check launch.
+// All per-step state (step counter, done flag, energy) lives in device
+// memory, so a captured chunk sequence replays unchanged: the time loop runs
+// as CUDA graph launches of G chunks, and the host only polls the status ring
+// the check kernel writes into mapped pinned memory (no per-chunk sync).
+#pragma once
+#include <functional>
+
+#include "runtime.cuh"
+
+namespace orf {
+
+struct ChunkEngine {
+    orf_ctx* ctx = nullptr;
+    bool fp64 = false;
+    int T = 1;                        // time steps fused per step launch
+    int par = 0;                      // field buffer holding the current state
+    // launches the step kernels of all instances for steps [off, off+nsub) of
+    // the chunk, reading buffer par; want_energy on the chunk's last launch
+    std::function<cudaError_t(int off, int nsub, int par, int want_energy, cudaStream_t)> step;
+    DftStream* d_streams = nullptr;
+    FlushItem* d_items = nullptr;
+    int nitems = 0;
+    JobState** d_states = nullptr;
+    int nstates = 0;
+
+    // graph cache
+    cudaGraphExec_t gexec = nullptr;
+    int gchunks = 0;
+    int gpar = -1;
+
+    // timing (orf_ctx_set_timing): events around the step launches of a chunk
+    std::vector<cudaEvent_t> evpool;
+    size_t evused = 0;
+
+    ~ChunkEngine();
+    int launches_per_chunk() const { return (kChunk + T - 1) / T; }
+    int enqueue_chunk(cudaStream_t s, bool timed);
+    // enqueue n chunks (graph replays where possible)
+    int enqueue(int nchunks, cudaStream_t s);
+    void drop_graph();
+    // fold the recorded events into ctx->stats (after a sync)
+    void collect_timing(int64_t cell_updates);
+};
+
+// Host-side progress loop over one job's status ring.
+struct ProgressLoop {
+    const ChunkStatus* ring = nullptr;   // mapped host ring of the job
+    volatile int* cancel = nullptr;      // mapped host cancel flag read by the check kernel
+    long long seen = 0;                  // ring entries consumed
+    double S = 0, src_end = 0, shutoff = 0;
+    bool done = false;
+    bool cancelled = false;
+    long long last_step = 0;
+    // consume finished entries; returns ORF_ECANCELLED if the callback asks
+    int poll(orf_progress_fn progress, void* user);
+};
+
+// Enqueue `chunks` chunks of one engine in batches, at most kInFlight
+// batches ahead of the GPU, reading the status ring after each batch: the
+// progress callback fires every chunk and enqueueing stops as soon as the
+// device reports the run done (shutoff) or the callback cancels.
+int run_chunks(ChunkEngine& eng, ProgressLoop& pl, orf_ctx* ctx, int64_t chunks, orf_progress_fn progress,
+               void* user);
+
+}  // namespace orf

@@ -1,0 +1,554 @@
+// job2d.cu -- one orf.fdtd2D run on the device (toolbox/+orf/fdtd2D.m:1-29).
+//
+// Host work at creation: validate the sim struct, turn the eps arrays into a
+// material index plus a table of update coefficients (exact: the table holds
+// every distinct eps value), build the CPML profiles, the TF/SF source
+// tables and the tile lists, and upload everything into one device arena.
+// The time loop is the shared ChunkEngine; outputs are the monitor DFT lines
+// and the fluxes of fdtd2D.m:25-29.
+#include <algorithm>
+#include <unordered_map>
+
+#include "engine.cuh"
+#include "job2d.cuh"
+
+namespace orf {
+
+int validate2d(const orf_sim2d* s) {
+    if (!s) { set_error("sim is NULL"); return ORF_EINVAL; }
+    if (s->pol != ORF_TE && s->pol != ORF_TM) { set_error("sim.pol must be TE or TM"); return ORF_EINVAL; }
+    if (s->nx < 3 || s->nz < 2) { set_error("grid must be at least 3 x 2 cells"); return ORF_EINVAL; }
+    if ((int64_t)s->nx * s->nz > (int64_t)1 << 31) { set_error("grid exceeds 2^31 cells"); return ORF_ETOOLARGE; }
+    if (!(s->dx > 0) || !std::isfinite(s->dx)) { set_error("grid spacing must be positive"); return ORF_EINVAL; }
+    if (!(s->courant > 0) || s->courant > 1.0 / std::sqrt(2.0) + 1e-12) {
+        set_error("courant %.6g outside (0, 1/sqrt(2)] (2D Yee stability limit)", s->courant);
+        return ORF_EINVAL;
+    }
+    const bool per = s->periodic_z != 0;
+    const int nz = s->nz, nx = s->nx, nzA = per ? nz : nz - 1;
+    if (s->pol == ORF_TE && !s->eps) { set_error("sim.eps is required for TE"); return ORF_EINVAL; }
+    if (s->pol == ORF_TM && (!s->eps_x || !s->eps_z)) { set_error("sim.epsX and sim.epsZ are required for TM"); return ORF_EINVAL; }
+    auto chk = [&](const double* e, size_t n, const char* nm) {
+        for (size_t q = 0; q < n; ++q)
+            if (!(e[q] > 0) || !std::isfinite(e[q])) {
+                set_error("%s(%zu) = %g: permittivity must be positive and finite", nm, q + 1, e[q]);
+                return false;
+            }
+        return true;
+    };
+    if (s->pol == ORF_TE && !chk(s->eps, (size_t)nx * nz, "sim.eps")) return ORF_EINVAL;
+    if (s->pol == ORF_TM && (!chk(s->eps_x, (size_t)nx * nzA, "sim.epsX") || !chk(s->eps_z, (size_t)(nx - 1) * nz, "sim.epsZ")))
+        return ORF_EINVAL;
+    const int npz = per ? 0 : s->npml_z;
+    if (s->npml_x < 0 || 2 * s->npml_x >= nx - 1) { set_error("npml(1) = %d does not fit numel(x) = %d", s->npml_x, nx); return ORF_EINVAL; }
+    if (npz < 0 || 2 * npz >= nz - 1) { set_error("npml(2) = %d does not fit numel(z) = %d", npz, nz); return ORF_EINVAL; }
+    if (s->src_ix < 0 || s->src_ix >= nx) { set_error("source.ix = %d outside 1..%d", s->src_ix + 1, nx); return ORF_EINVAL; }
+    if (s->src_ix < s->npml_x || s->src_ix >= nx - s->npml_x) { set_error("source.ix = %d lies inside the CPML", s->src_ix + 1); return ORF_EINVAL; }
+    if (!s->src_profile) { set_error("source.profile is required"); return ORF_EINVAL; }
+    if (!(s->src_lambda0 > 0) || !(s->src_bw > 0)) { set_error("source.lambda0 and source.bw must be positive"); return ORF_EINVAL; }
+    if (!std::isfinite(s->src_neff)) { set_error("source.neff must be finite"); return ORF_EINVAL; }
+    if (s->n_mon < 0 || s->n_mon > kMaxMon || s->n_monz < 0 || s->n_monz > kMaxMon) {
+        set_error("at most %d monitors per orientation", kMaxMon);
+        return ORF_EINVAL;
+    }
+    for (int m = 0; m < s->n_mon; ++m)
+        if (s->monitors[m] < 0 || s->monitors[m] >= nx) { set_error("monitors(%d) = %d outside 1..%d", m + 1, s->monitors[m] + 1, nx); return ORF_EINVAL; }
+    for (int m = 0; m < s->n_monz; ++m)
+        if (s->monitors_z[m] < 0 || s->monitors_z[m] >= nz) { set_error("monitorsZ(%d) = %d outside 1..%d", m + 1, s->monitors_z[m] + 1, nz); return ORF_EINVAL; }
+    if (s->n_lambda < 1 || !s->lambdas) { set_error("sim.lambdas must not be empty"); return ORF_EINVAL; }
+    for (int l = 0; l < s->n_lambda; ++l)
+        if (!(s->lambdas[l] > 0)) { set_error("lambdas(%d) must be positive", l + 1); return ORF_EINVAL; }
+    if (!(s->max_time >= 0) || !(s->shutoff >= 0)) { set_error("maxTime and shutoff must be non-negative"); return ORF_EINVAL; }
+    if (s->precision != ORF_DOUBLE && s->precision != ORF_SINGLE) { set_error("precision must be double or single"); return ORF_EINVAL; }
+    return ORF_OK;
+}
+
+// Distinct values -> dense index (insertion order), exact.
+struct Lut {
+    std::unordered_map<uint64_t, int> map;
+    std::vector<double> vals;
+    int get(double v) {
+        uint64_t key;
+        std::memcpy(&key, &v, 8);
+        auto it = map.find(key);
+        if (it != map.end()) return it->second;
+        const int id = (int)vals.size();
+        map.emplace(key, id);
+        vals.push_back(v);
+        return id;
+    }
+};
+
+template <class R>
+int Job2D<R>::create(const orf_sim2d* s) {
+    ORF_TRY(validate2d(s));
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev != ctx->device) ORF_CUDA(cudaSetDevice(ctx->device));
+    te = s->pol == ORF_TE;
+    per = s->periodic_z != 0;
+    nx = s->nx;
+    nz = s->nz;
+    nzA = per ? nz : nz - 1;
+    nxB = nx - 1;
+    pitch = (nx + 31) & ~31;
+    dx = s->dx;
+    Cc = s->courant;
+    S = Cc * dx;
+    nM = s->n_mon;
+    nMZ = s->n_monz;
+    nL = s->n_lambda;
+    const int npx = s->npml_x, npz = per ? 0 : s->npml_z;
+    const size_t cellsP = (size_t)pitch * nz;
+
+    // ---- material index + coefficient table
+    Lut lut;
+    std::vector<uint16_t> ix0(cellsP, 0), ix1(te ? 0 : cellsP, 0);
+    lut.get(te ? s->eps[0] : s->eps_x[0]);
+    for (int k = 0; k < nz; ++k) {
+        for (int i = 0; i < nx; ++i) {
+            if (te) {
+                ix0[(size_t)k * pitch + i] = 0;
+                const int v = lut.get(s->eps[i + (size_t)nx * k]);
+                if (v > 65535) { set_error("more than 65536 distinct permittivity values"); return ORF_ETOOLARGE; }
+                ix0[(size_t)k * pitch + i] = (uint16_t)v;
+            } else {
+                if (k < nzA) {
+                    const int v = lut.get(s->eps_x[i + (size_t)nx * k]);
+                    if (v > 65535) { set_error("more than 65536 distinct permittivity values"); return ORF_ETOOLARGE; }
+                    ix0[(size_t)k * pitch + i] = (uint16_t)v;
+                }
+                if (i < nxB) {
+                    const int v = lut.get(s->eps_z[i + (size_t)nxB * k]);
+                    if (v > 65535) { set_error("more than 65536 distinct permittivity values"); return ORF_ETOOLARGE; }
+                    ix1[(size_t)k * pitch + i] = (uint16_t)v;
+                }
+            }
+        }
+    }
+    nlut = (int)lut.vals.size();
+    idx16 = nlut > 256;
+    std::vector<R> hlutc(nlut);
+    for (int v = 0; v < nlut; ++v) hlutc[v] = R(Cc / lut.vals[v]);
+
+    // ---- CPML profiles
+    const double alpha_max = kPmlAlphaMaxPerK0 * 2.0 * kPi / s->src_lambda0;
+    std::vector<double> px, pxh, pz, pzh;
+    int ns;
+    pml_profile(nx, nx, npx, 0.0, dx, S, alpha_max, px, &ns);
+    pml_profile(nx, nxB, npx, 0.5, dx, S, alpha_max, pxh, &ns);
+    pml_profile(nz, nz, npz, 0.0, dx, S, alpha_max, pz, &ns);
+    pml_profile(nz, nzA, npz, 0.5, dx, S, alpha_max, pzh, &ns);
+    auto toR = [](const std::vector<double>& v) { return std::vector<R>(v.begin(), v.end()); };
+
+    // ---- source
+    const int sx = s->src_ix;
+    const Pulse g(s->src_lambda0, s->src_bw);
+    src_end = g.tend;
+    std::vector<R> hsrcB(nz), hsrcP(nz);
+    for (int k = 0; k < nz; ++k) {
+        const double f = s->src_profile[k];
+        const double epsB = te ? 1.0 : (sx >= 1 ? s->eps_z[(sx - 1) + (size_t)nxB * k] : 1.0);
+        const double cB = te ? Cc : (sx >= 1 ? Cc / s->eps_z[(sx - 1) + (size_t)nxB * k] : 0.0);
+        const double cP = te ? Cc / s->eps[sx + (size_t)nx * k] : Cc;
+        hsrcB[k] = R(cB * f);
+        hsrcP[k] = R(cP * (s->src_neff * f / epsB));
+    }
+    nsrc = (int64_t)std::ceil(g.tend / S) + 2;
+    std::vector<double> hgE(nsrc), hgH(nsrc);
+    for (int64_t n = 0; n < nsrc; ++n) {
+        hgE[n] = g(n * S);
+        hgH[n] = g((n + 0.5) * S + s->src_neff * 0.5 * dx);
+    }
+    nmax = max_steps(s->max_time, S);
+    shutoff = s->shutoff;
+
+    // ---- tiles
+    ORF_TRY(pick_tiling(npx, npz));
+
+    // ---- DFT streams: x monitors (P, B lines), z monitors (P, A lines)
+    const int sstride = 2 * nz * nM + 2 * nx * nMZ;
+    struct SDesc { int soff, len, half; };
+    std::vector<SDesc> sd;
+    for (int m = 0; m < nM; ++m) {
+        sd.push_back({m * 2 * nz, nz, 0});
+        sd.push_back({m * 2 * nz + nz, nz, 1});
+    }
+    for (int m = 0; m < nMZ; ++m) {
+        sd.push_back({nM * 2 * nz + m * 2 * nx, nx, 0});
+        sd.push_back({nM * 2 * nz + m * 2 * nx + nx, nx, 1});
+    }
+    nstreams = (int)sd.size();
+    std::vector<FlushItem> items;
+    for (int q = 0; q < nstreams; ++q)
+        for (int e0 = 0; e0 < sd[q].len; e0 += 128)
+            for (int l0 = 0; l0 < nL; l0 += 8) items.push_back({q, e0, l0, 0});
+    nitems = (int)items.size();
+    std::vector<FluxPair> pairs;
+    for (int m = 0; m < nM; ++m) pairs.push_back({2 * m, 2 * m + 1, -1, -1, m, nM, 0.5 * dx});
+    for (int m = 0; m < nMZ; ++m)
+        pairs.push_back({2 * nM + 2 * m, 2 * nM + 2 * m + 1, -1, -1, nM * nL + m, nMZ, -0.5 * dx});
+    npairs = (int)pairs.size();
+
+    // ---- device arena
+    Arena ar;
+    for (int b = 0; b < 2; ++b) {
+        ar.add(&h.P[b], cellsP);
+        ar.add(&h.A[b], cellsP);
+        ar.add(&h.B[b], cellsP);
+        ar.add(&h.psiB[b], (size_t)nz * 2 * npx + 1);
+        ar.add(&h.psiPx[b], (size_t)nz * 2 * npx + 1);
+        ar.add(&h.psiA[b], (size_t)2 * npz * nx + 1);
+        ar.add(&h.psiPz[b], (size_t)2 * npz * nx + 1);
+    }
+    const size_t isz = idx16 ? 2 : 1;
+    unsigned char *d_ix0 = nullptr, *d_ix1 = nullptr;
+    ar.add(&d_ix0, cellsP * isz);
+    if (!te) ar.add(&d_ix1, cellsP * isz);
+    R *d_lutc, *d_px, *d_pxh, *d_pz, *d_pzh, *d_srcB, *d_srcP, *d_samples;
+    double *d_lute, *d_gE, *d_gH;
+    ar.add(&d_lutc, nlut);
+    ar.add(&d_lute, nlut);
+    ar.add(&d_px, px.size());
+    ar.add(&d_pxh, pxh.size() + 3);
+    ar.add(&d_pz, pz.size());
+    ar.add(&d_pzh, pzh.size() + 3);
+    ar.add(&d_srcB, nz);
+    ar.add(&d_srcP, nz);
+    ar.add(&d_gE, nsrc);
+    ar.add(&d_gH, nsrc);
+    ar.add(&d_samples, (size_t)kChunk * sstride + 1);
+    size_t acc_elems = 0;
+    for (auto& q : sd) acc_elems += (size_t)q.len * nL;
+    ar.add(&d_acc, acc_elems * 16 + 16);
+    ar.add(&d_omega, nL);
+    ar.add(&d_flux, (size_t)(nM + nMZ) * nL + 1);
+    ar.add(&d_stage, (size_t)std::max(nx, nz) * nL);
+    ar.add(&d_inst, 1);
+    ar.add(&d_st, 1);
+    ar.add(&d_states, 1);
+    ar.add(&d_tint, tiles_int.size() + 1);
+    ar.add(&d_tpml, tiles_pml.size() + 1);
+    ar.add(&d_streams, nstreams + 1);
+    ar.add(&d_items, nitems + 1);
+    ar.add(&d_pairs, npairs + 1);
+    ORF_TRY(ar.alloc());
+    arena = ar;
+    cudaStream_t st = ctx->stream;
+    ORF_CUDA(cudaMemsetAsync(arena.base, 0, arena.total, st));
+
+    // mapped host status ring and cancel flag
+    ORF_CUDA(cudaHostAlloc((void**)&ring_h, sizeof(ChunkStatus) * kStatusRing, cudaHostAllocMapped));
+    std::memset(ring_h, 0, sizeof(ChunkStatus) * kStatusRing);
+    ORF_CUDA(cudaHostGetDevicePointer((void**)&ring_d, ring_h, 0));
+    ORF_CUDA(cudaHostAlloc((void**)&cancel_h, sizeof(int), cudaHostAllocMapped));
+    *cancel_h = 0;
+    ORF_CUDA(cudaHostGetDevicePointer((void**)&cancel_d, (void*)cancel_h, 0));
+
+    // ---- upload
+    std::vector<unsigned char> ib0(cellsP * isz), ib1(te ? 0 : cellsP * isz);
+    for (size_t q = 0; q < cellsP; ++q) {
+        if (idx16) {
+            std::memcpy(&ib0[2 * q], &ix0[q], 2);
+            if (!te) std::memcpy(&ib1[2 * q], &ix1[q], 2);
+        } else {
+            ib0[q] = (unsigned char)ix0[q];
+            if (!te) ib1[q] = (unsigned char)ix1[q];
+        }
+    }
+    auto up = [&](void* d, const void* hsrc, size_t bytes) -> int {
+        if (bytes == 0) return ORF_OK;
+        ORF_CUDA(cudaMemcpyAsync(d, hsrc, bytes, cudaMemcpyHostToDevice, st));
+        return ORF_OK;
+    };
+    ORF_TRY(up(d_ix0, ib0.data(), ib0.size()));
+    if (!te) ORF_TRY(up(d_ix1, ib1.data(), ib1.size()));
+    ORF_TRY(up(d_lutc, hlutc.data(), hlutc.size() * sizeof(R)));
+    ORF_TRY(up(d_lute, lut.vals.data(), lut.vals.size() * sizeof(double)));
+    auto pxR = toR(px), pxhR = toR(pxh), pzR = toR(pz), pzhR = toR(pzh);
+    ORF_TRY(up(d_px, pxR.data(), pxR.size() * sizeof(R)));
+    ORF_TRY(up(d_pxh, pxhR.data(), pxhR.size() * sizeof(R)));
+    ORF_TRY(up(d_pz, pzR.data(), pzR.size() * sizeof(R)));
+    ORF_TRY(up(d_pzh, pzhR.data(), pzhR.size() * sizeof(R)));
+    ORF_TRY(up(d_srcB, hsrcB.data(), nz * sizeof(R)));
+    ORF_TRY(up(d_srcP, hsrcP.data(), nz * sizeof(R)));
+    ORF_TRY(up(d_gE, hgE.data(), nsrc * sizeof(double)));
+    ORF_TRY(up(d_gH, hgH.data(), nsrc * sizeof(double)));
+    std::vector<double> om(nL);
+    for (int l = 0; l < nL; ++l) om[l] = 2.0 * kPi / s->lambdas[l];
+    ORF_TRY(up(d_omega, om.data(), nL * sizeof(double)));
+
+    h.nx = nx; h.nz = nz; h.pitch = pitch; h.nzA = nzA; h.nxB = nxB;
+    h.periodic = per ? 1 : 0; h.te = te ? 1 : 0; h.npx = npx; h.npz = npz; h.idx16 = idx16 ? 1 : 0;
+    h.C = R(Cc);
+    h.idx0 = d_ix0; h.idx1 = d_ix1; h.lutc = d_lutc; h.lute = d_lute;
+    h.pmlx = d_px; h.pmlxh = d_pxh; h.pmlz = d_pz; h.pmlzh = d_pzh;
+    h.src_ix = sx; h.nmon = nM; h.nmonz = nMZ; h.sstride = sstride;
+    h.srcB = d_srcB; h.srcP = d_srcP; h.gE = d_gE; h.gH = d_gH; h.nsrc = nsrc;
+    for (int m = 0; m < kMaxMon; ++m) {
+        h.mon[m] = m < nM ? s->monitors[m] : -1;
+        h.monz[m] = m < nMZ ? s->monitors_z[m] : -1;
+    }
+    h.samples = d_samples;
+    h.st = d_st;
+    ORF_TRY(up(d_inst, &h, sizeof(h)));
+    ORF_TRY(up(d_tint, tiles_int.data(), tiles_int.size() * sizeof(Tile2D)));
+    ORF_TRY(up(d_tpml, tiles_pml.data(), tiles_pml.size() * sizeof(Tile2D)));
+    std::vector<DftStream> hs(nstreams);
+    size_t aoff = 0;
+    for (int q = 0; q < nstreams; ++q) {
+        hs[q].st = d_st;
+        hs[q].samples = d_samples;
+        hs[q].sstride = sstride;
+        hs[q].soff = sd[q].soff;
+        hs[q].len = sd[q].len;
+        hs[q].half = sd[q].half;
+        hs[q].nl = nL;
+        hs[q].omega = d_omega;
+        hs[q].acc = static_cast<char*>(d_acc) + aoff * 16;
+        aoff += (size_t)sd[q].len * nL;
+    }
+    host_streams = hs;
+    ORF_TRY(up(d_streams, hs.data(), hs.size() * sizeof(DftStream)));
+    ORF_TRY(up(d_items, items.data(), items.size() * sizeof(FlushItem)));
+    ORF_TRY(up(d_pairs, pairs.data(), pairs.size() * sizeof(FluxPair)));
+    JobState* sp = d_st;
+    ORF_TRY(up(d_states, &sp, sizeof(sp)));
+    ORF_TRY(init_state());
+
+    eng.ctx = ctx;
+    eng.fp64 = sizeof(R) == 8;
+    eng.T = T;
+    eng.par = 0;
+    eng.d_streams = d_streams;
+    eng.d_items = d_items;
+    eng.nitems = nitems;
+    eng.d_states = d_states;
+    eng.nstates = 1;
+    eng.step = [this](int off, int nsub, int par, int we, cudaStream_t stream) -> cudaError_t {
+        const bool f64 = sizeof(R) == 8;
+        cudaError_t e = cudaSuccess;
+        if (!tiles_int.empty())
+            e = launch_step2d(f64, te, idx16, false, variant, d_inst, d_tint, (int)tiles_int.size(), T, off,
+                              nsub, par, we, grid_int, stream);
+        if (e != cudaSuccess) return e;
+        if (!tiles_pml.empty())
+            e = launch_step2d(f64, te, idx16, true, variant, d_inst, d_tpml, (int)tiles_pml.size(), T, off,
+                              nsub, par, we, grid_pml, stream);
+        return e;
+    };
+    ORF_CUDA(cudaStreamSynchronize(st));
+    return ORF_OK;
+}
+
+template <class R>
+int Job2D<R>::pick_tiling(int npx, int npz) {
+    const bool f64 = sizeof(R) == 8;
+    variant = ctx->tuning.variant > 0 ? ctx->tuning.variant : 1;
+    Variant2D v;
+    if (!variant2d_info(variant, f64, &v)) {
+        set_error("unknown 2D kernel variant %d", variant);
+        return ORF_EINVAL;
+    }
+    const int tmax = std::min(kMaxSub, (std::min(v.lx(), v.lz()) - 1) / 2);
+    T = ctx->tuning.tsteps > 0 ? ctx->tuning.tsteps : (f64 ? 4 : 6);
+    if (T > tmax) T = tmax;
+    if (T < 1) T = 1;
+    const int OX = v.lx() - 2 * T, OZ = v.lz() - 2 * T;
+    tiles_int.clear();
+    tiles_pml.clear();
+    for (int ok0 = 0; ok0 < nz; ok0 += OZ) {
+        for (int oi0 = 0; oi0 < nx; oi0 += OX) {
+            Tile2D t;
+            t.inst = 0;
+            t.oi0 = oi0;
+            t.ok0 = ok0;
+            t.ow = (short)std::min(OX, nx - oi0);
+            t.oh = (short)std::min(OZ, nz - ok0);
+            // loaded region [oi0-T, oi0-T+LX) x [ok0-T, ok0-T+LZ); does it reach a CPML cell?
+            const int li0 = oi0 - T, li1 = oi0 - T + v.lx();
+            const int lk0 = ok0 - T, lk1 = ok0 - T + v.lz();
+            bool pml = false;
+            if (npx > 0 && (li0 < npx || li1 > nx - 1 - npx)) pml = true;
+            if (npz > 0 && (lk0 < npz || lk1 > nz - 1 - npz)) pml = true;
+            (pml ? tiles_pml : tiles_int).push_back(t);
+        }
+    }
+    const int bps_i = step2d_blocks_per_sm(f64, te, idx16, false, variant);
+    const int bps_p = step2d_blocks_per_sm(f64, te, idx16, true, variant);
+    if (bps_i < 1 || bps_p < 1) {
+        set_error("2D kernel variant %d cannot be resident on this device (%s)", variant,
+                  cudaGetErrorString(cudaGetLastError()));
+        return ORF_ECUDA;
+    }
+    grid_int = (int)std::min<size_t>(tiles_int.size(), (size_t)ctx->sm_count * bps_i);
+    grid_pml = (int)std::min<size_t>(tiles_pml.size(), (size_t)ctx->sm_count * bps_p);
+    return ORF_OK;
+}
+
+template <class R>
+int Job2D<R>::init_state() {
+    JobState js{};
+    js.step = 0;
+    js.nmax = nmax;
+    js.chunk = 0;
+    js.done = nmax <= 0 ? 1 : 0;
+    js.converged = 0;
+    js.cur = 0;
+    js.energy = 0;
+    js.peak = 0;
+    js.S = S;
+    js.src_end = src_end;
+    js.shutoff = shutoff;
+    js.ring = ring_d;
+    js.cancel = cancel_d;
+    std::memset(ring_h, 0, sizeof(ChunkStatus) * kStatusRing);
+    *cancel_h = 0;
+    enq_steps = 0;
+    ORF_CUDA(cudaMemcpyAsync(d_st, &js, sizeof js, cudaMemcpyHostToDevice, ctx->stream));
+    pl = ProgressLoop{};
+    pl.ring = ring_h;
+    pl.cancel = cancel_h;
+    pl.S = S;
+    pl.src_end = src_end;
+    pl.shutoff = shutoff;
+    eng.par = 0;
+    return ORF_OK;
+}
+
+template <class R>
+Job2D<R>::~Job2D() {
+    if (arena.base) {
+        cudaStreamSynchronize(ctx->stream);
+        arena.release();
+    }
+    if (ring_h) cudaFreeHost(ring_h);
+    if (cancel_h) cudaFreeHost((void*)cancel_h);
+}
+
+template <class R>
+int Job2D<R>::reset() {
+    cudaStream_t st = ctx->stream;
+    ORF_CUDA(cudaStreamSynchronize(st));
+    for (int b = 0; b < 2; ++b) {
+        ORF_CUDA(cudaMemsetAsync(h.P[b], 0, sizeof(R) * pitch * nz, st));
+        ORF_CUDA(cudaMemsetAsync(h.A[b], 0, sizeof(R) * pitch * nz, st));
+        ORF_CUDA(cudaMemsetAsync(h.B[b], 0, sizeof(R) * pitch * nz, st));
+        ORF_CUDA(cudaMemsetAsync(h.psiB[b], 0, sizeof(R) * ((size_t)nz * 2 * h.npx + 1), st));
+        ORF_CUDA(cudaMemsetAsync(h.psiPx[b], 0, sizeof(R) * ((size_t)nz * 2 * h.npx + 1), st));
+        ORF_CUDA(cudaMemsetAsync(h.psiA[b], 0, sizeof(R) * ((size_t)2 * h.npz * nx + 1), st));
+        ORF_CUDA(cudaMemsetAsync(h.psiPz[b], 0, sizeof(R) * ((size_t)2 * h.npz * nx + 1), st));
+    }
+    size_t acc_elems = 0;
+    for (auto& q : host_streams) acc_elems += (size_t)q.len * nL;
+    ORF_CUDA(cudaMemsetAsync(d_acc, 0, acc_elems * 16, st));
+    ORF_TRY(init_state());
+    ORF_CUDA(cudaStreamSynchronize(st));
+    return ORF_OK;
+}
+
+template <class R>
+int Job2D<R>::advance(int64_t nsteps, orf_progress_fn progress, void* user) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev != ctx->device) ORF_CUDA(cudaSetDevice(ctx->device));
+    const int64_t left = std::max<int64_t>(0, nmax - enq_steps);
+    const int64_t chunks = (std::min(nsteps, left) + kChunk - 1) / kChunk;
+    enq_steps += chunks * kChunk;
+    const int64_t steps0 = pl.last_step;
+    ORF_TRY(run_chunks(eng, pl, ctx, chunks, progress, user));
+    if (ctx->timing) eng.collect_timing((pl.last_step - steps0) * (int64_t)nx * nz);
+    return pl.cancelled ? ORF_ECANCELLED : ORF_OK;
+}
+
+template <class R>
+int64_t Job2D<R>::steps_done() {
+    JobState js;
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return -1;
+    if (cudaMemcpy(&js, d_st, sizeof js, cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+    return js.step;
+}
+
+template <class R>
+int Job2D<R>::finish2d(orf_out2d* o) {
+    cudaStream_t st = ctx->stream;
+    ORF_CUDA(cudaStreamSynchronize(st));
+    JobState js;
+    ORF_CUDA(cudaMemcpy(&js, d_st, sizeof js, cudaMemcpyDeviceToHost));
+    const bool f64 = sizeof(R) == 8;
+    ORF_CUDA(launch_flux(f64, d_streams, d_pairs, npairs, nL, d_flux, st));
+    std::vector<double> fl((size_t)(nM + nMZ) * nL);
+    if (!fl.empty()) ORF_CUDA(cudaMemcpyAsync(fl.data(), d_flux, fl.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    // DFT lines: stream q -> complex [l][e]
+    auto fetch = [&](int q, double* dst) -> int {
+        if (!dst) return ORF_OK;
+        const DftStream& S = host_streams[q];
+        const size_t n = (size_t)S.len * nL;
+        if (f64) {
+            ORF_CUDA(cudaMemcpyAsync(dst, S.acc, n * sizeof(double2), cudaMemcpyDeviceToHost, st));
+        } else {
+            ORF_CUDA(launch_acc_to_complex(false, S.acc, n, d_stage, st));
+            ORF_CUDA(cudaMemcpyAsync(dst, d_stage, n * sizeof(double2), cudaMemcpyDeviceToHost, st));
+            ORF_CUDA(cudaStreamSynchronize(st));   // staging buffer is reused
+        }
+        return ORF_OK;
+    };
+    for (int m = 0; m < nM; ++m) {
+        ORF_TRY(fetch(2 * m, o->P ? o->P + (size_t)2 * nz * nL * m : nullptr));
+        ORF_TRY(fetch(2 * m + 1, o->B ? o->B + (size_t)2 * nz * nL * m : nullptr));
+    }
+    for (int m = 0; m < nMZ; ++m) {
+        ORF_TRY(fetch(2 * nM + 2 * m, o->PZ ? o->PZ + (size_t)2 * nx * nL * m : nullptr));
+        ORF_TRY(fetch(2 * nM + 2 * m + 1, o->AZ ? o->AZ + (size_t)2 * nx * nL * m : nullptr));
+    }
+    ORF_CUDA(cudaStreamSynchronize(st));
+    if (o->flux)
+        for (size_t q = 0; q < (size_t)nM * nL; ++q) o->flux[q] = fl[q];
+    if (o->flux_z)
+        for (size_t q = 0; q < (size_t)nMZ * nL; ++q) o->flux_z[q] = fl[(size_t)nM * nL + q];
+    o->converged = js.converged;
+    o->steps = js.step;
+    o->time = js.step * S;
+    return ORF_OK;
+}
+
+template <class R>
+int Job2D<R>::get_fields(double* const* f, int nf) {
+    if (nf < 3) { set_error("2D fields are P, A, B"); return ORF_EINVAL; }
+    ORF_CUDA(cudaStreamSynchronize(ctx->stream));
+    JobState js;
+    ORF_CUDA(cudaMemcpy(&js, d_st, sizeof js, cudaMemcpyDeviceToHost));
+    const int b = js.cur;
+    std::vector<R> tmp((size_t)pitch * nz);
+    R* src[3] = {h.P[b], h.A[b], h.B[b]};
+    const int w[3] = {nx, nx, nxB}, hh[3] = {nz, nzA, nz};
+    for (int q = 0; q < 3; ++q) {
+        if (!f[q]) continue;
+        ORF_CUDA(cudaMemcpy(tmp.data(), src[q], tmp.size() * sizeof(R), cudaMemcpyDeviceToHost));
+        for (int k = 0; k < hh[q]; ++k)
+            for (int i = 0; i < w[q]; ++i) f[q][i + (size_t)w[q] * k] = (double)tmp[(size_t)k * pitch + i];
+    }
+    return ORF_OK;
+}
+
+template struct Job2D<float>;
+template struct Job2D<double>;
+
+int make_job2d(orf_ctx* ctx, const orf_sim2d* sim, orf_job** out) {
+    *out = nullptr;
+    ORF_TRY(validate2d(sim));
+    if (sim->precision == ORF_SINGLE) {
+        auto j = std::make_unique<Job2D<float>>();
+        j->ctx = ctx;
+        ORF_TRY(j->create(sim));
+        *out = j.release();
+    } else {
+        auto j = std::make_unique<Job2D<double>>();
+        j->ctx = ctx;
+        ORF_TRY(j->create(sim));
+        *out = j.release();
+    }
+    return ORF_OK;
+}
+
+}  // namespace orf

@@ -1,0 +1,57 @@
+// job2d.cuh -- device-resident 2D run (orf.fdtd2D).
+#pragma once
+#include "engine.cuh"
+
+namespace orf {
+
+template <class R>
+struct Job2D : orf_job {
+    // geometry / options
+    bool te = true, per = false, idx16 = false;
+    int nx = 0, nz = 0, nzA = 0, nxB = 0, pitch = 0;
+    int nM = 0, nMZ = 0, nL = 0, nlut = 0;
+    double dx = 0, Cc = 0, S = 0, src_end = 0, shutoff = 0;
+    int64_t nmax = 0, nsrc = 0;
+    int64_t enq_steps = 0;     // steps enqueued since the last reset
+    // device
+    Arena arena;
+    Inst2D<R> h{};
+    Inst2D<R>* d_inst = nullptr;
+    JobState* d_st = nullptr;
+    JobState** d_states = nullptr;
+    Tile2D* d_tint = nullptr;
+    Tile2D* d_tpml = nullptr;
+    std::vector<Tile2D> tiles_int, tiles_pml;
+    int variant = 1, T = 1, grid_int = 0, grid_pml = 0;
+    DftStream* d_streams = nullptr;
+    std::vector<DftStream> host_streams;
+    FlushItem* d_items = nullptr;
+    FluxPair* d_pairs = nullptr;
+    int nstreams = 0, nitems = 0, npairs = 0;
+    void* d_acc = nullptr;
+    double* d_omega = nullptr;
+    double* d_flux = nullptr;
+    double2* d_stage = nullptr;
+    // mapped host memory
+    ChunkStatus* ring_h = nullptr;
+    ChunkStatus* ring_d = nullptr;
+    volatile int* cancel_h = nullptr;
+    int* cancel_d = nullptr;
+    ChunkEngine eng;
+    ProgressLoop pl;
+
+    Job2D() { dims = 2; }
+    ~Job2D() override;
+    int create(const orf_sim2d* s);
+    int pick_tiling(int npx, int npz);
+    int init_state();
+    int advance(int64_t nsteps, orf_progress_fn progress, void* user) override;
+    int64_t steps_done() override;
+    int64_t cells() const override { return (int64_t)nx * nz; }
+    int64_t step_budget() const override { return nmax; }
+    int reset() override;
+    int get_fields(double* const* f, int nf) override;
+    int finish2d(orf_out2d* o) override;
+};
+
+}  // namespace orf

@@ -1,0 +1,211 @@
+// orf_internal.cuh -- device-side data model of the B200 Yee-FDTD engine.
+//
+// One "instance" is one orf.fdtd2D / orf.fdtd3D run.  Instances live in a
+// device table; the step kernels walk a list of tiles (instance, output
+// rectangle) so that a single run, a batch of hundreds of runs and the
+// serving loop all use the same kernels.  Every instance advances in
+// "chunks" of kChunk steps: the step kernels (each fusing up to T time steps
+// of the H and E updates, CPML, TF/SF source and DFT sampling), then one DFT
+// flush kernel and one energy/shutoff check kernel.  Chunk boundaries are
+// where the reference calls its progress callback (fdtd2D.m:18-20).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace orf {
+
+constexpr int kChunk = 50;        // steps between energy checks and progress calls
+constexpr int kMaxMon = 16;       // monitors per orientation per instance
+constexpr int kMaxSub = 32;       // max time steps fused in one step-kernel launch
+constexpr int kStatusRing = 64;   // status ring entries per job (mapped host memory)
+
+// Written by the check kernel into mapped pinned host memory.
+struct ChunkStatus {
+    long long seq;          // chunk number + 1 (written last)
+    long long step;         // steps completed
+    double energy;
+    double peak;
+    int done;
+    int converged;
+};
+
+// Device-resident run state of one instance.
+struct JobState {
+    long long step;         // steps completed
+    long long nmax;         // step budget from maxTime
+    long long chunk;        // chunks completed
+    int done;               // no more steps (shutoff, budget or cancel)
+    int converged;          // stopped by the energy shutoff
+    int cur;                // field buffer (0/1) holding the latest state
+    int pad;
+    double energy;          // energy accumulator of the current chunk
+    double peak;
+    double S;               // c0*dt [um]
+    double src_end;         // end of the source pulse (c0*t)
+    double shutoff;
+    ChunkStatus* ring;      // mapped host ring, kStatusRing entries (may be null)
+    const volatile int* cancel;   // mapped host flag: non-zero stops the run at the next check
+};
+
+// One DFT stream: a monitor line (or plane) of one field, sampled every step
+// into the chunk's sample buffer and folded into running DFT sums by the
+// flush kernel.  Kernel e^{+i w t} (fdtd2DTE.m:18).
+struct DftStream {
+    JobState* st;
+    const void* samples;    // sample buffer of the instance (Real)
+    int sstride;            // elements per step in that buffer
+    int soff;               // offset of this stream inside one step's samples
+    int len;                // elements
+    int half;               // 1: field lives at t_{n+1/2}, 0: at t_{n+1}
+    int nl;                 // wavelengths
+    int pad;
+    const double* omega;    // 2*pi/lambda, nl values
+    void* acc;              // FP64: double2[nl][len]; FP32: float4[nl][len] (sum re, im; Kahan c re, im)
+};
+
+struct FlushItem {          // one block of the flush kernel
+    int stream;
+    int e0;                 // first element
+    int l0;                 // first wavelength
+    int pad;
+};
+
+// --------------------------------------------------------------------- 2D --
+// P/A/B fields (fdtd2D.m:3-7): TE P=Ey A=Hx B=Hz, TM P=Hy A=-Ex B=-Ez.
+// Device layout: every field is [nz][pitch] with x fastest, pitch a multiple
+// of 32 elements; A's row nz-1 (non-periodic) and B's column nx-1 do not
+// exist in the reference and stay zero here.
+template <class R>
+struct Inst2D {
+    int nx, nz, pitch, nzA, nxB;
+    int periodic, te;
+    int npx, npz;           // CPML cells per end (npz = 0 when periodic)
+    int idx16;              // material index width: 0 = uint8, 1 = uint16
+    R C;                    // courant number c0*dt/dx
+    R* P[2];
+    R* A[2];
+    R* B[2];
+    const void* idx0;       // TE: material index at P; TM: at A
+    const void* idx1;       // TM: material index at B
+    const R* lutc;          // C / eps per material index
+    const double* lute;     // eps per material index (energy)
+    // CPML profiles, (b, a, 1/kappa) interleaved: columns at P (x_i) and at
+    // B (x_i+1/2), rows at P (z_k) and at A (z_k+1/2)
+    const R* pmlx;
+    const R* pmlxh;
+    const R* pmlz;
+    const R* pmlzh;
+    // psi in compact slabs, ping-pong: x slabs [nz][2*npx], z slabs [2*npz][nx]
+    R* psiB[2];
+    R* psiPx[2];
+    R* psiA[2];
+    R* psiPz[2];
+    // TF/SF plane at P column src_ix: B column src_ix-1 gets srcB[k]*gE[n],
+    // P column src_ix gets srcP[k]*gH[n]
+    int src_ix;
+    int nmon, nmonz;
+    int sstride;            // samples per step: 2*nz*nmon + 2*nx*nmonz
+    const R* srcB;
+    const R* srcP;
+    const double* gE;
+    const double* gH;
+    long long nsrc;         // table length (pulse is zero beyond)
+    int mon[kMaxMon];
+    int monz[kMaxMon];
+    R* samples;             // [kChunk][sstride]
+    JobState* st;
+};
+
+struct Tile2D {
+    int inst;
+    int oi0, ok0;           // output origin (global cell coordinates)
+    short ow, oh;           // output extent
+};
+
+// --------------------------------------------------------------------- 3D --
+// Six components at their Yee positions (fdtd3D.m:2-5); layout [nz][ny][pitch].
+template <class R>
+struct Inst3D {
+    int n[3];
+    int pitch;
+    int per[3];
+    int np[3];              // CPML cells per end per axis
+    int idx16;
+    R C;
+    R* E[2][3];
+    R* H[2][3];
+    const void* idx[3];     // material index of Ex, Ey, Ez
+    const R* lutc;          // C / eps
+    const double* lute;
+    // CPML profiles per axis: integer (E derivative) and half (H derivative)
+    const R* pmlI[3];
+    const R* pmlH[3];
+    // psi per (component c, derivative axis q), compact along q:
+    // index [k][j][i] with the q coordinate replaced by its slab index
+    R* psiE[2][3][3];
+    R* psiH[2][3][3];
+    int nslabI[3], nslabH[3];
+    const int* slabI[3];    // slab index per coordinate along axis q, -1 outside
+    const int* slabH[3];
+    // source plane (axis sa, index ss): profiles Na x Nb (a fastest)
+    int sa, ss, na, nb;
+    const R* sEa;           // C * Ea * (per-E coefficient folded in at use)
+    const R* sEb;
+    const R* sHa;
+    const R* sHb;
+    const double* gE;
+    const double* gH;
+    long long nsrc;
+    int nmon;
+    int sstride;
+    int mon_axis[kMaxMon];
+    int mon_index[kMaxMon];
+    int mon_off[kMaxMon];   // offset of the monitor's 4 planes in one step's samples
+    R* samples;
+    JobState* st;
+};
+
+struct Tile3D {
+    int inst;
+    int oi0, oj0;           // output origin in x, y
+    short ow, oh;           // output extent in x, y (z is marched in full)
+};
+
+// ------------------------------------------------------------- launchers --
+// Implemented in step2d.cu / step3d.cu / dft.cu.
+struct Variant2D {
+    int id;
+    int ks, wx, wz;         // strip length, warps along x, warps along z
+    int lx() const { return 32 * wx; }
+    int lz() const { return ks * wz; }
+};
+
+// Returns the tile geometry of a compiled 2D variant (false if id unknown).
+bool variant2d_info(int id, bool fp64, Variant2D* v);
+int variant2d_count();
+
+cudaError_t launch_step2d(bool fp64, bool te, bool idx16, bool pml, int variant, const void* insts,
+                          const Tile2D* tiles, int ntiles, int halo, int launch_off, int nsub,
+                          int par, int want_energy, int grid, cudaStream_t s);
+size_t step2d_smem(bool fp64, bool te, bool pml, int variant);
+int step2d_blocks_per_sm(bool fp64, bool te, bool idx16, bool pml, int variant);
+
+cudaError_t launch_step3d(bool fp64, bool idx16, const void* insts, const Tile3D* tiles, int ntiles,
+                          int launch_off, int par, int want_energy, int grid, cudaStream_t s);
+int step3d_tile(bool fp64, int* tx, int* ty);
+int step3d_blocks_per_sm(bool fp64, bool idx16);
+
+cudaError_t launch_flush(bool fp64, const DftStream* streams, const FlushItem* items, int nitems,
+                         cudaStream_t s);
+cudaError_t launch_check(JobState* const* states, int n, cudaStream_t s);
+// flux[out + ostride*l] = scale * sum_e (Re(a1 conj(b1)) - Re(a2 conj(b2)))
+struct FluxPair {
+    int a1, b1, a2, b2;     // stream indices; a2 < 0: no second product
+    int out, ostride;
+    double scale;
+};
+cudaError_t launch_flux(bool fp64, const DftStream* streams, const FluxPair* pairs, int npairs, int nl,
+                        double* out, cudaStream_t s);
+cudaError_t launch_acc_to_complex(bool fp64, const void* acc, size_t n, double2* out, cudaStream_t s);
+
+}  // namespace orf

@@ -1,0 +1,238 @@
+// runtime.cu -- errors, shared physics definitions, context, chunk engine.
+#include <atomic>
+#include <thread>
+
+#include "engine.cuh"
+
+namespace orf {
+
+namespace {
+thread_local std::string g_err;
+}
+
+void set_error(const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+}
+const char* last_error() { return g_err.c_str(); }
+
+void pml_profile(int n, int npts, int npml, double off, double dx, double S, double alpha_max,
+                 std::vector<double>& bak, int* nslab) {
+    bak.assign((size_t)3 * npts, 0.0);
+    int ns = 0;
+    for (int i = 0; i < npts; ++i) {
+        bak[3 * i] = 1.0;
+        bak[3 * i + 1] = 0.0;
+        bak[3 * i + 2] = 1.0;
+        if (npml <= 0) continue;
+        const double u = i + off;
+        const double lo = npml, hi = (n - 1) - npml;
+        double depth = 0.0;
+        if (u < lo) depth = lo - u;
+        else if (u > hi) depth = u - hi;
+        if (depth <= 0.0) continue;
+        const double m = kPmlOrder;
+        const double sigma_max = 0.8 * (m + 1.0) / dx;
+        const double r = std::min(depth / npml, 1.0);
+        const double rm = std::pow(r, m);
+        const double sigma = sigma_max * rm;
+        const double kappa = 1.0 + (kPmlKappaMax - 1.0) * rm;
+        const double alpha = alpha_max * (1.0 - r);
+        const double b = std::exp(-(sigma / kappa + alpha) * S);
+        const double den = sigma * kappa + kappa * kappa * alpha;
+        bak[3 * i] = b;
+        bak[3 * i + 1] = den > 0.0 ? sigma / den * (b - 1.0) : 0.0;
+        bak[3 * i + 2] = 1.0 / kappa;
+        ++ns;
+    }
+    if (nslab) *nslab = ns;
+}
+
+int64_t max_steps(double max_time, double S) {
+    const double r = max_time / S;
+    const int64_t n = (int64_t)std::ceil(r - 1e-9);
+    return n < 0 ? 0 : n;
+}
+
+// fdtdProgress.m:6-12
+double progress_fraction(double t, double src_end, double ratio, double shutoff) {
+    double frac;
+    if (t <= src_end) {
+        frac = 0.3 * t / src_end;
+    } else {
+        const double so = shutoff > 0.0 ? shutoff : 1e-300;
+        const double decay = std::log(std::max(ratio, so)) / std::log(so);
+        frac = 0.3 + 0.7 * std::max(0.0, std::min(1.0, decay));
+    }
+    return std::max(0.0, std::min(1.0, frac));
+}
+
+// ----------------------------------------------------------- ChunkEngine --
+ChunkEngine::~ChunkEngine() {
+    drop_graph();
+    for (auto e : evpool) cudaEventDestroy(e);
+}
+
+void ChunkEngine::drop_graph() {
+    if (gexec) cudaGraphExecDestroy(gexec);
+    gexec = nullptr;
+    gchunks = 0;
+    gpar = -1;
+}
+
+int ChunkEngine::enqueue_chunk(cudaStream_t s, bool timed) {
+    if (timed) {
+        while (evpool.size() < evused + 4) {
+            cudaEvent_t e;
+            ORF_CUDA(cudaEventCreate(&e));
+            evpool.push_back(e);
+        }
+        ORF_CUDA(cudaEventRecord(evpool[evused], s));
+    }
+    for (int off = 0; off < kChunk; off += T) {
+        const int nsub = std::min(T, kChunk - off);
+        const int we = (off + nsub == kChunk) ? 1 : 0;
+        ORF_CUDA(step(off, nsub, par, we, s));
+        par ^= 1;
+    }
+    if (timed) ORF_CUDA(cudaEventRecord(evpool[evused + 1], s));
+    ORF_CUDA(launch_flush(fp64, d_streams, d_items, nitems, s));
+    ORF_CUDA(launch_check(d_states, nstates, s));
+    if (timed) {
+        ORF_CUDA(cudaEventRecord(evpool[evused + 2], s));
+        evused += 3;
+    }
+    return ORF_OK;
+}
+
+int ChunkEngine::enqueue(int nchunks, cudaStream_t s) {
+    const bool timed = ctx->timing;
+    const bool use_graph = ctx->tuning.use_graph != 0 && !timed;
+    const int lpc = launches_per_chunk();
+    // graph of G chunks with an even launch count, so the buffer parity is
+    // the same before and after every replay
+    const int G = (lpc & 1) ? 8 : 4;
+    while (nchunks > 0) {
+        if (use_graph && nchunks >= G) {
+            if (!gexec || gpar != par || gchunks != G) {
+                drop_graph();
+                const int p0 = par;
+                cudaGraph_t g = nullptr;
+                ORF_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+                int st = ORF_OK;
+                for (int c = 0; c < G && st == ORF_OK; ++c) st = enqueue_chunk(s, false);
+                cudaError_t ce = cudaStreamEndCapture(s, &g);
+                if (st != ORF_OK) {
+                    if (g) cudaGraphDestroy(g);
+                    par = p0;
+                    return st;
+                }
+                ORF_CUDA(ce);
+                cudaError_t ie = cudaGraphInstantiate(&gexec, g, 0);
+                cudaGraphDestroy(g);
+                ORF_CUDA(ie);
+                par = p0;   // capture only recorded the launches
+                gpar = p0;
+                gchunks = G;
+            }
+            ORF_CUDA(cudaGraphLaunch(gexec, s));
+            par ^= (G * lpc) & 1;
+            nchunks -= G;
+        } else {
+            ORF_TRY(enqueue_chunk(s, timed));
+            nchunks -= 1;
+        }
+    }
+    return ORF_OK;
+}
+
+void ChunkEngine::collect_timing(int64_t cell_updates) {
+    if (!ctx->timing) return;
+    for (size_t q = 0; q + 2 < evused + 1 && q + 2 <= evused; q += 3) {
+        float a = 0.f, b = 0.f;
+        if (cudaEventElapsedTime(&a, evpool[q], evpool[q + 1]) == cudaSuccess) {
+            ctx->stats.step_ms += a;
+            ctx->stats.step_launches += launches_per_chunk();
+        }
+        if (cudaEventElapsedTime(&b, evpool[q + 1], evpool[q + 2]) == cudaSuccess) {
+            ctx->stats.flush_ms += b;
+            ctx->stats.flush_launches += 2;
+        }
+    }
+    cudaGetLastError();
+    ctx->stats.cell_updates += cell_updates;
+    evused = 0;
+}
+
+// ---------------------------------------------------------- ProgressLoop --
+int ProgressLoop::poll(orf_progress_fn progress, void* user) {
+    if (!ring) return ORF_OK;
+    for (;;) {
+        const volatile ChunkStatus* r = ring + (seen % kStatusRing);
+        const long long seq = r->seq;
+        if (seq != seen + 1) break;
+        std::atomic_thread_fence(std::memory_order_acquire);
+        const long long step = r->step;
+        const double e = r->energy, pk = r->peak;
+        const int dn = r->done;
+        ++seen;
+        last_step = step;
+        if (progress && !done) {
+            const double t = step * S;
+            const double ratio = pk > 0.0 ? e / pk : 1.0;
+            const double fr = r->converged ? 1.0 : progress_fraction(t, src_end, ratio, shutoff);
+            char msg[96];
+            std::snprintf(msg, sizeof msg, "step %lld, t = %.3g um", step, t);
+            if (progress(fr, msg, user)) {
+                if (cancel) *cancel = 1;
+                done = true;
+                cancelled = true;
+                return ORF_ECANCELLED;
+            }
+        }
+        if (dn) {
+            done = true;
+            break;
+        }
+    }
+    return ORF_OK;
+}
+
+int run_chunks(ChunkEngine& eng, ProgressLoop& pl, orf_ctx* ctx, int64_t chunks, orf_progress_fn progress,
+               void* user) {
+    cudaStream_t st = ctx->stream;
+    constexpr int kBatch = 8, kInFlight = 4;
+    std::vector<cudaEvent_t> evs;
+    int64_t enq = 0;
+    size_t head = 0;
+    int rc = ORF_OK;
+    while (!pl.done) {
+        while (enq < chunks && evs.size() - head < (size_t)kInFlight && !pl.done) {
+            const int n = (int)std::min<int64_t>(kBatch, chunks - enq);
+            ORF_TRY(eng.enqueue(n, st));
+            enq += n;
+            cudaEvent_t e;
+            ORF_CUDA(cudaEventCreateWithFlags(&e, cudaEventBlockingSync | cudaEventDisableTiming));
+            ORF_CUDA(cudaEventRecord(e, st));
+            evs.push_back(e);
+        }
+        if (head < evs.size()) {
+            ORF_CUDA(cudaEventSynchronize(evs[head]));
+            ++head;
+        }
+        rc = pl.poll(progress, user);
+        if (rc != ORF_OK) break;
+        if (head == evs.size() && enq >= chunks) break;
+    }
+    cudaError_t e = cudaStreamSynchronize(st);
+    for (auto ev : evs) cudaEventDestroy(ev);
+    ORF_CUDA(e);
+    if (rc == ORF_OK) rc = pl.poll(progress, user);
+    return rc == ORF_ECANCELLED ? ORF_OK : rc;
+}
+
+}  // namespace orf

@@ -1,0 +1,156 @@
+// runtime.cuh -- host-side runtime shared by the 2D, 3D, batch and serve paths.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "orf_fdtd.h"
+#include "orf_internal.cuh"
+
+namespace orf {
+
+// ------------------------------------------------------------------ errors --
+void set_error(const char* fmt, ...);
+const char* last_error();
+
+struct Err {
+    int code = ORF_OK;
+    explicit operator bool() const { return code != ORF_OK; }
+};
+
+#define ORF_CUDA(call)                                                                    \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess) {                                                          \
+            ::orf::set_error("%s:%d: %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(e_)); \
+            return e_ == cudaErrorMemoryAllocation ? ORF_ENOMEM_DEVICE : ORF_ECUDA;       \
+        }                                                                                 \
+    } while (0)
+
+#define ORF_TRY(expr)                      \
+    do {                                   \
+        int s_ = (expr);                   \
+        if (s_ != ORF_OK) return s_;       \
+    } while (0)
+
+inline double now_s() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// --------------------------------------------------------- shared physics --
+// These restate the reference's documented formulas; the CPU oracle holds an
+// independent copy of the same definitions.
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kPmlOrder = 3.0;          // cpmlCoefficients.m:6-8 grading law; constants chosen here
+constexpr double kPmlKappaMax = 1.0;
+constexpr double kPmlAlphaMaxPerK0 = 0.0;
+
+// Gaussian pulse of relative 1/e spectral half-width bw (fdtd2DTE.m:14-15):
+// g(t) = exp(-((t-t0)/tau)^2) sin(k0 (t-t0)), tau = 2/(bw k0), t0 = 5 tau, zero outside [0, 2 t0].
+struct Pulse {
+    double k0, tau, t0, tend;
+    Pulse(double lambda0, double bw) {
+        k0 = 2.0 * kPi / lambda0;
+        tau = 2.0 / (bw * k0);
+        t0 = 5.0 * tau;
+        tend = 2.0 * t0;
+    }
+    double operator()(double t) const {
+        if (t < 0.0 || t > tend) return 0.0;
+        const double u = (t - t0) / tau;
+        return std::exp(-u * u) * std::sin(k0 * (t - t0));
+    }
+};
+
+// CPML (b, a, 1/kappa) at positions u = i + off on an n-point grid with npml
+// cells per end (cpmlCoefficients.m:2-8); identity outside the layer.
+void pml_profile(int n, int npts, int npml, double off, double dx, double S, double alpha_max,
+                 std::vector<double>& bak, int* nslab);
+
+int64_t max_steps(double max_time, double S);
+double progress_fraction(double t, double src_end, double ratio, double shutoff);
+
+// ---------------------------------------------------------------- context --
+struct orf_ctx_impl;
+
+// Bump allocator over one cudaMalloc: a job's buffers come from one block.
+struct Arena {
+    std::vector<std::pair<void**, size_t>> req;
+    void* base = nullptr;
+    size_t total = 0;
+    template <class T>
+    void add(T** p, size_t n) {
+        req.push_back({reinterpret_cast<void**>(p), n * sizeof(T)});
+    }
+    size_t bytes() const {
+        size_t s = 0;
+        for (auto& r : req) s += (r.second + 255) & ~size_t(255);
+        return s;
+    }
+    int alloc() {
+        total = bytes();
+        if (total == 0) return ORF_OK;
+        cudaError_t e = cudaMalloc(&base, total);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            set_error("device allocation of %.3f GB failed: %s", total / 1e9, cudaGetErrorString(e));
+            return ORF_ENOMEM_DEVICE;
+        }
+        char* p = static_cast<char*>(base);
+        for (auto& r : req) {
+            *r.first = p;
+            p += (r.second + 255) & ~size_t(255);
+        }
+        return ORF_OK;
+    }
+    void release() {
+        if (base) cudaFree(base);
+        base = nullptr;
+    }
+};
+
+}  // namespace orf
+
+struct orf_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int sm_count = 148;
+    orf_tuning tuning{};
+    bool timing = false;
+    orf_kernel_stats stats{};
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+// A device-resident run (2D or 3D).  Implemented in job2d.cu / job3d.cu.
+struct orf_job {
+    virtual ~orf_job() = default;
+    orf_ctx* ctx = nullptr;
+    int dims = 2;
+    virtual int advance(int64_t nsteps, orf_progress_fn progress, void* user) = 0;
+    virtual int64_t steps_done() = 0;
+    virtual int64_t step_budget() const = 0;
+    virtual int64_t cells() const = 0;
+    virtual int reset() = 0;
+    virtual int get_fields(double* const* f, int nf) = 0;
+    virtual int finish2d(orf_out2d*) { return ORF_EINVAL; }
+    virtual int finish3d(orf_out3d*) { return ORF_EINVAL; }
+};
+
+namespace orf {
+int make_job2d(orf_ctx* ctx, const orf_sim2d* sim, orf_job** out);
+int make_job3d(orf_ctx* ctx, const orf_sim3d* sim, orf_job** out);
+int batch2d_run(orf_ctx* ctx, int n, const orf_sim2d* sims, orf_out2d* outs, orf_progress_fn progress,
+                void* user);
+int validate2d(const orf_sim2d* s);
+int validate3d(const orf_sim3d* s);
+orf_ctx* default_ctx(int* status);
+}  // namespace orf

@@ -1,0 +1,175 @@
+"""orf.fdtd2D / orf.fdtd2DTE / orf.fdtd3D on the B200 engine.
+
+Host-side mirror of the reference's MATLAB interface (toolbox/+orf/fdtd2D.m,
+fdtd2DTE.m:33-34, fdtd3D.m): the same sim fields with the same defaults and
+1-based indices, the same out fields (flux, DFT lines, TE/TM aliases,
+converged, steps, time, wallTime), the same progress/cancel behaviour (an
+exception raised in sim['progress'] stops the run and propagates unchanged,
+tests/TestGUISupport.m:39-43) and the same fdtd2D:notConverged warning.
+Everything numeric runs in liborf_fdtd.so; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import warnings
+
+import numpy as np
+
+from . import _abi, _lib
+
+
+class Context:
+    """An orf_ctx: one device, one CUDA stream, tuning knobs and kernel timing."""
+
+    def __init__(self, device: int = 0, stream: int | None = None):
+        self._lib = _lib.load()
+        h = C.c_void_p()
+        _lib.check(self._lib.orf_ctx_create(device, C.c_void_p(stream) if stream else None, C.byref(h)),
+                   "orf_ctx_create")
+        self.handle = h
+
+    def set_tuning(self, tsteps: int = 0, variant: int = 0, use_graph: bool = True) -> None:
+        t = _abi.OrfTuning(tsteps, variant, 1 if use_graph else 0, 0)
+        _lib.check(self._lib.orf_ctx_set_tuning(self.handle, C.byref(t)), "orf_ctx_set_tuning")
+
+    def set_timing(self, on: bool) -> None:
+        _lib.check(self._lib.orf_ctx_set_timing(self.handle, 1 if on else 0))
+
+    def stats(self) -> dict:
+        s = _abi.OrfKernelStats()
+        _lib.check(self._lib.orf_ctx_get_stats(self.handle, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in s._fields_}
+
+    def reset_stats(self) -> None:
+        _lib.check(self._lib.orf_ctx_reset_stats(self.handle))
+
+    def close(self) -> None:
+        if self.handle:
+            self._lib.orf_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _warn_nc(out: dict, name: str) -> None:
+    if not out["converged"]:
+        warnings.warn(f"{name}:notConverged: maxTime reached before the field energy fell below the shutoff",
+                      _abi.NotConvergedWarning, stacklevel=3)
+
+
+def fdtd2D(sim, ctx: Context | None = None) -> dict:
+    """out = fdtd2D(sim): 2D TE/TM FDTD (fdtd2D.m:1-29) on the GPU."""
+    lib = _lib.load()
+    m = _abi.marshal_sim2d(sim)
+    o, bufs = _abi.alloc_out2d(m)
+    cb, box = _abi.make_progress(_abi._get(sim, "progress"))
+    fn = cb or _abi.PROGRESS_FN(0)
+    if ctx is None:
+        st = lib.orf_fdtd2d_run(C.byref(m.struct), C.byref(o), fn, None)
+    else:
+        st = lib.orf_fdtd2d_run_ctx(ctx.handle, C.byref(m.struct), C.byref(o), fn, None)
+    if box and "exc" in box:
+        raise box["exc"]
+    _lib.check(st, "fdtd2D")
+    out = _abi.finish_out2d(m, o, bufs)
+    _warn_nc(out, "fdtd2D")
+    return out
+
+
+def fdtd2DTE(sim, ctx: Context | None = None) -> dict:
+    """fdtd2D with sim.pol = "TE" (fdtd2DTE.m:33-34)."""
+    sim = dict(sim) if isinstance(sim, dict) else dict(vars(sim))
+    sim["pol"] = "TE"
+    return fdtd2D(sim, ctx)
+
+
+def fdtd3D(sim, ctx: Context | None = None) -> dict:
+    """out = fdtd3D(sim): 3D Yee FDTD (fdtd3D.m:1-29) on the GPU."""
+    lib = _lib.load()
+    m = _abi.marshal_sim3d(sim)
+    o, bufs = _abi.alloc_out3d(m)
+    cb, box = _abi.make_progress(_abi._get(sim, "progress"))
+    fn = cb or _abi.PROGRESS_FN(0)
+    if ctx is None:
+        st = lib.orf_fdtd3d_run(C.byref(m.struct), C.byref(o), fn, None)
+    else:
+        st = lib.orf_fdtd3d_run_ctx(ctx.handle, C.byref(m.struct), C.byref(o), fn, None)
+    if box and "exc" in box:
+        raise box["exc"]
+    _lib.check(st, "fdtd3D")
+    out = _abi.finish_out3d(m, o, bufs)
+    _warn_nc(out, "fdtd3D")
+    return out
+
+
+class Job:
+    """Device-resident run: fields and DFT sums stay on the GPU between
+    advance() calls (orf_job_* in include/orf_fdtd.h)."""
+
+    def __init__(self, sim, ctx: Context, dims: int = 2):
+        self.lib = _lib.load()
+        self.ctx = ctx
+        self.dims = dims
+        self.m = _abi.marshal_sim2d(sim) if dims == 2 else _abi.marshal_sim3d(sim)
+        h = C.c_void_p()
+        fn = self.lib.orf_job2d_create if dims == 2 else self.lib.orf_job3d_create
+        _lib.check(fn(ctx.handle, C.byref(self.m.struct), C.byref(h)), "job create")
+        self.handle = h
+
+    def advance(self, nsteps: int) -> None:
+        _lib.check(self.lib.orf_job_advance(self.handle, int(nsteps)), "advance")
+
+    def sync(self) -> None:
+        _lib.check(self.lib.orf_job_sync(self.handle), "sync")
+
+    def reset(self) -> None:
+        _lib.check(self.lib.orf_job_reset(self.handle), "reset")
+
+    @property
+    def steps(self) -> int:
+        return int(self.lib.orf_job_steps_done(self.handle))
+
+    @property
+    def cells(self) -> int:
+        return int(self.lib.orf_job_cells(self.handle))
+
+    def fields(self) -> list[np.ndarray]:
+        """Current fields in the reference layout: 2D [P, A, B]; 3D [Ex Ey Ez Hx Hy Hz]."""
+        if self.dims == 2:
+            nx, nz = self.m.meta["nx"], self.m.meta["nz"]
+            per = bool(self.m.struct.periodic_z)
+            shapes = [(nx, nz), (nx, nz if per else nz - 1), (nx - 1, nz)]
+        else:
+            shapes = [tuple(self.m.meta["n"])] * 6
+        arrs = [np.zeros(s, order="F") for s in shapes]
+        ptrs = (C.POINTER(C.c_double) * len(arrs))(*[a.ctypes.data_as(C.POINTER(C.c_double)) for a in arrs])
+        _lib.check(self.lib.orf_job_get_fields(self.handle, ptrs, len(arrs)), "get_fields")
+        return arrs
+
+    def finish(self) -> dict:
+        if self.dims == 2:
+            o, bufs = _abi.alloc_out2d(self.m)
+            _lib.check(self.lib.orf_job2d_finish(self.handle, C.byref(o)), "finish")
+            return _abi.finish_out2d(self.m, o, bufs)
+        o, bufs = _abi.alloc_out3d(self.m)
+        _lib.check(self.lib.orf_job3d_finish(self.handle, C.byref(o)), "finish")
+        return _abi.finish_out3d(self.m, o, bufs)
+
+    def close(self) -> None:
+        if self.handle:
+            self.lib.orf_job_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def device_count() -> int:
+    return int(_lib.load().orf_device_count())

@@ -1,0 +1,355 @@
+"""Subpixel-averaged permittivity on the Yee grid (host-side preparation).
+
+Mirrors the reference's geometry front end of the FDTD:
+  - epsFromBoxes     toolbox/+orf/epsFromBoxes.m:1-31 (open code)
+  - epsCellMean      toolbox/+orf/epsCellMean.m:1-9 (documented behaviour)
+  - epsComponents2D  toolbox/+orf/epsComponents2D.m:1-10 (documented behaviour)
+  - epsComponents3D  toolbox/+orf/epsComponents3D.m:1-27 (documented behaviour)
+
+Boxes are painted in order, later rows over earlier (epsFromBoxes.m:4-5), a
+sample at (X, Z) being inside a box when x1 <= X < x2 and z1 <= Z < z2
+(epsFromBoxes.m:25).  Each painter visits only the sample columns/rows a box
+covers (found by binary search), so cost scales with box area, not grid area.
+"""
+from __future__ import annotations
+
+from typing import Any, Sequence
+
+import numpy as np
+
+
+def _offsets(nsub: int) -> np.ndarray:
+    # epsFromBoxes.m:17
+    return (np.arange(1, nsub + 1) - (nsub + 1) / 2.0) / nsub
+
+
+def _ranges(coords: np.ndarray, lo: float, hi: float) -> tuple[int, int]:
+    """Index range [a, b) of sorted coords with lo <= c < hi."""
+    a = int(np.searchsorted(coords, lo, side="left"))
+    b = int(np.searchsorted(coords, hi, side="left"))
+    return a, b
+
+
+def _paint2d(xs: np.ndarray, zs: np.ndarray, nbg: float, boxes: np.ndarray,
+             wrap_z: tuple[float, float] | None = None) -> np.ndarray:
+    """eps of axis-aligned boxes at sample points xs (sorted) x zs."""
+    e = np.full((xs.size, zs.size), float(nbg) ** 2)
+    if wrap_z is not None:
+        z0, L = wrap_z
+        zf = z0 + np.mod(zs - z0, L)
+        order = np.argsort(zf, kind="stable")
+        zsorted = zf[order]
+    for b in boxes:
+        i0, i1 = _ranges(xs, b[0], b[1])
+        if i1 <= i0:
+            continue
+        val = b[4] ** 2
+        if wrap_z is None:
+            k0, k1 = _ranges(zs, b[2], b[3])
+            if k1 > k0:
+                e[i0:i1, k0:k1] = val
+        else:
+            # the structure repeats with period L: fold the box into [z0, z0+L)
+            lo, hi = b[2], b[3]
+            if hi - lo >= L:
+                spans = [(z0, z0 + L)]
+            else:
+                a = z0 + np.mod(lo - z0, L)
+                end = a + (hi - lo)
+                spans = [(a, min(end, z0 + L))]
+                if end > z0 + L:
+                    spans.append((z0, end - L))
+            for s0, s1 in spans:
+                k0, k1 = _ranges(zsorted, s0, s1)
+                if k1 > k0:
+                    e[i0:i1, order[k0:k1]] = val
+    return e
+
+
+def _as_boxes(boxes) -> np.ndarray:
+    b = np.asarray(boxes, dtype=float)
+    if b.size == 0:
+        return np.zeros((0, 5))
+    return b.reshape(-1, 5)
+
+
+def epsCellMean(xc, yc, dx: float, dy: float, boxes, nBg: float, harmonicDir: str = "none",
+                NSub: int = 4, WrapY: Sequence[float] | None = None) -> np.ndarray:
+    """Cell-averaged eps of boxes [x1 x2 y1 y2 n] at points (xc, yc), ndgrid layout.
+
+    harmonicDir "none": arithmetic mean of NSub x NSub samples; "x" / "y":
+    harmonic mean along that direction, then arithmetic along the other
+    (epsCellMean.m:6-8).  WrapY = [y0 Ly] folds sample y into [y0, y0+Ly).
+    """
+    xc = np.asarray(xc, dtype=float).ravel()
+    yc = np.asarray(yc, dtype=float).ravel()
+    boxes = _as_boxes(boxes)
+    off = _offsets(NSub)
+    wrap = None if WrapY is None else (float(WrapY[0]), float(WrapY[1]))
+    if harmonicDir == "none":
+        acc = np.zeros((xc.size, yc.size))
+        for ox in off:
+            xs = xc + ox * dx
+            for oy in off:
+                acc += _paint2d(xs, yc + oy * dy, nBg, boxes, wrap)
+        return acc / NSub ** 2
+    if harmonicDir == "x":
+        acc = np.zeros((xc.size, yc.size))
+        for oy in off:
+            inv = np.zeros((xc.size, yc.size))
+            for ox in off:
+                inv += 1.0 / _paint2d(xc + ox * dx, yc + oy * dy, nBg, boxes, wrap)
+            acc += NSub / inv
+        return acc / NSub
+    if harmonicDir == "y":
+        acc = np.zeros((xc.size, yc.size))
+        for ox in off:
+            inv = np.zeros((xc.size, yc.size))
+            for oy in off:
+                inv += 1.0 / _paint2d(xc + ox * dx, yc + oy * dy, nBg, boxes, wrap)
+            acc += NSub / inv
+        return acc / NSub
+    raise ValueError('harmonicDir must be "none", "x" or "y"')
+
+
+def epsFromBoxes(x, z, nBackground: float, boxes, nSub: int = 4) -> np.ndarray:
+    """Arithmetic cell mean at the grid points (epsFromBoxes.m:1-31)."""
+    x = np.asarray(x, dtype=float).ravel()
+    z = np.asarray(z, dtype=float).ravel()
+    return epsCellMean(x, z, x[1] - x[0], z[1] - z[0], boxes, nBackground, "none", nSub)
+
+
+def epsComponents2D(x, z, nBg: float, boxes, NSub: int = 4, PeriodicZ: bool = False) -> dict:
+    """eps at the 2D Yee locations (epsComponents2D.m:2-10).
+
+    e["y"] at (x_i, z_k): arithmetic mean (numel(x) x numel(z));
+    e["x"] at (x_i, z_k+1/2): harmonic along x, arithmetic along z
+           (numel(x) x numel(z)-1, or numel(z) when PeriodicZ);
+    e["z"] at (x_i+1/2, z_k): harmonic along z, arithmetic along x
+           ((numel(x)-1) x numel(z)).
+    """
+    x = np.asarray(x, dtype=float).ravel()
+    z = np.asarray(z, dtype=float).ravel()
+    dx, dz = x[1] - x[0], z[1] - z[0]
+    wrap = (z[0] - dz / 2, z.size * dz) if PeriodicZ else None
+    zh = z + dz / 2 if PeriodicZ else z[:-1] + dz / 2
+    xh = x[:-1] + dx / 2
+    return {
+        "y": epsCellMean(x, z, dx, dz, boxes, nBg, "none", NSub, wrap),
+        "x": epsCellMean(x, zh, dx, dz, boxes, nBg, "x", NSub, wrap),
+        "z": epsCellMean(xh, z, dx, dz, boxes, nBg, "y", NSub, wrap),
+    }
+
+
+# --------------------------------------------------------------------- 3D --
+def _shape_list(shapes) -> list[tuple[str, Any]]:
+    out = []
+    for s in shapes or []:
+        kind, par = s[0], s[1]
+        out.append((str(kind).lower(), par))
+    return out
+
+
+def _get(p, name, default=None):
+    if isinstance(p, dict):
+        return p.get(name, default)
+    return getattr(p, name, default)
+
+
+class _Shape:
+    """Inside test and interface band of one epsComponents3D shape."""
+
+    def __init__(self, kind: str, par: Any):
+        self.kind = kind
+        if kind == "box":
+            b = np.asarray(par, dtype=float).ravel()
+            self.lo = b[[0, 2, 4]]
+            self.hi = b[[1, 3, 5]]
+            self.n = b[6]
+        elif kind in ("cyl", "cone"):
+            b = np.asarray(par, dtype=float).ravel()
+            if kind == "cyl":
+                cx, cy, r, z1, z2, n = b
+                r1 = r2 = r
+            else:
+                cx, cy, r1, r2, z1, z2, n = b
+            self.c = (cx, cy)
+            self.r1, self.r2, self.z1, self.z2, self.n = r1, r2, z1, z2, n
+            rmax = max(r1, r2)
+            self.lo = np.array([cx - rmax, cy - rmax, z1])
+            self.hi = np.array([cx + rmax, cy + rmax, z2])
+        elif kind == "polygon":
+            self.xy = np.asarray(_get(par, "xy"), dtype=float).reshape(-1, 2)
+            self.z1, self.z2 = float(_get(par, "z1")), float(_get(par, "z2"))
+            self.n = float(_get(par, "n"))
+            self.lo = np.array([self.xy[:, 0].min(), self.xy[:, 1].min(), self.z1])
+            self.hi = np.array([self.xy[:, 0].max(), self.xy[:, 1].max(), self.z2])
+        elif kind == "lattice":
+            self.x0, self.y0 = float(_get(par, "x0")), float(_get(par, "y0"))
+            self.P = float(_get(par, "period"))
+            self.R = np.atleast_2d(np.asarray(_get(par, "R"), dtype=float))
+            self.z1, self.z2 = float(_get(par, "z1")), float(_get(par, "z2"))
+            self.n = float(_get(par, "n"))
+            self.dRdz = float(_get(par, "dRdz", 0.0) or 0.0)
+            rmax = float(self.R.max()) + abs(self.dRdz) * (self.z2 - self.z1)
+            self.rmax = rmax
+            self.lo = np.array([self.x0 - rmax, self.y0 - rmax, self.z1])
+            self.hi = np.array([self.x0 + (self.R.shape[0] - 1) * self.P + rmax,
+                                self.y0 + (self.R.shape[1] - 1) * self.P + rmax, self.z2])
+        else:
+            raise ValueError(f"unknown shape kind {kind!r}")
+
+    def inside(self, X, Y, Z):
+        k = self.kind
+        if k == "box":
+            return ((X >= self.lo[0]) & (X < self.hi[0]) & (Y >= self.lo[1]) & (Y < self.hi[1])
+                    & (Z >= self.lo[2]) & (Z < self.hi[2]))
+        if k in ("cyl", "cone"):
+            zin = (Z >= self.z1) & (Z < self.z2)
+            t = np.clip((Z - self.z1) / max(self.z2 - self.z1, 1e-300), 0.0, 1.0)
+            r = self.r1 + (self.r2 - self.r1) * t
+            return zin & ((X - self.c[0]) ** 2 + (Y - self.c[1]) ** 2 < r * r)
+        if k == "polygon":
+            zin = (Z >= self.z1) & (Z < self.z2)
+            xs, ys = self.xy[:, 0], self.xy[:, 1]
+            inside = np.zeros(np.broadcast(X, Y).shape, dtype=bool)
+            Xb, Yb = np.broadcast_arrays(X, Y)
+            for a in range(xs.size):
+                b = (a + 1) % xs.size
+                cond = (ys[a] > Yb) != (ys[b] > Yb)
+                xcross = (xs[b] - xs[a]) * (Yb - ys[a]) / np.where(ys[b] != ys[a], ys[b] - ys[a], 1.0) + xs[a]
+                inside ^= cond & (Xb < xcross)
+            return zin & inside
+        if k == "lattice":
+            ix = np.rint((X - self.x0) / self.P).astype(np.int64)
+            iy = np.rint((Y - self.y0) / self.P).astype(np.int64)
+            ok = (ix >= 0) & (ix < self.R.shape[0]) & (iy >= 0) & (iy < self.R.shape[1])
+            ixc = np.clip(ix, 0, self.R.shape[0] - 1)
+            iyc = np.clip(iy, 0, self.R.shape[1] - 1)
+            r = self.R[ixc, iyc] + self.dRdz * (Z - self.z1)
+            cx = self.x0 + ixc * self.P
+            cy = self.y0 + iyc * self.P
+            zin = (Z >= self.z1) & (Z < self.z2)
+            return ok & zin & (r > 0) & ((X - cx) ** 2 + (Y - cy) ** 2 < r * r)
+        raise AssertionError
+
+    def band(self, X, Y, Z, h):
+        """Cells (centres X, Y, Z, half-size h) that the shape boundary may cross."""
+        near = ((X >= self.lo[0] - h) & (X <= self.hi[0] + h) & (Y >= self.lo[1] - h)
+                & (Y <= self.hi[1] + h) & (Z >= self.lo[2] - h) & (Z <= self.hi[2] + h))
+        k = self.kind
+        if k == "box":
+            full = ((X - h >= self.lo[0]) & (X + h < self.hi[0]) & (Y - h >= self.lo[1])
+                    & (Y + h < self.hi[1]) & (Z - h >= self.lo[2]) & (Z + h < self.hi[2]))
+            return near & ~full
+        if k in ("cyl", "cone", "lattice", "polygon"):
+            zface = (np.abs(Z - self.z1) <= h) | (np.abs(Z - self.z2) <= h)
+            hd = h * np.sqrt(2.0) * 1.0000001
+            if k in ("cyl", "cone"):
+                rho = np.sqrt((X - self.c[0]) ** 2 + (Y - self.c[1]) ** 2)
+                rlo = min(self.r1, self.r2)
+                rhi = max(self.r1, self.r2)
+                side = (rho >= rlo - hd) & (rho <= rhi + hd)
+                return near & (zface | side)
+            if k == "lattice":
+                ix = np.clip(np.rint((X - self.x0) / self.P).astype(np.int64), 0, self.R.shape[0] - 1)
+                iy = np.clip(np.rint((Y - self.y0) / self.P).astype(np.int64), 0, self.R.shape[1] - 1)
+                dz = abs(self.dRdz) * h
+                r = self.R[ix, iy] + self.dRdz * (Z - self.z1)
+                rho = np.sqrt((X - (self.x0 + ix * self.P)) ** 2 + (Y - (self.y0 + iy * self.P)) ** 2)
+                side = np.abs(rho - r) <= hd + dz
+                # pillar boundaries near a lattice-cell edge: also flag cells within
+                # reach of the neighbouring pillar by testing the cell as a whole
+                edge = (np.abs(np.mod(X - self.x0 + self.P / 2, self.P) - self.P / 2) > self.P / 2 - self.rmax - hd) | \
+                       (np.abs(np.mod(Y - self.y0 + self.P / 2, self.P) - self.P / 2) > self.P / 2 - self.rmax - hd)
+                return near & (zface | side | edge)
+            # polygon: distance to any edge
+            xs, ys = self.xy[:, 0], self.xy[:, 1]
+            dmin = np.full(np.broadcast(X, Y).shape, np.inf)
+            for a in range(xs.size):
+                b = (a + 1) % xs.size
+                ex, ey = xs[b] - xs[a], ys[b] - ys[a]
+                L2 = max(ex * ex + ey * ey, 1e-300)
+                t = np.clip(((X - xs[a]) * ex + (Y - ys[a]) * ey) / L2, 0, 1)
+                dmin = np.minimum(dmin, np.hypot(X - xs[a] - t * ex, Y - ys[a] - t * ey))
+            return near & (zface | (dmin <= hd))
+        raise AssertionError
+
+
+def _fold(v, L):
+    if L is None or not np.isfinite(L):
+        return v
+    return np.mod(v + L / 2, L) - L / 2
+
+
+def epsComponents3D(x, y, z, nBg: float, shapes, NSub: int = 4, Period=None,
+                    Method: str = "directional") -> dict:
+    """eps at the 3D Yee E locations (epsComponents3D.m:1-27).
+
+    e["x"] at (x+d/2, y, z), e["y"] at (x, y+d/2, z), e["z"] at (x, y, z+d/2),
+    each numel(x) x numel(y) x numel(z).  Shapes paint in order (box, cyl,
+    cone, polygon, lattice).  "directional": harmonic mean along the
+    component's own axis, arithmetic over the other two; "kottke":
+    1/eps_cc = n_c^2 <1/eps> + (1 - n_c^2)/<eps> with n from the first moment
+    of eps.  Only cells an interface crosses are sub-sampled; Period = [Lx Ly]
+    folds x, y into [-L/2, L/2).
+    """
+    x = np.asarray(x, dtype=float).ravel()
+    y = np.asarray(y, dtype=float).ravel()
+    z = np.asarray(z, dtype=float).ravel()
+    d = x[1] - x[0]
+    h = d / 2
+    sh = [_Shape(k, p) for k, p in _shape_list(shapes)]
+    Lx = Ly = None
+    if Period is not None:
+        Lx, Ly = (float(Period[0]), float(Period[1]))
+    off = _offsets(NSub)
+    out = {}
+    for c, name in enumerate(("x", "y", "z")):
+        shift = [0.0, 0.0, 0.0]
+        shift[c] = h
+        X = (x + shift[0])[:, None, None]
+        Y = (y + shift[1])[None, :, None]
+        Z = (z + shift[2])[None, None, :]
+        Xf, Yf = _fold(X, Lx), _fold(Y, Ly)
+        shape3 = (x.size, y.size, z.size)
+        # material at the cell centres
+        e = np.full(shape3, float(nBg) ** 2)
+        band = np.zeros(shape3, dtype=bool)
+        for s in sh:
+            Xb, Yb, Zb = np.broadcast_arrays(Xf, Yf, Z)
+            e[s.inside(Xb, Yb, Zb)] = s.n ** 2
+            band |= s.band(Xb, Yb, Zb, h)
+        if NSub > 1 and band.any():
+            ii, jj, kk = np.nonzero(band)
+            cx, cy, cz = X.ravel()[ii], Y.ravel()[jj], Z.ravel()[kk]
+            m = ii.size
+            # samples s[m, a, b, c] with a along x, b along y, c along z
+            sx = cx[:, None] + off[None, :] * d
+            sy = cy[:, None] + off[None, :] * d
+            sz = cz[:, None] + off[None, :] * d
+            SX = _fold(sx[:, :, None, None], Lx)
+            SY = _fold(sy[:, None, :, None], Ly)
+            SZ = sz[:, None, None, :]
+            SXb, SYb, SZb = np.broadcast_arrays(SX, SY, SZ)
+            es = np.full(SXb.shape, float(nBg) ** 2)
+            for s in sh:
+                es[s.inside(SXb, SYb, SZb)] = s.n ** 2
+            if Method == "directional":
+                inv_along = (1.0 / es).mean(axis=1 + c)                 # harmonic along c
+                val = (1.0 / inv_along).reshape(m, -1).mean(axis=1)
+            elif Method == "kottke":
+                mean_e = es.reshape(m, -1).mean(axis=1)
+                mean_inv = (1.0 / es).reshape(m, -1).mean(axis=1)
+                grads = []
+                for ax in range(3):
+                    w = off.reshape([-1 if a == ax else 1 for a in range(3)])
+                    grads.append((es * w[None]).reshape(m, -1).sum(axis=1))
+                gn = np.sqrt(sum(g * g for g in grads))
+                nc2 = np.where(gn > 0, (grads[c] / np.where(gn > 0, gn, 1.0)) ** 2, 0.0)
+                val = 1.0 / (nc2 * mean_inv + (1.0 - nc2) / mean_e)
+            else:
+                raise ValueError('Method must be "directional" or "kottke"')
+            e[ii, jj, kk] = val
+        out[name] = e
+    return out

@@ -1,0 +1,99 @@
+"""Simulation setups shared by the tests, written after the reference's own
+FDTD tests (tests/TestFDTD2D.m, TestFDTD3D.m, TestGUISupport.m, TestCPO.m)."""
+from __future__ import annotations
+
+import numpy as np
+
+from opticrcwafdtd_b200 import epsComponents2D, epsFromBoxes, slabModes
+
+
+def slab_sim(dx=0.01, extra=None):
+    """TestFDTD2D.slabRun (tests/TestFDTD2D.m:11-32): plane wave, periodic z,
+    0.5 um n = 2 slab; returns (sim, eps_empty, eps_slab)."""
+    x = np.round(np.arange(0, 6 + dx / 2, dx), 12)
+    z = np.arange(4) * dx
+    lam = np.linspace(1.2, 1.8, 7)
+    ixOf = lambda xx: int(round(xx / dx)) + 1
+    s = dict(x=x, z=z, npml=[round(0.2 / dx), 0], periodicZ=True, lambdas=lam,
+             monitors=[ixOf(0.6), ixOf(5)])
+    s["source"] = dict(ix=ixOf(1), profile=np.ones(4), neff=1, lambda0=1.5, bw=0.3)
+    if extra:
+        s.update(extra)
+    e0 = np.ones((x.size, z.size))
+    e1 = epsFromBoxes(x, z, 1, [3.0, 3.5, -np.inf, np.inf, 2.0])
+    return s, e0, e1
+
+
+def slab_rt(run, dx=0.01, extra=None):
+    s, e0, e1 = slab_sim(dx, extra)
+    s["eps"] = e0
+    o0 = run(s)
+    s["eps"] = e1
+    o1 = run(s)
+    R = -o1["flux"][0] / o0["flux"][1]
+    T = o1["flux"][1] / o0["flux"][1]
+    Rempty = np.abs(o0["flux"][0] / o0["flux"][1])
+    return R, T, Rempty
+
+
+def waveguide_sim(lambdas=None):
+    """TestFDTD2D.waveguideRun (tests/TestFDTD2D.m:38-48): Si slab in SiO2, TE0 source."""
+    dx = 0.02
+    x = np.round(np.arange(0, 8 + dx / 2, dx), 12)
+    z = np.arange(-1.5, 1.5 + dx / 2, dx) + dx / 2
+    epsw = epsFromBoxes(x, z, 1.444, [-np.inf, np.inf, -0.11, 0.11, 3.476])
+    m = slabModes(z, np.sqrt(epsw[0, :]), 1.55, "TE")
+    sim = dict(x=x, z=z, eps=epsw, npml=[15, 15],
+               lambdas=np.linspace(1.5, 1.6, 5) if lambdas is None else lambdas, monitors=[51, 151, 301])
+    sim["source"] = dict(ix=101, profile=m["field"][:, 0], neff=m["neff"][0], lambda0=1.55, bw=0.1)
+    return sim, m
+
+
+def waveguide_tm_sim():
+    """TestFDTD2D.tmGuidedModeMatchesDiscreteDispersion (tests/TestFDTD2D.m:115-124)."""
+    dx = 0.02
+    x = np.round(np.arange(0, 8 + dx / 2, dx), 12)
+    z = np.arange(-1.5, 1.5 + dx / 2, dx) + dx / 2
+    e = epsComponents2D(x, z, 1.444, [-np.inf, np.inf, -0.11, 0.11, 3.476])
+    m = slabModes(z, np.sqrt(e["z"][0, :]), 1.55, "TM", EpsHalf=e["x"][0, :])
+    sim = dict(pol="TM", x=x, z=z, epsX=e["x"], epsZ=e["z"], npml=[15, 15], lambdas=[1.55],
+               monitors=[51, 151, 301])
+    sim["source"] = dict(ix=101, profile=m["field"][:, 0], neff=m["neff"][0], lambda0=1.55, bw=0.1)
+    return sim, m, e
+
+
+def progress_sim():
+    """TestGUISupport.fdtdReportsProgressAndCanBeCancelled (tests/TestGUISupport.m:27-33)."""
+    dx = 0.02
+    x = np.round(np.arange(0, 4 + dx / 2, dx), 12)
+    z = np.arange(4) * dx
+    s = dict(x=x, z=z, npml=[15, 0], periodicZ=True, lambdas=[1.5], monitors=[30, 170],
+             eps=np.ones((x.size, 4)))
+    s["source"] = dict(ix=40, profile=np.ones(4), neff=1, lambda0=1.5, bw=0.3)
+    return s
+
+
+def mixed_te_sim(nx=150, nz=90, steps=400, precision="double", seed=0, pol="TE", periodic=False):
+    """Small random-structure run touching every code path: CPML on all sides
+    (or periodic z), TF/SF mode-like source, x and z monitors, many materials."""
+    rng = np.random.default_rng(seed)
+    dx = 0.02
+    x = np.arange(nx) * dx
+    z = np.arange(nz) * dx
+    boxes = []
+    for _ in range(12):
+        x1 = rng.uniform(1.0, nx * dx - 0.6)
+        z1 = rng.uniform(0.1, nz * dx - 0.3)
+        boxes.append([x1, x1 + rng.uniform(0.05, 0.5), z1, z1 + rng.uniform(0.05, 0.4), rng.uniform(1.3, 3.5)])
+    e = epsComponents2D(x, z, 1.444, boxes, PeriodicZ=periodic)
+    prof = np.exp(-((z - z.mean()) / (0.2 * nz * dx)) ** 2)
+    sim = dict(pol=pol, x=x, z=z, npml=[12, 0 if periodic else 10], periodicZ=periodic,
+               lambdas=np.linspace(1.45, 1.65, 7), monitors=[20, nx - 25, nx // 2],
+               monitorsZ=[15, nz - 14] if not periodic else [5], shutoff=0, maxTime=steps * 0.99 / np.sqrt(2) * dx,
+               precision=precision)
+    if pol == "TE":
+        sim["eps"] = e["y"]
+    else:
+        sim["epsX"], sim["epsZ"] = e["x"], e["z"]
+    sim["source"] = dict(ix=30, profile=prof, neff=1.8, lambda0=1.55, bw=0.25)
+    return sim

@@ -1,0 +1,71 @@
+"""The C ABI library: loads without a GPU, exports exactly what include/orf_fdtd.h
+declares, and rejects malformed sims on the host (no device needed)."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from opticrcwafdtd_b200 import _abi, _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_functions():
+    src = open(os.path.join(ROOT, "include", "orf_fdtd.h")).read()
+    return sorted(set(re.findall(r"^ORF_API\s+[\w\s\*]+?\b(orf_\w+)\(", src, re.M)))
+
+
+def test_library_exports_every_header_symbol():
+    lib = _lib.load()
+    names = header_functions()
+    assert len(names) >= 30
+    for n in names:
+        assert hasattr(lib, n), n
+    assert set(names) == set(_lib.exported_names())
+    assert lib.orf_abi_version() == 1
+
+
+def _sim(**kw):
+    s = dict(x=np.arange(40) * 0.02, z=np.arange(20) * 0.02, eps=np.ones((40, 20)), npml=[5, 5],
+             source=dict(ix=10, profile=np.ones(20), neff=1, lambda0=1.5), lambdas=[1.5], monitors=[8, 30])
+    s.update(kw)
+    return s
+
+
+@pytest.mark.parametrize("bad,frag", [
+    (dict(source=dict(ix=3, profile=np.ones(20), neff=1, lambda0=1.5)), "inside the CPML"),
+    (dict(monitors=[0]), "outside"),
+    (dict(monitors=[41]), "outside"),
+    (dict(eps=-np.ones((40, 20))), "positive"),
+    (dict(courant=0.9), "stability"),
+    (dict(npml=[25, 5]), "does not fit"),
+    (dict(lambdas=[-1.0]), "positive"),
+])
+def test_host_validation_rejects_bad_sims(bad, frag):
+    lib = _lib.load()
+    m = _abi.marshal_sim2d(_sim(**bad))
+    o, _ = _abi.alloc_out2d(m)
+    st = lib.orf_fdtd2d_run(C.byref(m.struct), C.byref(o), _abi.PROGRESS_FN(0), None)
+    assert st == 1, _lib.last_error()
+    assert frag in _lib.last_error()
+
+
+def test_marshal_rejects_wrong_shapes():
+    with pytest.raises(_abi.OrfError) as e:
+        _abi.marshal_sim2d(_sim(eps=np.ones((39, 20))))
+    assert e.value.identifier == "orf:invalidInput"
+    with pytest.raises(_abi.OrfError):
+        _abi.marshal_sim2d(_sim(pol="XX"))
+    with pytest.raises(_abi.OrfError):
+        _abi.marshal_sim2d(_sim(z=np.array([0, 0.02, 0.05])))
+
+
+def test_no_device_fails_loudly_without_fallback():
+    import opticrcwafdtd_b200 as orf
+    if orf.device_count() > 0:
+        pytest.skip("a GPU is present")
+    with pytest.raises(_abi.OrfError) as e:
+        orf.fdtd2DTE(_sim())
+    assert e.value.identifier == "orf:noDevice"

@@ -1,0 +1,186 @@
+"""2D parity of the CUDA engine against the CPU oracle, through the C ABI.
+
+Bars: FP64 fields <= 1e-10 relative L2, monitored flux
+<= 1e-9 absolute after normalisation; FP32 + Kahan form within the
+reference's single-vs-double tolerance (1e-4, tests/TestFDTD2D.m:68-74).
+Physics tests of the reference are repeated on the GPU path at the
+reference's tolerances."""
+import numpy as np
+import pytest
+
+import oracle
+import opticrcwafdtd_b200 as orf
+from opticrcwafdtd_b200 import Context, Job
+from tests import cases
+
+pytestmark = pytest.mark.gpu
+
+FIELD_TOL = 1e-10
+FLUX_TOL = 1e-9
+
+
+def rel_l2(a, b):
+    n = np.linalg.norm(b.ravel())
+    return np.linalg.norm((a - b).ravel()) / (n if n > 0 else 1.0)
+
+
+def gpu_run(sim, tsteps=0, variant=0, graph=True):
+    ctx = Context(0)
+    ctx.set_tuning(tsteps=tsteps, variant=variant, use_graph=graph)
+    job = Job(sim, ctx)
+    job.advance(10 ** 9)
+    f = job.fields()
+    out = job.finish()
+    job.close()
+    ctx.close()
+    out["fields"] = f
+    return out
+
+
+def compare(out, ref, field_tol=FIELD_TOL, flux_tol=FLUX_TOL):
+    for a, b, name in zip(out["fields"], ref["fields"], "PAB"):
+        assert rel_l2(a, b) <= field_tol, (name, rel_l2(a, b))
+    scale = max(np.max(np.abs(ref["flux"])), 1e-300)
+    assert np.max(np.abs(out["flux"] - ref["flux"])) / scale <= flux_tol
+    if ref["fluxZ"].size:
+        sz = max(np.max(np.abs(ref["fluxZ"])), 1e-300)
+        assert np.max(np.abs(out["fluxZ"] - ref["fluxZ"])) / sz <= flux_tol
+    for k in ("P", "B", "PZ", "AZ"):
+        if ref[k].size:
+            s = max(np.max(np.abs(ref[k])), 1e-300)
+            assert np.max(np.abs(out[k] - ref[k])) / s <= flux_tol, k
+    assert out["steps"] == ref["steps"]
+
+
+@pytest.mark.parametrize("pol,periodic", [("TE", False), ("TM", False), ("TE", True), ("TM", True)])
+def test_fp64_parity_mixed(pol, periodic):
+    sim = cases.mixed_te_sim(pol=pol, periodic=periodic, steps=420)
+    ref = oracle.fdtd2D(sim, fields=True)
+    out = gpu_run(sim)
+    compare(out, ref)
+
+
+@pytest.mark.parametrize("tsteps", [1, 2, 5, 8])
+@pytest.mark.parametrize("variant", [1, 2])
+def test_temporal_block_depth_and_variant_invariance(tsteps, variant):
+    sim = cases.mixed_te_sim(steps=333, seed=5)
+    ref = oracle.fdtd2D(sim, fields=True)
+    out = gpu_run(sim, tsteps=tsteps, variant=variant)
+    compare(out, ref)
+
+
+def test_graph_and_direct_launch_agree_bitwise():
+    sim = cases.mixed_te_sim(steps=1000, seed=2)
+    a = gpu_run(sim, graph=True)
+    b = gpu_run(sim, graph=False)
+    for x, y in zip(a["fields"], b["fields"]):
+        assert np.array_equal(x, y)
+    assert np.array_equal(a["flux"], b["flux"])
+
+
+def test_many_materials_uses_uint16_index():
+    sim = cases.mixed_te_sim(steps=200, seed=9)
+    rng = np.random.default_rng(1)
+    sim["eps"] = 1.0 + 11.0 * rng.random(sim["eps"].shape)   # > 256 distinct values
+    ref = oracle.fdtd2D(sim, fields=True)
+    compare(gpu_run(sim), ref)
+
+
+def test_fp32_kahan_form_against_fp64_oracle():
+    sim = cases.mixed_te_sim(steps=600, precision="single", seed=4)
+    out = gpu_run(sim)
+    sim64 = dict(sim, precision="double")
+    ref = oracle.fdtd2D(sim64, fields=True)
+    scale = np.max(np.abs(ref["flux"]))
+    assert np.max(np.abs(out["flux"] - ref["flux"])) / scale < 1e-4
+    for a, b in zip(out["fields"], ref["fields"]):
+        assert rel_l2(a, b) < 1e-4
+
+
+def test_slab_matches_tmm_on_gpu():
+    # tests/TestFDTD2D.m:52-58, 136-140 on the GPU path
+    R, T, Re = cases.slab_rt(orf.fdtd2DTE, 0.01)
+    tm = oracle.tmm(np.linspace(1.2, 1.8, 7), [1, 2, 1], [0.5], 0, "s")
+    assert np.max(np.abs(R - tm["R"].ravel())) < 3e-3
+    assert np.max(np.abs(R + T - 1)) < 2e-5
+    assert np.max(Re) < 1e-8
+    # gpuMatchesCpu (tests/TestFDTD2D.m:76-84): GPU double vs CPU double 1e-10
+    Ro, To, _ = cases.slab_rt(oracle.fdtd2DTE, 0.01)
+    assert np.max(np.abs(R - Ro)) < 1e-10 and np.max(np.abs(T - To)) < 1e-10
+    R3, _, _ = cases.slab_rt(orf.fdtd2DTE, 0.01, {"precision": "single"})
+    assert np.max(np.abs(R3 - Ro)) < 1e-4
+
+
+def test_mode_source_unidirectional_on_gpu():
+    # tests/TestFDTD2D.m:142-147
+    sim, _ = cases.waveguide_sim()
+    o = orf.fdtd2DTE(sim)
+    back = -o["flux"][0] / o["flux"][1]
+    assert np.max(np.abs(back)) < 1e-4
+    assert np.max(np.abs(o["flux"][2] / o["flux"][1] - 1)) < 1e-4
+    ref = oracle.fdtd2DTE(sim)
+    assert o["steps"] == ref["steps"]
+    assert np.max(np.abs(o["flux"] - ref["flux"])) / np.max(np.abs(ref["flux"])) < FLUX_TOL
+
+
+def test_tm_guided_mode_on_gpu():
+    sim, _, _ = cases.waveguide_tm_sim()
+    o = orf.fdtd2D(sim)
+    assert -o["flux"][0, 0] / o["flux"][1, 0] < 1e-6
+    assert abs(o["flux"][2, 0] / o["flux"][1, 0] - 1) < 1e-5
+    ref = oracle.fdtd2D(sim)
+    assert np.max(np.abs(o["Hy"] - ref["Hy"])) / np.max(np.abs(ref["Hy"])) < FLUX_TOL
+
+
+def test_progress_and_cancel_on_gpu():
+    # tests/TestGUISupport.m:27-45
+    s = cases.progress_sim()
+    fr = []
+    s["progress"] = lambda f, msg: fr.append(f)
+    o = orf.fdtd2DTE(s)
+    assert o["converged"]
+    assert len(fr) > 3 and all(0 <= f <= 1 for f in fr) and fr[-1] > 0.9
+    ref = oracle.fdtd2DTE(dict(s, progress=None))
+    assert o["steps"] == ref["steps"]
+
+    class Cancelled(Exception):
+        identifier = "orf:cancelled"
+
+    def cancel_after(f, msg):
+        if f > 0.2:
+            raise Cancelled("stop")
+
+    s["progress"] = cancel_after
+    with pytest.raises(Cancelled):
+        orf.fdtd2DTE(s)
+    # the context stays usable after a cancel
+    s["progress"] = None
+    assert orf.fdtd2DTE(s)["converged"]
+
+
+def test_not_converged_warning():
+    s = cases.progress_sim()
+    s["maxTime"] = 2.0
+    with pytest.warns(orf.NotConvergedWarning):
+        o = orf.fdtd2DTE(s)
+    assert not o["converged"]
+
+
+def test_job_reset_is_deterministic():
+    sim = cases.mixed_te_sim(steps=300, seed=7)
+    ctx = Context(0)
+    job = Job(sim, ctx)
+    job.advance(300)
+    f1 = job.fields()
+    o1 = job.finish()
+    job.reset()
+    job.advance(120)
+    assert job.steps == 150            # whole chunks of 50 steps
+    job.advance(300)
+    f2 = job.fields()
+    o2 = job.finish()
+    for a, b in zip(f1, f2):
+        assert np.array_equal(a, b)
+    assert np.array_equal(o1["flux"], o2["flux"])
+    job.close()
+    ctx.close()

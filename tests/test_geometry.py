@@ -1,0 +1,81 @@
+"""Host-side geometry and mode helpers (product code) against the reference's
+open algorithms and known answers."""
+import numpy as np
+
+import oracle
+from opticrcwafdtd_b200 import epsComponents2D, epsComponents3D, epsFromBoxes, slabModes
+
+
+def test_eps_from_boxes_matches_literal_restatement():
+    # toolbox/+orf/epsFromBoxes.m:16-30 restated literally in oracle/geometry_ref.py
+    rng = np.random.default_rng(3)
+    x = np.arange(60) * 0.03 - 0.2
+    z = np.arange(45) * 0.03 + 0.1
+    boxes = []
+    for _ in range(8):
+        a, b = sorted(rng.uniform(-0.3, 1.9, 2))
+        c, d = sorted(rng.uniform(0.0, 1.5, 2))
+        boxes.append([a, b, c, d, rng.uniform(1, 3.5)])
+    boxes.append([0.4, np.inf, -np.inf, 0.5, 2.2])
+    for nsub in (1, 3, 4):
+        assert np.array_equal(epsFromBoxes(x, z, 1.3, boxes, nsub),
+                              oracle.epsFromBoxes_ref(x, z, 1.3, boxes, nsub)) or \
+            np.max(np.abs(epsFromBoxes(x, z, 1.3, boxes, nsub) - oracle.epsFromBoxes_ref(x, z, 1.3, boxes, nsub))) < 1e-13
+
+
+def test_directional_eps_averaging_known_answers():
+    # tests/TestFDTD2D.m:86-97
+    x = np.round(np.arange(0, 2.0001, 0.1), 12)
+    z = np.round(np.arange(0, 1.0001, 0.1), 12)
+    e = epsComponents2D(x, z, 1, [1.0, np.inf, -np.inf, np.inf, 2])
+    i = int(np.nonzero(np.abs(x - 1.0) < 1e-12)[0][0])
+    assert abs(e["y"][i, 4] - 2.5) < 1e-12
+    assert abs(e["x"][i, 4] - 1.6) < 1e-12
+    assert abs(e["z"][i, 4] - 4) < 1e-12
+    assert abs(e["z"][i - 1, 4] - 1) < 1e-12
+
+
+def test_eps_components_shapes_and_periodic():
+    x = np.arange(20) * 0.05
+    z = (np.arange(16) + 0.5) * 0.05 - 0.4
+    e = epsComponents2D(x, z, 1, [0.3, 0.7, -0.1, 0.1, 2], PeriodicZ=True)
+    assert e["y"].shape == (20, 16) and e["x"].shape == (20, 16) and e["z"].shape == (19, 16)
+    e2 = epsComponents2D(x, z, 1, [0.3, 0.7, -0.1, 0.1, 2])
+    assert e2["x"].shape == (20, 15)
+    # a box straddling the periodic seam paints both ends
+    e3 = epsComponents2D(x, z, 1, [0.3, 0.7, 0.35, 0.45, 2], PeriodicZ=True)
+    assert e3["y"][8, 0] > 1 and e3["y"][8, -1] > 1
+
+
+def test_eps_components_3d_box_directional():
+    d = 0.1
+    x = np.arange(12) * d
+    e = epsComponents3D(x, x, x, 1, [["box", [0.5, np.inf, -np.inf, np.inf, -np.inf, np.inf, 2]]])
+    # the face x = 0.5 cuts the Ex cell at x_i+1/2 = 0.45 + ... check the known 1D means
+    i = 4   # Ey cell centred at x = 0.4 spans [0.35, 0.45): outside
+    assert abs(e["y"][i, 3, 3] - 1) < 1e-12
+    i = 5   # Ey cell at x = 0.5 spans [0.45, 0.55): half inside -> arithmetic 2.5
+    assert abs(e["y"][i, 3, 3] - 2.5) < 1e-12
+    i = 4   # Ex cell at x = 0.45 spans [0.4, 0.5): outside
+    assert abs(e["x"][i, 3, 3] - 1) < 1e-12
+    # Ex at x = 0.5 + 0.05 -> inside
+    assert abs(e["x"][5, 3, 3] - 4) < 1e-12
+
+
+def test_slab_modes_te_tm():
+    dx = 0.02
+    z = np.arange(-1.5, 1.5 + dx / 2, dx) + dx / 2
+    epsw = epsFromBoxes(np.arange(3) * dx, z, 1.444, [-np.inf, np.inf, -0.11, 0.11, 3.476])
+    m = slabModes(z, np.sqrt(epsw[0, :]), 1.55, "TE", 2)
+    assert m["field"].shape == (z.size, 2)
+    assert 2.8 < m["neff"][0] < 2.9 and m["neff"][0] > m["neff"][1]
+    assert abs(np.max(np.abs(m["field"][:, 0])) - 1) < 1e-12 and np.max(m["field"][:, 0]) == 1.0
+    # compare with a dense eig of the same matrix (slabModes.m:29-30, 44-47)
+    N = z.size
+    k0 = 2 * np.pi / 1.55
+    A = (np.diag(np.full(N - 1, 1 / dx ** 2), -1) + np.diag(np.full(N - 1, 1 / dx ** 2), 1)
+         + np.diag(-2 / dx ** 2 + k0 ** 2 * epsw[0, :]))
+    w = np.sort(np.linalg.eigvals(A).real)[::-1]
+    assert abs(np.sqrt(w[0]) / k0 - m["neff"][0]) < 1e-12
+    mt = slabModes(z, np.sqrt(epsw[0, :]), 1.55, "TM")
+    assert 2.0 < mt["neff"][0] < m["neff"][0]
