@@ -156,13 +156,22 @@ typedef struct orf_tuning {
     int32_t _pad;
 } orf_tuning;
 
-/* Per-kernel timing, collected when orf_ctx_set_timing(ctx, 1). */
+/* Per-kernel timing, collected when orf_ctx_set_timing(ctx, 1): CUDA events
+ * around every launch on the context's stream.  "interior" is the pipelined
+ * step kernel of tiles away from the CPML, "frame" the step kernel of the
+ * CPML/boundary tiles (2D), "flush" the DFT flush + check kernels. */
 typedef struct orf_kernel_stats {
-    double step_ms;            /* summed CUDA-event time of the step kernels        */
-    int64_t step_launches;
-    int64_t cell_updates;      /* cells x steps advanced by those launches          */
-    double flush_ms;           /* DFT flush + check kernels                         */
+    double interior_ms;
+    int64_t interior_launches;
+    int64_t interior_cell_updates;   /* cells x time steps those launches advanced */
+    double frame_ms;
+    int64_t frame_launches;
+    int64_t frame_cell_updates;
+    double flush_ms;
     int64_t flush_launches;
+    int64_t cell_updates;            /* all cells x time steps advanced           */
+    int64_t h2d_bytes;               /* host->device bytes copied by run/create   */
+    int64_t d2h_bytes;               /* device->host bytes copied by finish       */
 } orf_kernel_stats;
 
 ORF_API int32_t     orf_abi_version(void);

@@ -95,9 +95,11 @@ class OrfTuning(C.Structure):
 
 
 class OrfKernelStats(C.Structure):
-    _fields_ = [("step_ms", C.c_double), ("step_launches", C.c_int64),
-                ("cell_updates", C.c_int64), ("flush_ms", C.c_double),
-                ("flush_launches", C.c_int64)]
+    _fields_ = [("interior_ms", C.c_double), ("interior_launches", C.c_int64),
+                ("interior_cell_updates", C.c_int64),
+                ("frame_ms", C.c_double), ("frame_launches", C.c_int64), ("frame_cell_updates", C.c_int64),
+                ("flush_ms", C.c_double), ("flush_launches", C.c_int64),
+                ("cell_updates", C.c_int64), ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64)]
 
 
 class OrfServeCfg(C.Structure):

@@ -13,6 +13,22 @@
 
 namespace orf {
 
+// CUDA events around individual launches (orf_ctx_set_timing).
+struct KernelTimer {
+    struct Rec {
+        int kind;                 // 0 interior, 1 frame, 2 flush/check
+        int64_t cells;            // cell updates of the launch
+        cudaEvent_t a, b;
+    };
+    std::vector<cudaEvent_t> pool;
+    std::vector<Rec> recs;
+    size_t used = 0;
+    ~KernelTimer();
+    int begin(cudaStream_t s, cudaEvent_t* a);
+    int end(cudaStream_t s, int kind, int64_t cells, cudaEvent_t a);
+    void collect(orf_kernel_stats* st);
+};
+
 struct ChunkEngine {
     orf_ctx* ctx = nullptr;
     bool fp64 = false;
@@ -20,7 +36,8 @@ struct ChunkEngine {
     int par = 0;                      // field buffer holding the current state
     // launches the step kernels of all instances for steps [off, off+nsub) of
     // the chunk, reading buffer par; want_energy on the chunk's last launch
-    std::function<cudaError_t(int off, int nsub, int par, int want_energy, cudaStream_t)> step;
+    // timer (may be null) records per-kernel events in timing mode
+    std::function<cudaError_t(int off, int nsub, int par, int want_energy, cudaStream_t, KernelTimer* timer)> step;
     DftStream* d_streams = nullptr;
     FlushItem* d_items = nullptr;
     int nitems = 0;
@@ -32,9 +49,7 @@ struct ChunkEngine {
     int gchunks = 0;
     int gpar = -1;
 
-    // timing (orf_ctx_set_timing): events around the step launches of a chunk
-    std::vector<cudaEvent_t> evpool;
-    size_t evused = 0;
+    KernelTimer timer;
 
     ~ChunkEngine();
     int launches_per_chunk() const { return (kChunk + T - 1) / T; }
@@ -43,7 +58,7 @@ struct ChunkEngine {
     int enqueue(int nchunks, cudaStream_t s);
     void drop_graph();
     // fold the recorded events into ctx->stats (after a sync)
-    void collect_timing(int64_t cell_updates);
+    void collect_timing();
 };
 
 // Host-side progress loop over one job's status ring.

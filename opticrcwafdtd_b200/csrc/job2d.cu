@@ -165,6 +165,11 @@ int Job2D<R>::create(const orf_sim2d* s) {
 
     // ---- tiles
     ORF_TRY(pick_tiling(npx, npz));
+    int fast_wx = 1;
+    {
+        Variant2D fv;
+        if (fast2d_info(fvariant, sizeof(R) == 8, &fv)) fast_wx = fv.wx;
+    }
 
     // ---- DFT streams: x monitors (P, B lines), z monitors (P, A lines)
     const int sstride = 2 * nz * nM + 2 * nx * nMZ;
@@ -228,6 +233,7 @@ int Job2D<R>::create(const orf_sim2d* s) {
     ar.add(&d_st, 1);
     ar.add(&d_states, 1);
     ar.add(&d_tint, tiles_int.size() + 1);
+    ar.add(&d_ftiles, ftiles_host.size() + 1);
     ar.add(&d_tpml, tiles_pml.size() + 1);
     ar.add(&d_streams, nstreams + 1);
     ar.add(&d_items, nitems + 1);
@@ -259,6 +265,7 @@ int Job2D<R>::create(const orf_sim2d* s) {
     auto up = [&](void* d, const void* hsrc, size_t bytes) -> int {
         if (bytes == 0) return ORF_OK;
         ORF_CUDA(cudaMemcpyAsync(d, hsrc, bytes, cudaMemcpyHostToDevice, st));
+        ctx->stats.h2d_bytes += (int64_t)bytes;
         return ORF_OK;
     };
     ORF_TRY(up(d_ix0, ib0.data(), ib0.size()));
@@ -293,6 +300,24 @@ int Job2D<R>::create(const orf_sim2d* s) {
     h.st = d_st;
     ORF_TRY(up(d_inst, &h, sizeof(h)));
     ORF_TRY(up(d_tint, tiles_int.data(), tiles_int.size() * sizeof(Tile2D)));
+    for (auto& t : ftiles_host) {
+        for (int b = 0; b < 2; ++b) {
+            t.f[b][0] = h.P[b];
+            t.f[b][1] = h.A[b];
+            t.f[b][2] = h.B[b];
+        }
+        t.idx0 = d_ix0;
+        t.idx1 = te ? d_ix0 : d_ix1;
+        t.st = d_st;
+        t.inst = d_inst;
+        t.flags = 0;
+        if ((sx - 1 >= t.li0 && sx - 1 < t.li0 + 32 * fast_wx) || (sx >= t.li0 && sx < t.li0 + 32 * fast_wx)) t.flags |= 1;
+        for (int m = 0; m < nM; ++m)
+            if (s->monitors[m] >= t.oi0 && s->monitors[m] < t.oi0 + t.ow) t.flags |= 2;
+        for (int m = 0; m < nMZ; ++m)
+            if (s->monitors_z[m] >= t.ok0 && s->monitors_z[m] < t.ok0 + t.oh) t.flags |= 4;
+    }
+    ORF_TRY(up(d_ftiles, ftiles_host.data(), ftiles_host.size() * sizeof(FastTile2D)));
     ORF_TRY(up(d_tpml, tiles_pml.data(), tiles_pml.size() * sizeof(Tile2D)));
     std::vector<DftStream> hs(nstreams);
     size_t aoff = 0;
@@ -325,16 +350,28 @@ int Job2D<R>::create(const orf_sim2d* s) {
     eng.nitems = nitems;
     eng.d_states = d_states;
     eng.nstates = 1;
-    eng.step = [this](int off, int nsub, int par, int we, cudaStream_t stream) -> cudaError_t {
+    int64_t interior_cells = 0;
+    for (auto& t : ftiles_host) interior_cells += (int64_t)t.ow * t.oh;
+    eng.step = [this, interior_cells](int off, int nsub, int par, int we, cudaStream_t stream,
+                                      KernelTimer* tm) -> cudaError_t {
         const bool f64 = sizeof(R) == 8;
         cudaError_t e = cudaSuccess;
-        if (!tiles_int.empty())
-            e = launch_step2d(f64, te, idx16, false, variant, d_inst, d_tint, (int)tiles_int.size(), T, off,
-                              nsub, par, we, grid_int, stream);
-        if (e != cudaSuccess) return e;
-        if (!tiles_pml.empty())
+        cudaEvent_t a = nullptr;
+        if (!ftiles_host.empty()) {
+            if (tm && tm->begin(stream, &a) != ORF_OK) return cudaErrorUnknown;
+            e = launch_fast2d(f64, te, idx16, fvariant, d_ftiles, (int)ftiles_host.size(), off, nsub, par, we,
+                              grid_fast, stream);
+            if (e != cudaSuccess) return e;
+            if (tm && tm->end(stream, 0, interior_cells * nsub, a) != ORF_OK) return cudaErrorUnknown;
+        }
+        if (!tiles_pml.empty()) {
+            if (tm && tm->begin(stream, &a) != ORF_OK) return cudaErrorUnknown;
             e = launch_step2d(f64, te, idx16, true, variant, d_inst, d_tpml, (int)tiles_pml.size(), T, off,
                               nsub, par, we, grid_pml, stream);
+            if (e != cudaSuccess) return e;
+            if (tm && tm->end(stream, 1, ((int64_t)nx * nz - interior_cells) * nsub, a) != ORF_OK)
+                return cudaErrorUnknown;
+        }
         return e;
     };
     ORF_CUDA(cudaStreamSynchronize(st));
@@ -344,44 +381,82 @@ int Job2D<R>::create(const orf_sim2d* s) {
 template <class R>
 int Job2D<R>::pick_tiling(int npx, int npz) {
     const bool f64 = sizeof(R) == 8;
-    variant = ctx->tuning.variant > 0 ? ctx->tuning.variant : 1;
-    Variant2D v;
-    if (!variant2d_info(variant, f64, &v)) {
-        set_error("unknown 2D kernel variant %d", variant);
+    // interior tiles: pipelined kernel; CPML / boundary frame: masked kernel
+    fvariant = ctx->tuning.variant > 0 ? ctx->tuning.variant : 1;
+    Variant2D fv, bv;
+    if (!fast2d_info(fvariant, f64, &fv)) {
+        set_error("unknown 2D kernel variant %d", fvariant);
         return ORF_EINVAL;
     }
-    const int tmax = std::min(kMaxSub, (std::min(v.lx(), v.lz()) - 1) / 2);
-    T = ctx->tuning.tsteps > 0 ? ctx->tuning.tsteps : (f64 ? 4 : 6);
+    variant = 2;
+    variant2d_info(variant, f64, &bv);
+    const int tmax = std::min({kMaxSub, (bv.lz() - 1) / 2, (bv.lx() - 1) / 2, (fv.lz() - 1) / 2, (fv.lx() - 4) / 2});
+    T = ctx->tuning.tsteps > 0 ? ctx->tuning.tsteps : (f64 ? 6 : 6);
     if (T > tmax) T = tmax;
     if (T < 1) T = 1;
-    const int OX = v.lx() - 2 * T, OZ = v.lz() - 2 * T;
-    tiles_int.clear();
+
+    // An output cell's T-step dependency cone needs correct (CPML-free,
+    // unmasked) updates of P within distance T-1 and of A (B) within distance
+    // T on the low side: A at rows >= npz, B at columns >= npx, P at rows and
+    // columns >= 1.  On the high side P, A and B within distance T-1 must lie
+    // below the upper slabs (A starts at nz-1-npz, B at nx-1-npx) and exist.
+    int ax = npx + T, bx = nx - npx - T;
+    int az = per ? 0 : npz + T, bz = per ? nz : nz - npz - T;
+    if (bx - ax < 8 || bz - az < 4) { ax = bx = 0; az = bz = 0; }   // everything is frame
+    ftiles_host.clear();
     tiles_pml.clear();
-    for (int ok0 = 0; ok0 < nz; ok0 += OZ) {
-        for (int oi0 = 0; oi0 < nx; oi0 += OX) {
-            Tile2D t;
-            t.inst = 0;
+    tiles_int.clear();
+    const int FX = fv.lx(), FZ = fv.lz();
+    for (int ok0 = az; ok0 < bz;) {
+        const int oh = std::min(FZ - 2 * T, bz - ok0);
+        for (int oi0 = ax; oi0 < bx;) {
+            const int li0 = ((oi0 - T) / 4) * 4;   // oi0 - T >= cl - 1 >= 0
+            const int ow = std::min(li0 + FX - T - oi0, bx - oi0);
+            FastTile2D t{};
+            t.pitch = pitch;
+            t.nz = nz;
+            t.periodic = per ? 1 : 0;
+            t.li0 = li0;
+            t.lk0 = ok0 - T;
             t.oi0 = oi0;
             t.ok0 = ok0;
-            t.ow = (short)std::min(OX, nx - oi0);
-            t.oh = (short)std::min(OZ, nz - ok0);
-            // loaded region [oi0-T, oi0-T+LX) x [ok0-T, ok0-T+LZ); does it reach a CPML cell?
-            const int li0 = oi0 - T, li1 = oi0 - T + v.lx();
-            const int lk0 = ok0 - T, lk1 = ok0 - T + v.lz();
-            bool pml = false;
-            if (npx > 0 && (li0 < npx || li1 > nx - 1 - npx)) pml = true;
-            if (npz > 0 && (lk0 < npz || lk1 > nz - 1 - npz)) pml = true;
-            (pml ? tiles_pml : tiles_int).push_back(t);
+            t.ow = ow;
+            t.oh = oh;
+            ftiles_host.push_back(t);
+            oi0 += ow;
         }
+        ok0 += oh;
     }
-    const int bps_i = step2d_blocks_per_sm(f64, te, idx16, false, variant);
+    // frame strips: bottom, top (full width), left, right (between az and bz)
+    const int OX = bv.lx() - 2 * T, OZ = bv.lz() - 2 * T;
+    auto strip = [&](int x0, int x1, int z0, int z1) {
+        for (int ok0 = z0; ok0 < z1; ok0 += OZ)
+            for (int oi0 = x0; oi0 < x1; oi0 += OX) {
+                Tile2D t;
+                t.inst = 0;
+                t.oi0 = oi0;
+                t.ok0 = ok0;
+                t.ow = (short)std::min(OX, x1 - oi0);
+                t.oh = (short)std::min(OZ, z1 - ok0);
+                tiles_pml.push_back(t);
+            }
+    };
+    if (bx > ax) {
+        strip(0, nx, 0, az);
+        strip(0, nx, bz, nz);
+        strip(0, ax, az, bz);
+        strip(bx, nx, az, bz);
+    } else {
+        strip(0, nx, 0, nz);
+    }
+    const int bps_f = ftiles_host.empty() ? 1 : fast2d_blocks_per_sm(f64, te, idx16, fvariant);
     const int bps_p = step2d_blocks_per_sm(f64, te, idx16, true, variant);
-    if (bps_i < 1 || bps_p < 1) {
-        set_error("2D kernel variant %d cannot be resident on this device (%s)", variant,
+    if (bps_f < 1 || bps_p < 1) {
+        set_error("2D kernel variant %d cannot be resident on this device (%s)", fvariant,
                   cudaGetErrorString(cudaGetLastError()));
         return ORF_ECUDA;
     }
-    grid_int = (int)std::min<size_t>(tiles_int.size(), (size_t)ctx->sm_count * bps_i);
+    grid_fast = (int)std::min<size_t>(ftiles_host.size(), (size_t)ctx->sm_count * bps_f);
     grid_pml = (int)std::min<size_t>(tiles_pml.size(), (size_t)ctx->sm_count * bps_p);
     return ORF_OK;
 }
@@ -457,7 +532,8 @@ int Job2D<R>::advance(int64_t nsteps, orf_progress_fn progress, void* user) {
     enq_steps += chunks * kChunk;
     const int64_t steps0 = pl.last_step;
     ORF_TRY(run_chunks(eng, pl, ctx, chunks, progress, user));
-    if (ctx->timing) eng.collect_timing((pl.last_step - steps0) * (int64_t)nx * nz);
+    eng.collect_timing();
+    ctx->stats.cell_updates += (pl.last_step - steps0) * (int64_t)nx * nz;
     return pl.cancelled ? ORF_ECANCELLED : ORF_OK;
 }
 
@@ -479,11 +555,13 @@ int Job2D<R>::finish2d(orf_out2d* o) {
     ORF_CUDA(launch_flux(f64, d_streams, d_pairs, npairs, nL, d_flux, st));
     std::vector<double> fl((size_t)(nM + nMZ) * nL);
     if (!fl.empty()) ORF_CUDA(cudaMemcpyAsync(fl.data(), d_flux, fl.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    ctx->stats.d2h_bytes += (int64_t)(fl.size() * sizeof(double));
     // DFT lines: stream q -> complex [l][e]
     auto fetch = [&](int q, double* dst) -> int {
         if (!dst) return ORF_OK;
         const DftStream& S = host_streams[q];
         const size_t n = (size_t)S.len * nL;
+        ctx->stats.d2h_bytes += (int64_t)(n * sizeof(double2));
         if (f64) {
             ORF_CUDA(cudaMemcpyAsync(dst, S.acc, n * sizeof(double2), cudaMemcpyDeviceToHost, st));
         } else {

@@ -22,7 +22,9 @@ struct Job2D : orf_job {
     Tile2D* d_tint = nullptr;
     Tile2D* d_tpml = nullptr;
     std::vector<Tile2D> tiles_int, tiles_pml;
-    int variant = 1, T = 1, grid_int = 0, grid_pml = 0;
+    std::vector<FastTile2D> ftiles_host;
+    FastTile2D* d_ftiles = nullptr;
+    int variant = 2, fvariant = 1, T = 1, grid_int = 0, grid_pml = 0, grid_fast = 0;
     DftStream* d_streams = nullptr;
     std::vector<DftStream> host_streams;
     FlushItem* d_items = nullptr;

@@ -122,6 +122,23 @@ struct Tile2D {
     short ow, oh;           // output extent
 };
 
+// Self-contained descriptor of an interior tile for the pipelined kernel
+// (step2d_fast.cuh): everything its prefetch needs, 128 bytes, copied into
+// shared memory with cp.async two tiles ahead.
+struct alignas(16) FastTile2D {
+    const void* f[2][3];    // P, A, B of buffer 0 and 1
+    const void* idx0;
+    const void* idx1;
+    JobState* st;
+    const void* inst;       // Inst2D<R>* (source, monitors, tables)
+    int pitch, nz, periodic;
+    int li0, lk0;           // loaded origin; li0 is a multiple of 4 cells
+    int oi0, ok0, ow, oh;   // output rectangle
+    int flags;              // 1: TF/SF plane in the loaded columns, 2: x monitor, 4: z monitor
+    int pad[2];
+};
+static_assert(sizeof(FastTile2D) == 128, "FastTile2D must stay 128 bytes");
+
 // --------------------------------------------------------------------- 3D --
 // Six components at their Yee positions (fdtd3D.m:2-5); layout [nz][ny][pitch].
 template <class R>
@@ -188,6 +205,12 @@ cudaError_t launch_step2d(bool fp64, bool te, bool idx16, bool pml, int variant,
                           const Tile2D* tiles, int ntiles, int halo, int launch_off, int nsub,
                           int par, int want_energy, int grid, cudaStream_t s);
 size_t step2d_smem(bool fp64, bool te, bool pml, int variant);
+
+// Pipelined interior kernel (step2d_fast.cuh).
+bool fast2d_info(int id, bool fp64, Variant2D* v);
+cudaError_t launch_fast2d(bool fp64, bool te, bool idx16, int variant, const FastTile2D* tiles, int ntiles,
+                          int launch_off, int nsub, int par, int want_energy, int grid, cudaStream_t s);
+int fast2d_blocks_per_sm(bool fp64, bool te, bool idx16, int variant);
 int step2d_blocks_per_sm(bool fp64, bool te, bool idx16, bool pml, int variant);
 
 cudaError_t launch_step3d(bool fp64, bool idx16, const void* insts, const Tile3D* tiles, int ntiles,

@@ -72,10 +72,56 @@ double progress_fraction(double t, double src_end, double ratio, double shutoff)
 }
 
 // ----------------------------------------------------------- ChunkEngine --
-ChunkEngine::~ChunkEngine() {
-    drop_graph();
-    for (auto e : evpool) cudaEventDestroy(e);
+KernelTimer::~KernelTimer() {
+    for (auto e : pool) cudaEventDestroy(e);
 }
+
+int KernelTimer::begin(cudaStream_t s, cudaEvent_t* a) {
+    if (used >= pool.size()) {
+        cudaEvent_t e;
+        ORF_CUDA(cudaEventCreate(&e));
+        pool.push_back(e);
+    }
+    *a = pool[used++];
+    ORF_CUDA(cudaEventRecord(*a, s));
+    return ORF_OK;
+}
+
+int KernelTimer::end(cudaStream_t s, int kind, int64_t cells, cudaEvent_t a) {
+    if (used >= pool.size()) {
+        cudaEvent_t e;
+        ORF_CUDA(cudaEventCreate(&e));
+        pool.push_back(e);
+    }
+    cudaEvent_t b = pool[used++];
+    ORF_CUDA(cudaEventRecord(b, s));
+    recs.push_back({kind, cells, a, b});
+    return ORF_OK;
+}
+
+void KernelTimer::collect(orf_kernel_stats* st) {
+    for (auto& r : recs) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, r.a, r.b) != cudaSuccess) continue;
+        if (r.kind == 0) {
+            st->interior_ms += ms;
+            st->interior_launches += 1;
+            st->interior_cell_updates += r.cells;
+        } else if (r.kind == 1) {
+            st->frame_ms += ms;
+            st->frame_launches += 1;
+            st->frame_cell_updates += r.cells;
+        } else {
+            st->flush_ms += ms;
+            st->flush_launches += 2;
+        }
+    }
+    cudaGetLastError();
+    recs.clear();
+    used = 0;
+}
+
+ChunkEngine::~ChunkEngine() { drop_graph(); }
 
 void ChunkEngine::drop_graph() {
     if (gexec) cudaGraphExecDestroy(gexec);
@@ -85,27 +131,18 @@ void ChunkEngine::drop_graph() {
 }
 
 int ChunkEngine::enqueue_chunk(cudaStream_t s, bool timed) {
-    if (timed) {
-        while (evpool.size() < evused + 4) {
-            cudaEvent_t e;
-            ORF_CUDA(cudaEventCreate(&e));
-            evpool.push_back(e);
-        }
-        ORF_CUDA(cudaEventRecord(evpool[evused], s));
-    }
+    KernelTimer* tm = timed ? &timer : nullptr;
     for (int off = 0; off < kChunk; off += T) {
         const int nsub = std::min(T, kChunk - off);
         const int we = (off + nsub == kChunk) ? 1 : 0;
-        ORF_CUDA(step(off, nsub, par, we, s));
+        ORF_CUDA(step(off, nsub, par, we, s, tm));
         par ^= 1;
     }
-    if (timed) ORF_CUDA(cudaEventRecord(evpool[evused + 1], s));
+    cudaEvent_t a = nullptr;
+    if (tm) ORF_TRY(tm->begin(s, &a));
     ORF_CUDA(launch_flush(fp64, d_streams, d_items, nitems, s));
     ORF_CUDA(launch_check(d_states, nstates, s));
-    if (timed) {
-        ORF_CUDA(cudaEventRecord(evpool[evused + 2], s));
-        evused += 3;
-    }
+    if (tm) ORF_TRY(tm->end(s, 2, 0, a));
     return ORF_OK;
 }
 
@@ -126,16 +163,15 @@ int ChunkEngine::enqueue(int nchunks, cudaStream_t s) {
                 int st = ORF_OK;
                 for (int c = 0; c < G && st == ORF_OK; ++c) st = enqueue_chunk(s, false);
                 cudaError_t ce = cudaStreamEndCapture(s, &g);
+                par = p0;   // capture only recorded the launches
                 if (st != ORF_OK) {
                     if (g) cudaGraphDestroy(g);
-                    par = p0;
                     return st;
                 }
                 ORF_CUDA(ce);
                 cudaError_t ie = cudaGraphInstantiate(&gexec, g, 0);
                 cudaGraphDestroy(g);
                 ORF_CUDA(ie);
-                par = p0;   // capture only recorded the launches
                 gpar = p0;
                 gchunks = G;
             }
@@ -150,22 +186,9 @@ int ChunkEngine::enqueue(int nchunks, cudaStream_t s) {
     return ORF_OK;
 }
 
-void ChunkEngine::collect_timing(int64_t cell_updates) {
+void ChunkEngine::collect_timing() {
     if (!ctx->timing) return;
-    for (size_t q = 0; q + 2 < evused + 1 && q + 2 <= evused; q += 3) {
-        float a = 0.f, b = 0.f;
-        if (cudaEventElapsedTime(&a, evpool[q], evpool[q + 1]) == cudaSuccess) {
-            ctx->stats.step_ms += a;
-            ctx->stats.step_launches += launches_per_chunk();
-        }
-        if (cudaEventElapsedTime(&b, evpool[q + 1], evpool[q + 2]) == cudaSuccess) {
-            ctx->stats.flush_ms += b;
-            ctx->stats.flush_launches += 2;
-        }
-    }
-    cudaGetLastError();
-    ctx->stats.cell_updates += cell_updates;
-    evused = 0;
+    timer.collect(&ctx->stats);
 }
 
 // ---------------------------------------------------------- ProgressLoop --

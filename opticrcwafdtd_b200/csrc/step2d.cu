@@ -57,3 +57,45 @@ int step2d_blocks_per_sm(bool fp64, bool te, bool idx16, bool pml, int variant) 
 }
 
 }  // namespace orf
+
+namespace orf {
+
+cudaError_t launch_fast2d_f32(bool te, bool idx16, int variant, const FastTile2D* tiles, int ntiles, int off,
+                              int nsub, int par, int we, int grid, cudaStream_t s);
+cudaError_t launch_fast2d_f64(bool te, bool idx16, int variant, const FastTile2D* tiles, int ntiles, int off,
+                              int nsub, int par, int we, int grid, cudaStream_t s);
+int occ_fast2d_f32(bool te, bool idx16, int variant);
+int occ_fast2d_f64(bool te, bool idx16, int variant);
+
+namespace {
+// pipelined interior kernel geometries; must match fast2d_f32.cu / fast2d_f64.cu
+constexpr VDesc kF32[] = {{1, 16, 4, 4}, {2, 8, 4, 4}};
+constexpr VDesc kF64[] = {{1, 8, 4, 4}, {2, 8, 2, 8}};
+}  // namespace
+
+bool fast2d_info(int id, bool fp64, Variant2D* v) {
+    const VDesc* tab = fp64 ? kF64 : kF32;
+    for (int q = 0; q < 2; ++q) {
+        if (tab[q].id == id) {
+            v->id = id;
+            v->ks = tab[q].ks;
+            v->wx = tab[q].wx;
+            v->wz = tab[q].wz;
+            return true;
+        }
+    }
+    return false;
+}
+
+cudaError_t launch_fast2d(bool fp64, bool te, bool idx16, int variant, const FastTile2D* tiles, int ntiles,
+                          int launch_off, int nsub, int par, int want_energy, int grid, cudaStream_t s) {
+    if (nsub < 1 || nsub > kMaxSub || ntiles <= 0) return cudaErrorInvalidValue;
+    if (fp64) return launch_fast2d_f64(te, idx16, variant, tiles, ntiles, launch_off, nsub, par, want_energy, grid, s);
+    return launch_fast2d_f32(te, idx16, variant, tiles, ntiles, launch_off, nsub, par, want_energy, grid, s);
+}
+
+int fast2d_blocks_per_sm(bool fp64, bool te, bool idx16, int variant) {
+    return fp64 ? occ_fast2d_f64(te, idx16, variant) : occ_fast2d_f32(te, idx16, variant);
+}
+
+}  // namespace orf

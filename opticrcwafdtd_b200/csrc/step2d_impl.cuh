@@ -227,7 +227,7 @@ k_step2d(const Inst2D<R>* __restrict__ insts, const Tile2D* __restrict__ tiles, 
             }
         }
         const int six = I->src_ix;
-        __syncthreads();   // sg / spz / psi ready
+        const bool has_mon = __syncthreads_or(xm >= 0 || zmask != 0) != 0;   // also: sg / spz / psi ready
 
         // ---------------------------------------------------------- steps
         for (int s = 0; s < nsub; ++s) {
@@ -281,8 +281,6 @@ k_step2d(const Inst2D<R>* __restrict__ insts, const Tile2D* __restrict__ tiles, 
             xAr[warp][lane] = A[KS - 1];
             __syncthreads();
             const R Aup = (wz > 0) ? xAr[warp - WX][lane] : R(0);
-            const R gh = (R)sg[1][s];
-            const int slot = launch_off + s;
 #pragma unroll
             for (int j = 0; j < KS; ++j) {
                 R bl = __shfl_up_sync(FULL, B[j], 1);
@@ -300,27 +298,40 @@ k_step2d(const Inst2D<R>* __restrict__ insts, const Tile2D* __restrict__ tiles, 
                     db = db * pxk + px;
                 }
                 const R cp = TE ? c0s[(KS * wz + j) * LX + cx] : C;
-                if ((mP >> j) & 1u) {
-                    P[j] += cp * (da - db);
-                    if (i == six) {   // TF/SF: the plane is total field
+                if ((mP >> j) & 1u) P[j] += cp * (da - db);
+            }
+            if (i == six) {   // TF/SF: the plane is total field
+                const R gh = (R)sg[1][s];
+#pragma unroll
+                for (int j = 0; j < KS; ++j) {
+                    if ((mP >> j) & 1u) {
                         const int kk = per ? pmod(kb + j, nz) : kb + j;
                         P[j] += ldg(I->srcP + kk) * gh;
                     }
                 }
-                if (xm >= 0 && ((own >> j) & 1u)) {
-                    const int kk = per ? pmod(kb + j, nz) : kb + j;
-                    R* smp = I->samples + (size_t)slot * I->sstride + (size_t)xm * 2 * nz;
-                    smp[kk] = P[j];
-                    smp[nz + kk] = R(0.5) * (bl + B[j]);
-                }
-                if ((zmask >> j) & 1u) {
-                    const int kk = per ? pmod(kb + j, nz) : kb + j;
-                    for (int m = 0; m < I->nmonz; ++m) {
-                        if (I->monz[m] != kk) continue;
-                        R* smp = I->samples + (size_t)slot * I->sstride + (size_t)I->nmon * 2 * nz +
-                                 (size_t)m * 2 * nx;
-                        smp[i] = P[j];
-                        smp[nx + i] = R(0.5) * (am + A[j]);
+            }
+            if (has_mon) {    // DFT monitor samples of this step (block-uniform flag)
+                const int slot = launch_off + s;
+#pragma unroll
+                for (int j = 0; j < KS; ++j) {
+                    R bl = __shfl_up_sync(FULL, B[j], 1);
+                    if (lane == 0) bl = (wx > 0) ? xBc[warp - 1][j] : R(0);
+                    if (xm >= 0 && ((own >> j) & 1u)) {
+                        const int kk = per ? pmod(kb + j, nz) : kb + j;
+                        R* smp = I->samples + (size_t)slot * I->sstride + (size_t)xm * 2 * nz;
+                        smp[kk] = P[j];
+                        smp[nz + kk] = R(0.5) * (bl + B[j]);
+                    }
+                    if ((zmask >> j) & 1u) {
+                        const R am = (j > 0) ? A[j - 1] : Aup;
+                        const int kk = per ? pmod(kb + j, nz) : kb + j;
+                        for (int m = 0; m < I->nmonz; ++m) {
+                            if (I->monz[m] != kk) continue;
+                            R* smp = I->samples + (size_t)slot * I->sstride + (size_t)I->nmon * 2 * nz +
+                                     (size_t)m * 2 * nx;
+                            smp[i] = P[j];
+                            smp[nx + i] = R(0.5) * (am + A[j]);
+                        }
                     }
                 }
             }

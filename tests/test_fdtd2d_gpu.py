@@ -184,3 +184,23 @@ def test_job_reset_is_deterministic():
     assert np.array_equal(o1["flux"], o2["flux"])
     job.close()
     ctx.close()
+
+
+@pytest.mark.parametrize("pol,periodic,tsteps,variant", [
+    ("TE", False, 6, 1), ("TM", False, 6, 1), ("TE", True, 4, 2), ("TM", False, 3, 2), ("TE", False, 1, 1),
+])
+def test_fp64_parity_many_interior_tiles(pol, periodic, tsteps, variant):
+    """Grid large enough for dozens of pipelined interior tiles plus the CPML frame."""
+    sim = cases.mixed_te_sim(nx=700, nz=330, steps=250, pol=pol, periodic=periodic, seed=11)
+    ref = oracle.fdtd2D(sim, fields=True)
+    compare(gpu_run(sim, tsteps=tsteps, variant=variant), ref)
+
+
+def test_fp32_many_tiles_against_fp64_oracle():
+    sim = cases.mixed_te_sim(nx=700, nz=330, steps=400, pol="TM", precision="single", seed=12)
+    out = gpu_run(sim, tsteps=6)
+    ref = oracle.fdtd2D(dict(sim, precision="double"), fields=True)
+    scale = np.max(np.abs(ref["flux"]))
+    assert np.max(np.abs(out["flux"] - ref["flux"])) / scale < 1e-4
+    for a, b in zip(out["fields"], ref["fields"]):
+        assert rel_l2(a, b) < 1e-4
