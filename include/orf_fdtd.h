@@ -221,6 +221,23 @@ ORF_API int32_t orf_job3d_finish(orf_job* job, orf_out3d* out);
 ORF_API int32_t orf_job_get_fields(orf_job* job, double* const* fields, int32_t nfields);
 ORF_API int32_t orf_job_destroy(orf_job* job);
 
+/* No counterpart in the reference.  orf.fdtd2D(sim) for callers that cannot
+ * allocate device memory at call time (a host with its own device memory
+ * pool, such as a MATLAB gpuArray session, a serving process with a fixed
+ * budget, or a loop that must not block on the allocator).  Runs the same
+ * kernels as orf_fdtd2d_run but calls no cudaMalloc/cudaFree and no other
+ * allocating routine.  All device state lives in one 64 MiB static
+ * __device__ array that every GPU loading this library reserves until exit.
+ * Runs needing more return ORF_ETOOLARGE, before any device work (the
+ * config-1 grating coupler, 800 x 300 FP64 with 51 wavelengths, needs
+ * about 20 MiB).  The first
+ * call on a device looks up the array's address and should come before any
+ * stream capture.  Calls share the array: calls that overlap on the GPU race,
+ * and each call zeroes what it uses first.  There is no progress callback;
+ * work is queued on `stream` (a cudaStream_t; NULL = per-thread default
+ * stream) and the call returns when the run is done. */
+ORF_API int32_t orf_fdtd2d_run_noalloc(const orf_sim2d* sim, orf_out2d* out, void* stream);
+
 /* ------------------------------------------------------------ 3D runs --- */
 /* Plane sizes Na, Nb of each monitor (arrays of n_mon). */
 ORF_API int32_t orf_out3d_sizes(const orf_sim3d* sim, int32_t* na, int32_t* nb);

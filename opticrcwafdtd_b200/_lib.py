@@ -30,6 +30,7 @@ _SIGS = {
     "orf_out2d_sizes": (C.c_int32, [P(_abi.OrfSim2D), P(C.c_int64), P(C.c_int64), P(C.c_int64), P(C.c_int64)]),
     "orf_fdtd2d_run": (C.c_int32, [P(_abi.OrfSim2D), P(_abi.OrfOut2D), _abi.PROGRESS_FN, C.c_void_p]),
     "orf_fdtd2d_run_ctx": (C.c_int32, [C.c_void_p, P(_abi.OrfSim2D), P(_abi.OrfOut2D), _abi.PROGRESS_FN, C.c_void_p]),
+    "orf_fdtd2d_run_noalloc": (C.c_int32, [P(_abi.OrfSim2D), P(_abi.OrfOut2D), C.c_void_p]),
     "orf_job2d_create": (C.c_int32, [C.c_void_p, P(_abi.OrfSim2D), P(C.c_void_p)]),
     "orf_job3d_create": (C.c_int32, [C.c_void_p, P(_abi.OrfSim3D), P(C.c_void_p)]),
     "orf_job_advance": (C.c_int32, [C.c_void_p, C.c_int64]),

@@ -238,18 +238,24 @@ int Job2D<R>::create(const orf_sim2d* s) {
     ar.add(&d_streams, nstreams + 1);
     ar.add(&d_items, nitems + 1);
     ar.add(&d_pairs, npairs + 1);
-    ORF_TRY(ar.alloc());
+    if (ext_base) {
+        ORF_TRY(ar.place(ext_base, ext_cap));
+    } else {
+        ORF_TRY(ar.alloc());
+    }
     arena = ar;
     cudaStream_t st = ctx->stream;
     ORF_CUDA(cudaMemsetAsync(arena.base, 0, arena.total, st));
 
-    // mapped host status ring and cancel flag
-    ORF_CUDA(cudaHostAlloc((void**)&ring_h, sizeof(ChunkStatus) * kStatusRing, cudaHostAllocMapped));
-    std::memset(ring_h, 0, sizeof(ChunkStatus) * kStatusRing);
-    ORF_CUDA(cudaHostGetDevicePointer((void**)&ring_d, ring_h, 0));
-    ORF_CUDA(cudaHostAlloc((void**)&cancel_h, sizeof(int), cudaHostAllocMapped));
-    *cancel_h = 0;
-    ORF_CUDA(cudaHostGetDevicePointer((void**)&cancel_d, (void*)cancel_h, 0));
+    // mapped host status ring and cancel flag (not in no-allocation mode)
+    if (!ext_base) {
+        ORF_CUDA(cudaHostAlloc((void**)&ring_h, sizeof(ChunkStatus) * kStatusRing, cudaHostAllocMapped));
+        std::memset(ring_h, 0, sizeof(ChunkStatus) * kStatusRing);
+        ORF_CUDA(cudaHostGetDevicePointer((void**)&ring_d, ring_h, 0));
+        ORF_CUDA(cudaHostAlloc((void**)&cancel_h, sizeof(int), cudaHostAllocMapped));
+        *cancel_h = 0;
+        ORF_CUDA(cudaHostGetDevicePointer((void**)&cancel_d, (void*)cancel_h, 0));
+    }
 
     // ---- upload
     std::vector<unsigned char> ib0(cellsP * isz), ib1(te ? 0 : cellsP * isz);
@@ -477,8 +483,8 @@ int Job2D<R>::init_state() {
     js.shutoff = shutoff;
     js.ring = ring_d;
     js.cancel = cancel_d;
-    std::memset(ring_h, 0, sizeof(ChunkStatus) * kStatusRing);
-    *cancel_h = 0;
+    if (ring_h) std::memset(ring_h, 0, sizeof(ChunkStatus) * kStatusRing);
+    if (cancel_h) *cancel_h = 0;
     enq_steps = 0;
     ORF_CUDA(cudaMemcpyAsync(d_st, &js, sizeof js, cudaMemcpyHostToDevice, ctx->stream));
     pl = ProgressLoop{};
@@ -535,6 +541,15 @@ int Job2D<R>::advance(int64_t nsteps, orf_progress_fn progress, void* user) {
     eng.collect_timing();
     ctx->stats.cell_updates += (pl.last_step - steps0) * (int64_t)nx * nz;
     return pl.cancelled ? ORF_ECANCELLED : ORF_OK;
+}
+
+template <class R>
+int Job2D<R>::advance_all_direct() {
+    const int64_t chunks = (std::max<int64_t>(0, nmax - enq_steps) + kChunk - 1) / kChunk;
+    enq_steps += chunks * kChunk;
+    for (int64_t c = 0; c < chunks; ++c) ORF_TRY(eng.enqueue_chunk(ctx->stream, false));
+    ORF_CUDA(cudaStreamSynchronize(ctx->stream));
+    return ORF_OK;
 }
 
 template <class R>

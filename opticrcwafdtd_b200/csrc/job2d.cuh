@@ -41,6 +41,10 @@ struct Job2D : orf_job {
     int* cancel_d = nullptr;
     ChunkEngine eng;
     ProgressLoop pl;
+    // no-allocation mode: device state carved from ext_base (see noalloc.cu),
+    // no mapped status ring, no graphs, no events
+    void* ext_base = nullptr;
+    size_t ext_cap = 0;
 
     Job2D() { dims = 2; }
     ~Job2D() override;
@@ -54,6 +58,8 @@ struct Job2D : orf_job {
     int reset() override;
     int get_fields(double* const* f, int nf) override;
     int finish2d(orf_out2d* o) override;
+    // enqueue every remaining chunk with direct launches, then synchronize
+    int advance_all_direct();
 };
 
 }  // namespace orf

@@ -111,8 +111,27 @@ struct Arena {
         }
         return ORF_OK;
     }
+    // Carve the requests from caller-provided device memory instead of
+    // cudaMalloc (no allocation); fails with ORF_ETOOLARGE if they do not fit.
+    int place(void* ext, size_t cap) {
+        total = bytes();
+        if (total > cap) {
+            set_error("run needs %.1f MB of device scratch, above the %.1f MB limit", total / 1048576.0,
+                      cap / 1048576.0);
+            return ORF_ETOOLARGE;
+        }
+        base = ext;
+        owned = false;
+        char* p = static_cast<char*>(base);
+        for (auto& r : req) {
+            *r.first = p;
+            p += (r.second + 255) & ~size_t(255);
+        }
+        return ORF_OK;
+    }
+    bool owned = true;
     void release() {
-        if (base) cudaFree(base);
+        if (base && owned) cudaFree(base);
         base = nullptr;
     }
 };
