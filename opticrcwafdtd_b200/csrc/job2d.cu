@@ -394,6 +394,8 @@ int Job2D<R>::pick_tiling(int npx, int npz) {
         set_error("unknown 2D kernel variant %d", fvariant);
         return ORF_EINVAL;
     }
+    // frame strips (npml + T cells wide) use the 128 x 32 / 64 x 32 geometry
+    // (measured faster than 64 x 64 on the config-2 grid)
     variant = 2;
     variant2d_info(variant, f64, &bv);
     const int tmax = std::min({kMaxSub, (bv.lz() - 1) / 2, (bv.lx() - 1) / 2, (fv.lz() - 1) / 2, (fv.lx() - 4) / 2});

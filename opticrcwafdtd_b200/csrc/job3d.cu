@@ -1,0 +1,582 @@
+// job3d.cu -- one orf.fdtd3D run on the device (toolbox/+orf/fdtd3D.m:1-29).
+//
+// Host work at creation: validate the sim struct, turn the three eps arrays
+// into material indices (uint8/16/32) plus a table of C/eps (exact), build the
+// CPML profiles and slab maps of every axis, the TF/SF plane tables, the DFT
+// streams of the monitor planes (Ea, Eb, Ha, Hb) and the column tiles, and
+// upload everything into one device arena.  One z-marching launch advances
+// one step; the shared ChunkEngine runs the loop.
+#include <algorithm>
+#include <unordered_map>
+
+#include "engine.cuh"
+
+namespace orf {
+
+int validate3d(const orf_sim3d* s) {
+    if (!s) { set_error("sim is NULL"); return ORF_EINVAL; }
+    const int n[3] = {s->nx, s->ny, s->nz};
+    for (int q = 0; q < 3; ++q)
+        if (n[q] < 2) { set_error("every grid axis needs at least 2 points"); return ORF_EINVAL; }
+    if ((int64_t)n[0] * n[1] * n[2] > ((int64_t)1 << 34)) { set_error("grid exceeds 2^34 cells"); return ORF_ETOOLARGE; }
+    if (!(s->d > 0) || !std::isfinite(s->d)) { set_error("grid spacing must be positive"); return ORF_EINVAL; }
+    if (!(s->courant > 0) || s->courant > 1.0 / std::sqrt(3.0) + 1e-12) {
+        set_error("courant %.6g outside (0, 1/sqrt(3)] (3D Yee stability limit)", s->courant);
+        return ORF_EINVAL;
+    }
+    if (!s->eps_x || !s->eps_y || !s->eps_z) { set_error("sim.eps.x/.y/.z are required"); return ORF_EINVAL; }
+    const size_t N = (size_t)n[0] * n[1] * n[2];
+    const double* e[3] = {s->eps_x, s->eps_y, s->eps_z};
+    for (int c = 0; c < 3; ++c)
+        for (size_t q = 0; q < N; ++q)
+            if (!(e[c][q] > 0) || !std::isfinite(e[c][q])) {
+                set_error("sim.eps.%c(%zu) = %g: permittivity must be positive and finite", "xyz"[c], q + 1, e[c][q]);
+                return ORF_EINVAL;
+            }
+    for (int q = 0; q < 3; ++q) {
+        const int np = s->periodic[q] ? 0 : s->npml[q];
+        if (np < 0 || 2 * np >= n[q] - 1) { set_error("npml(%d) = %d does not fit the grid", q + 1, np); return ORF_EINVAL; }
+    }
+    const int a = s->src_axis;
+    if (a < 0 || a > 2) { set_error("source.axis must be 1, 2 or 3"); return ORF_EINVAL; }
+    const int np = s->periodic[a] ? 0 : s->npml[a];
+    if (s->src_index < 0 || s->src_index >= n[a]) { set_error("source.index outside the grid"); return ORF_EINVAL; }
+    if (s->src_index < np || s->src_index >= n[a] - np) { set_error("source.index lies inside the CPML"); return ORF_EINVAL; }
+    if (!s->src_Ea || !s->src_Eb || !s->src_Ha || !s->src_Hb) { set_error("source profiles Ea, Eb, Ha, Hb are required"); return ORF_EINVAL; }
+    if (!(s->src_lambda0 > 0) || !(s->src_bw > 0)) { set_error("source.lambda0 and source.bw must be positive"); return ORF_EINVAL; }
+    if (s->n_mon < 0 || s->n_mon > kMaxMon) { set_error("at most %d monitors", kMaxMon); return ORF_EINVAL; }
+    for (int m = 0; m < s->n_mon; ++m) {
+        const int q = s->mon_axis[m];
+        if (q < 0 || q > 2) { set_error("monitors(%d).axis must be 1..3", m + 1); return ORF_EINVAL; }
+        if (s->mon_index[m] < 0 || s->mon_index[m] >= n[q]) { set_error("monitors(%d).index outside the grid", m + 1); return ORF_EINVAL; }
+    }
+    if (s->n_lambda < 1 || !s->lambdas) { set_error("sim.lambdas must not be empty"); return ORF_EINVAL; }
+    for (int l = 0; l < s->n_lambda; ++l)
+        if (!(s->lambdas[l] > 0)) { set_error("lambdas(%d) must be positive", l + 1); return ORF_EINVAL; }
+    if (!(s->max_time >= 0) || !(s->shutoff >= 0)) { set_error("maxTime and shutoff must be non-negative"); return ORF_EINVAL; }
+    if (s->precision != ORF_DOUBLE && s->precision != ORF_SINGLE) { set_error("precision must be double or single"); return ORF_EINVAL; }
+    return ORF_OK;
+}
+
+namespace {
+
+template <class R>
+struct Job3D : orf_job {
+    int n[3] = {0, 0, 0};
+    bool per[3] = {false, false, false};
+    int pitch = 0, nM = 0, nL = 0, idxw = 1;
+    double d = 0, Cc = 0, S = 0, src_end = 0, shutoff = 0;
+    int64_t nmax = 0, nsrc = 0, enq_steps = 0;
+    Arena arena;
+    Inst3D<R> h{};
+    Inst3D<R>* d_inst = nullptr;
+    JobState* d_st = nullptr;
+    JobState** d_states = nullptr;
+    std::vector<Tile3D> tiles;
+    Tile3D* d_tiles = nullptr;
+    DftStream* d_streams = nullptr;
+    std::vector<DftStream> host_streams;
+    FlushItem* d_items = nullptr;
+    FluxPair* d_pairs = nullptr;
+    int nstreams = 0, nitems = 0, npairs = 0;
+    void* d_acc = nullptr;
+    double* d_omega = nullptr;
+    double* d_flux = nullptr;
+    double2* d_stage = nullptr;
+    size_t stage_elems = 0;
+    std::vector<std::pair<int, int>> planes;   // (Na, Nb) per monitor
+    ChunkStatus* ring_h = nullptr;
+    ChunkStatus* ring_d = nullptr;
+    volatile int* cancel_h = nullptr;
+    int* cancel_d = nullptr;
+    ChunkEngine eng;
+    ProgressLoop pl;
+
+    Job3D() { dims = 3; }
+    ~Job3D() override {
+        if (arena.base) {
+            cudaStreamSynchronize(ctx->stream);
+            arena.release();
+        }
+        if (ring_h) cudaFreeHost(ring_h);
+        if (cancel_h) cudaFreeHost((void*)cancel_h);
+    }
+    size_t N() const { return (size_t)n[0] * n[1] * n[2]; }
+    size_t NP() const { return (size_t)pitch * n[1] * n[2]; }
+    int64_t cells() const override { return (int64_t)N(); }
+    int64_t step_budget() const override { return nmax; }
+
+    int create(const orf_sim3d* s);
+    int init_state();
+    int advance(int64_t nsteps, orf_progress_fn progress, void* user) override;
+    int64_t steps_done() override;
+    int reset() override;
+    int get_fields(double* const* f, int nf) override;
+    int finish3d(orf_out3d* o) override;
+};
+
+struct Lut3 {
+    std::unordered_map<uint64_t, uint32_t> map;
+    std::vector<double> vals;
+    uint64_t last_key = ~0ull;
+    uint32_t last_id = 0;
+    uint32_t get(double v) {
+        uint64_t key;
+        std::memcpy(&key, &v, 8);
+        if (key == last_key) return last_id;
+        auto it = map.find(key);
+        uint32_t id;
+        if (it != map.end()) {
+            id = it->second;
+        } else {
+            id = (uint32_t)vals.size();
+            map.emplace(key, id);
+            vals.push_back(v);
+        }
+        last_key = key;
+        last_id = id;
+        return id;
+    }
+};
+
+template <class R>
+int Job3D<R>::create(const orf_sim3d* s) {
+    ORF_TRY(validate3d(s));
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev != ctx->device) ORF_CUDA(cudaSetDevice(ctx->device));
+    n[0] = s->nx; n[1] = s->ny; n[2] = s->nz;
+    for (int q = 0; q < 3; ++q) per[q] = s->periodic[q] != 0;
+    pitch = (n[0] + 31) & ~31;
+    d = s->d;
+    Cc = s->courant;
+    S = Cc * d;
+    nM = s->n_mon;
+    nL = s->n_lambda;
+    cudaStream_t st = ctx->stream;
+
+    // ---- material indices (exact table of distinct eps values)
+    Lut3 lut;
+    const double* eps[3] = {s->eps_x, s->eps_y, s->eps_z};
+    std::vector<uint32_t> ix[3];
+    for (int c = 0; c < 3; ++c) {
+        ix[c].assign(NP(), 0);
+        for (int k = 0; k < n[2]; ++k)
+            for (int j = 0; j < n[1]; ++j) {
+                const double* src = eps[c] + (size_t)n[0] * ((size_t)j + (size_t)n[1] * k);
+                uint32_t* dst = ix[c].data() + ((size_t)k * n[1] + j) * pitch;
+                for (int i = 0; i < n[0]; ++i) dst[i] = lut.get(src[i]);
+            }
+    }
+    const size_t nlut = lut.vals.size();
+    idxw = nlut <= 256 ? 1 : (nlut <= 65536 ? 2 : 4);
+    std::vector<R> hlutc(nlut);
+    for (size_t v = 0; v < nlut; ++v) hlutc[v] = R(Cc / lut.vals[v]);
+
+    // ---- CPML per axis
+    const double alpha_max = kPmlAlphaMaxPerK0 * 2.0 * kPi / s->src_lambda0;
+    std::vector<double> pI[3], pH[3];
+    std::vector<int> slI[3], slH[3];
+    int nsI[3], nsH[3];
+    for (int q = 0; q < 3; ++q) {
+        const int np = per[q] ? 0 : s->npml[q];
+        pml_profile(n[q], n[q], np, 0.0, d, S, alpha_max, pI[q], &nsI[q]);
+        pml_profile(n[q], n[q], np, 0.5, d, S, alpha_max, pH[q], &nsH[q]);
+        slI[q].assign(n[q], -1);
+        slH[q].assign(n[q], -1);
+        int a = 0, b = 0;
+        for (int u = 0; u < n[q]; ++u) {
+            if (pI[q][3 * u + 1] != 0.0 || pI[q][3 * u] != 1.0 || pI[q][3 * u + 2] != 1.0) slI[q][u] = a++;
+            if (pH[q][3 * u + 1] != 0.0 || pH[q][3 * u] != 1.0 || pH[q][3 * u + 2] != 1.0) slH[q][u] = b++;
+        }
+        nsI[q] = a;
+        nsH[q] = b;
+    }
+
+    // ---- TF/SF plane: d = axis, a = d+1, b = d+2 (fdtd3D.m:15-21)
+    const int sa = s->src_axis, sb = (sa + 1) % 3, sc = (sa + 2) % 3, ss = s->src_index;
+    const int Na = n[sb], Nb = n[sc];
+    std::vector<R> hsHa((size_t)Na * Nb), hsHb(hsHa.size()), hsEa(hsHa.size()), hsEb(hsHa.size());
+    for (int ib = 0; ib < Nb; ++ib)
+        for (int ia = 0; ia < Na; ++ia) {
+            const size_t pq = (size_t)ia + (size_t)Na * ib;
+            int v[3];
+            v[sa] = ss;
+            v[sb] = ia;
+            v[sc] = ib;
+            const size_t q0 = (size_t)v[0] + (size_t)n[0] * ((size_t)v[1] + (size_t)n[1] * v[2]);
+            hsHa[pq] = R(-Cc * s->src_Eb[pq]);
+            hsHb[pq] = R(Cc * s->src_Ea[pq]);
+            hsEa[pq] = R((Cc / eps[sb][q0]) * s->src_Hb[pq]);
+            hsEb[pq] = R(-(Cc / eps[sc][q0]) * s->src_Ha[pq]);
+        }
+    const Pulse g(s->src_lambda0, s->src_bw);
+    src_end = g.tend;
+    nsrc = (int64_t)std::ceil(g.tend / S) + 2;
+    std::vector<double> hgE(nsrc), hgH(nsrc);
+    for (int64_t k = 0; k < nsrc; ++k) {
+        hgE[k] = g(k * S);
+        hgH[k] = g((k + 0.5) * S + s->src_neff * 0.5 * d);
+    }
+    nmax = max_steps(s->max_time, S);
+    shutoff = s->shutoff;
+
+    // ---- monitors -> DFT streams (Ea, Eb at t_{n+1}; Ha, Hb at t_{n+1/2})
+    int sstride = 0;
+    std::vector<int> moff(nM);
+    planes.clear();
+    for (int m = 0; m < nM; ++m) {
+        const int q = s->mon_axis[m];
+        const int na = n[(q + 1) % 3], nb = n[(q + 2) % 3];
+        planes.push_back({na, nb});
+        moff[m] = sstride;
+        sstride += 4 * na * nb;
+    }
+    struct SDesc { int soff, len, half; };
+    std::vector<SDesc> sd;
+    for (int m = 0; m < nM; ++m) {
+        const int np = planes[m].first * planes[m].second;
+        for (int f = 0; f < 4; ++f) sd.push_back({moff[m] + f * np, np, f >= 2 ? 1 : 0});
+    }
+    nstreams = (int)sd.size();
+    std::vector<FlushItem> items;
+    for (int q = 0; q < nstreams; ++q)
+        for (int e0 = 0; e0 < sd[q].len; e0 += 128)
+            for (int l0 = 0; l0 < nL; l0 += 8) items.push_back({q, e0, l0, 0});
+    nitems = (int)items.size();
+    std::vector<FluxPair> pairs;
+    for (int m = 0; m < nM; ++m)   // 1/2 Re sum(Ea Hb* - Eb Ha*) dA  (fdtd3D.m:26)
+        pairs.push_back({4 * m, 4 * m + 3, 4 * m + 1, 4 * m + 2, m, nM, 0.5 * d * d});
+    npairs = (int)pairs.size();
+
+    // ---- tiles: kTile3X x kTile3Y columns, full z
+    tiles.clear();
+    for (int j0 = 0; j0 < n[1]; j0 += kTile3Y)
+        for (int i0 = 0; i0 < n[0]; i0 += kTile3X) {
+            Tile3D t;
+            t.inst = 0;
+            t.i0 = i0;
+            t.j0 = j0;
+            t.tw = (short)std::min(kTile3X, n[0] - i0);
+            t.th = (short)std::min(kTile3Y, n[1] - j0);
+            tiles.push_back(t);
+        }
+
+    // ---- device arena
+    Arena ar;
+    for (int b = 0; b < 2; ++b)
+        for (int c = 0; c < 3; ++c) {
+            ar.add(&h.E[b][c], NP());
+            ar.add(&h.H[b][c], NP());
+        }
+    for (int b = 0; b < 2; ++b)
+        for (int c = 0; c < 3; ++c)
+            for (int q = 0; q < 3; ++q) {
+                h.psiE[b][c][q] = nullptr;
+                h.psiH[b][c][q] = nullptr;
+                if (q == c) continue;
+                if (nsI[q] > 0) ar.add(&h.psiE[b][c][q], N() / n[q] * nsI[q]);
+                if (nsH[q] > 0) ar.add(&h.psiH[b][c][q], N() / n[q] * nsH[q]);
+            }
+    unsigned char* d_ix[3];
+    for (int c = 0; c < 3; ++c) ar.add(&d_ix[c], NP() * idxw);
+    R *d_lutc, *d_pI[3], *d_pH[3], *d_sHa, *d_sHb, *d_sEa, *d_sEb, *d_samples;
+    int *d_slI[3], *d_slH[3];
+    double *d_lute, *d_gE, *d_gH;
+    ar.add(&d_lutc, nlut);
+    ar.add(&d_lute, nlut);
+    for (int q = 0; q < 3; ++q) {
+        ar.add(&d_pI[q], pI[q].size());
+        ar.add(&d_pH[q], pH[q].size());
+        ar.add(&d_slI[q], n[q]);
+        ar.add(&d_slH[q], n[q]);
+    }
+    ar.add(&d_sHa, hsHa.size());
+    ar.add(&d_sHb, hsHa.size());
+    ar.add(&d_sEa, hsHa.size());
+    ar.add(&d_sEb, hsHa.size());
+    ar.add(&d_gE, nsrc);
+    ar.add(&d_gH, nsrc);
+    ar.add(&d_samples, (size_t)kChunk * sstride + 1);
+    size_t acc_elems = 0;
+    stage_elems = 1;
+    for (auto& q : sd) {
+        acc_elems += (size_t)q.len * nL;
+        stage_elems = std::max(stage_elems, (size_t)q.len * nL);
+    }
+    ar.add(&d_acc, acc_elems * 16 + 16);
+    ar.add(&d_omega, nL);
+    ar.add(&d_flux, (size_t)nM * nL + 1);
+    ar.add(&d_stage, stage_elems);
+    ar.add(&d_inst, 1);
+    ar.add(&d_st, 1);
+    ar.add(&d_states, 1);
+    ar.add(&d_tiles, tiles.size());
+    ar.add(&d_streams, nstreams + 1);
+    ar.add(&d_items, nitems + 1);
+    ar.add(&d_pairs, npairs + 1);
+    ORF_TRY(ar.alloc());
+    arena = ar;
+    ORF_CUDA(cudaMemsetAsync(arena.base, 0, arena.total, st));
+    ORF_CUDA(cudaHostAlloc((void**)&ring_h, sizeof(ChunkStatus) * kStatusRing, cudaHostAllocMapped));
+    ORF_CUDA(cudaHostGetDevicePointer((void**)&ring_d, ring_h, 0));
+    ORF_CUDA(cudaHostAlloc((void**)&cancel_h, sizeof(int), cudaHostAllocMapped));
+    ORF_CUDA(cudaHostGetDevicePointer((void**)&cancel_d, (void*)cancel_h, 0));
+
+    auto up = [&](void* dst, const void* src, size_t bytes) -> int {
+        if (bytes == 0) return ORF_OK;
+        ORF_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
+        ORF_CUDA(cudaStreamSynchronize(st));   // host staging vectors are freed on return
+        ctx->stats.h2d_bytes += (int64_t)bytes;
+        return ORF_OK;
+    };
+    for (int c = 0; c < 3; ++c) {
+        if (idxw == 4) {
+            ORF_TRY(up(d_ix[c], ix[c].data(), NP() * 4));
+        } else if (idxw == 2) {
+            std::vector<uint16_t> t(ix[c].begin(), ix[c].end());
+            ORF_TRY(up(d_ix[c], t.data(), NP() * 2));
+        } else {
+            std::vector<uint8_t> t(ix[c].begin(), ix[c].end());
+            ORF_TRY(up(d_ix[c], t.data(), NP()));
+        }
+        std::vector<uint32_t>().swap(ix[c]);
+    }
+    ORF_TRY(up(d_lutc, hlutc.data(), nlut * sizeof(R)));
+    ORF_TRY(up(d_lute, lut.vals.data(), nlut * sizeof(double)));
+    for (int q = 0; q < 3; ++q) {
+        std::vector<R> a(pI[q].begin(), pI[q].end()), b(pH[q].begin(), pH[q].end());
+        ORF_TRY(up(d_pI[q], a.data(), a.size() * sizeof(R)));
+        ORF_TRY(up(d_pH[q], b.data(), b.size() * sizeof(R)));
+        ORF_TRY(up(d_slI[q], slI[q].data(), n[q] * sizeof(int)));
+        ORF_TRY(up(d_slH[q], slH[q].data(), n[q] * sizeof(int)));
+    }
+    ORF_TRY(up(d_sHa, hsHa.data(), hsHa.size() * sizeof(R)));
+    ORF_TRY(up(d_sHb, hsHb.data(), hsHb.size() * sizeof(R)));
+    ORF_TRY(up(d_sEa, hsEa.data(), hsEa.size() * sizeof(R)));
+    ORF_TRY(up(d_sEb, hsEb.data(), hsEb.size() * sizeof(R)));
+    ORF_TRY(up(d_gE, hgE.data(), nsrc * sizeof(double)));
+    ORF_TRY(up(d_gH, hgH.data(), nsrc * sizeof(double)));
+    std::vector<double> om(nL);
+    for (int l = 0; l < nL; ++l) om[l] = 2.0 * kPi / s->lambdas[l];
+    ORF_TRY(up(d_omega, om.data(), nL * sizeof(double)));
+
+    for (int q = 0; q < 3; ++q) {
+        h.n[q] = n[q];
+        h.per[q] = per[q] ? 1 : 0;
+        h.pmlI[q] = d_pI[q];
+        h.pmlH[q] = d_pH[q];
+        h.slabI[q] = d_slI[q];
+        h.slabH[q] = d_slH[q];
+        h.nslabI[q] = nsI[q];
+        h.nslabH[q] = nsH[q];
+        h.idx[q] = d_ix[q];
+    }
+    h.pitch = pitch;
+    h.idxw = idxw;
+    h.C = R(Cc);
+    h.lutc = d_lutc;
+    h.lute = d_lute;
+    h.sa = sa; h.ss = ss; h.na = Na; h.nb = Nb;
+    h.sHa = d_sHa; h.sHb = d_sHb; h.sEa = d_sEa; h.sEb = d_sEb;
+    h.gE = d_gE; h.gH = d_gH; h.nsrc = nsrc;
+    h.nmon = nM;
+    h.sstride = sstride;
+    for (int m = 0; m < kMaxMon; ++m) {
+        h.mon_axis[m] = m < nM ? s->mon_axis[m] : 0;
+        h.mon_index[m] = m < nM ? s->mon_index[m] : -1;
+        h.mon_off[m] = m < nM ? moff[m] : 0;
+    }
+    h.samples = d_samples;
+    h.st = d_st;
+    ORF_TRY(up(d_inst, &h, sizeof(h)));
+    ORF_TRY(up(d_tiles, tiles.data(), tiles.size() * sizeof(Tile3D)));
+    std::vector<DftStream> hs(nstreams);
+    size_t aoff = 0;
+    for (int q = 0; q < nstreams; ++q) {
+        hs[q].st = d_st;
+        hs[q].samples = d_samples;
+        hs[q].sstride = sstride;
+        hs[q].soff = sd[q].soff;
+        hs[q].len = sd[q].len;
+        hs[q].half = sd[q].half;
+        hs[q].nl = nL;
+        hs[q].omega = d_omega;
+        hs[q].acc = static_cast<char*>(d_acc) + aoff * 16;
+        aoff += (size_t)sd[q].len * nL;
+    }
+    host_streams = hs;
+    ORF_TRY(up(d_streams, hs.data(), hs.size() * sizeof(DftStream)));
+    ORF_TRY(up(d_items, items.data(), items.size() * sizeof(FlushItem)));
+    ORF_TRY(up(d_pairs, pairs.data(), pairs.size() * sizeof(FluxPair)));
+    JobState* sp = d_st;
+    ORF_TRY(up(d_states, &sp, sizeof(sp)));
+    ORF_TRY(init_state());
+
+    eng.ctx = ctx;
+    eng.fp64 = sizeof(R) == 8;
+    eng.T = 1;
+    eng.par = 0;
+    eng.d_streams = d_streams;
+    eng.d_items = d_items;
+    eng.nitems = nitems;
+    eng.d_states = d_states;
+    eng.nstates = 1;
+    const int64_t ncell = (int64_t)N();
+    eng.step = [this, ncell](int off, int nsub, int par, int we, cudaStream_t stream, KernelTimer* tm) -> cudaError_t {
+        (void)nsub;
+        cudaEvent_t a = nullptr;
+        if (tm && tm->begin(stream, &a) != ORF_OK) return cudaErrorUnknown;
+        cudaError_t e = launch_step3d(sizeof(R) == 8, idxw, d_inst, d_tiles, (int)tiles.size(), off, par, we, stream);
+        if (e != cudaSuccess) return e;
+        if (tm && tm->end(stream, 0, ncell, a) != ORF_OK) return cudaErrorUnknown;
+        return e;
+    };
+    ORF_CUDA(cudaStreamSynchronize(st));
+    return ORF_OK;
+}
+
+template <class R>
+int Job3D<R>::init_state() {
+    JobState js{};
+    js.nmax = nmax;
+    js.done = nmax <= 0 ? 1 : 0;
+    js.S = S;
+    js.src_end = src_end;
+    js.shutoff = shutoff;
+    js.ring = ring_d;
+    js.cancel = cancel_d;
+    if (ring_h) std::memset(ring_h, 0, sizeof(ChunkStatus) * kStatusRing);
+    if (cancel_h) *cancel_h = 0;
+    enq_steps = 0;
+    ORF_CUDA(cudaMemcpyAsync(d_st, &js, sizeof js, cudaMemcpyHostToDevice, ctx->stream));
+    ORF_CUDA(cudaStreamSynchronize(ctx->stream));
+    pl = ProgressLoop{};
+    pl.ring = ring_h;
+    pl.cancel = cancel_h;
+    pl.S = S;
+    pl.src_end = src_end;
+    pl.shutoff = shutoff;
+    eng.par = 0;
+    return ORF_OK;
+}
+
+template <class R>
+int Job3D<R>::reset() {
+    cudaStream_t st = ctx->stream;
+    ORF_CUDA(cudaStreamSynchronize(st));
+    for (int b = 0; b < 2; ++b)
+        for (int c = 0; c < 3; ++c) {
+            ORF_CUDA(cudaMemsetAsync(h.E[b][c], 0, NP() * sizeof(R), st));
+            ORF_CUDA(cudaMemsetAsync(h.H[b][c], 0, NP() * sizeof(R), st));
+            for (int q = 0; q < 3; ++q) {
+                if (h.psiE[b][c][q]) ORF_CUDA(cudaMemsetAsync(h.psiE[b][c][q], 0, N() / n[q] * h.nslabI[q] * sizeof(R), st));
+                if (h.psiH[b][c][q]) ORF_CUDA(cudaMemsetAsync(h.psiH[b][c][q], 0, N() / n[q] * h.nslabH[q] * sizeof(R), st));
+            }
+        }
+    size_t acc_elems = 0;
+    for (auto& q : host_streams) acc_elems += (size_t)q.len * nL;
+    ORF_CUDA(cudaMemsetAsync(d_acc, 0, acc_elems * 16, st));
+    return init_state();
+}
+
+template <class R>
+int Job3D<R>::advance(int64_t nsteps, orf_progress_fn progress, void* user) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev != ctx->device) ORF_CUDA(cudaSetDevice(ctx->device));
+    const int64_t left = std::max<int64_t>(0, nmax - enq_steps);
+    const int64_t chunks = (std::min(nsteps, left) + kChunk - 1) / kChunk;
+    enq_steps += chunks * kChunk;
+    const int64_t steps0 = pl.last_step;
+    ORF_TRY(run_chunks(eng, pl, ctx, chunks, progress, user));
+    eng.collect_timing();
+    ctx->stats.cell_updates += (pl.last_step - steps0) * (int64_t)N();
+    return pl.cancelled ? ORF_ECANCELLED : ORF_OK;
+}
+
+template <class R>
+int64_t Job3D<R>::steps_done() {
+    JobState js;
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return -1;
+    if (cudaMemcpy(&js, d_st, sizeof js, cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+    return js.step;
+}
+
+template <class R>
+int Job3D<R>::finish3d(orf_out3d* o) {
+    cudaStream_t st = ctx->stream;
+    ORF_CUDA(cudaStreamSynchronize(st));
+    JobState js;
+    ORF_CUDA(cudaMemcpy(&js, d_st, sizeof js, cudaMemcpyDeviceToHost));
+    const bool f64 = sizeof(R) == 8;
+    ORF_CUDA(launch_flux(f64, d_streams, d_pairs, npairs, nL, d_flux, st));
+    std::vector<double> fl((size_t)nM * nL);
+    if (!fl.empty()) ORF_CUDA(cudaMemcpyAsync(fl.data(), d_flux, fl.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    ctx->stats.d2h_bytes += (int64_t)(fl.size() * sizeof(double));
+    for (int m = 0; m < nM; ++m) {
+        double* const* dsts[4] = {o->mon_Ea, o->mon_Eb, o->mon_Ha, o->mon_Hb};
+        for (int f = 0; f < 4; ++f) {
+            if (!dsts[f] || !dsts[f][m]) continue;
+            const DftStream& S = host_streams[4 * m + f];
+            const size_t ne = (size_t)S.len * nL;
+            if (f64) {
+                ORF_CUDA(cudaMemcpyAsync(dsts[f][m], S.acc, ne * sizeof(double2), cudaMemcpyDeviceToHost, st));
+            } else {
+                ORF_CUDA(launch_acc_to_complex(false, S.acc, ne, d_stage, st));
+                ORF_CUDA(cudaMemcpyAsync(dsts[f][m], d_stage, ne * sizeof(double2), cudaMemcpyDeviceToHost, st));
+            }
+            ORF_CUDA(cudaStreamSynchronize(st));
+            ctx->stats.d2h_bytes += (int64_t)(ne * sizeof(double2));
+        }
+    }
+    ORF_CUDA(cudaStreamSynchronize(st));
+    if (o->flux)
+        for (size_t q = 0; q < fl.size(); ++q) o->flux[q] = fl[q];
+    o->converged = js.converged;
+    o->steps = js.step;
+    o->time = js.step * S;
+    return ORF_OK;
+}
+
+template <class R>
+int Job3D<R>::get_fields(double* const* f, int nf) {
+    if (nf < 6) { set_error("3D fields are Ex Ey Ez Hx Hy Hz"); return ORF_EINVAL; }
+    ORF_CUDA(cudaStreamSynchronize(ctx->stream));
+    JobState js;
+    ORF_CUDA(cudaMemcpy(&js, d_st, sizeof js, cudaMemcpyDeviceToHost));
+    const int b = js.cur;
+    std::vector<R> tmp(NP());
+    for (int q = 0; q < 6; ++q) {
+        if (!f[q]) continue;
+        R* src = q < 3 ? h.E[b][q] : h.H[b][q - 3];
+        ORF_CUDA(cudaMemcpy(tmp.data(), src, NP() * sizeof(R), cudaMemcpyDeviceToHost));
+        for (int k = 0; k < n[2]; ++k)
+            for (int j = 0; j < n[1]; ++j)
+                for (int i = 0; i < n[0]; ++i)
+                    f[q][(size_t)i + (size_t)n[0] * ((size_t)j + (size_t)n[1] * k)] =
+                        (double)tmp[((size_t)k * n[1] + j) * pitch + i];
+    }
+    return ORF_OK;
+}
+
+}  // namespace
+
+int make_job3d(orf_ctx* ctx, const orf_sim3d* sim, orf_job** out) {
+    *out = nullptr;
+    ORF_TRY(validate3d(sim));
+    if (sim->precision == ORF_SINGLE) {
+        auto j = std::make_unique<Job3D<float>>();
+        j->ctx = ctx;
+        ORF_TRY(j->create(sim));
+        *out = j.release();
+    } else {
+        auto j = std::make_unique<Job3D<double>>();
+        j->ctx = ctx;
+        ORF_TRY(j->create(sim));
+        *out = j.release();
+    }
+    return ORF_OK;
+}
+
+}  // namespace orf

@@ -140,52 +140,54 @@ struct alignas(16) FastTile2D {
 static_assert(sizeof(FastTile2D) == 128, "FastTile2D must stay 128 bytes");
 
 // --------------------------------------------------------------------- 3D --
-// Six components at their Yee positions (fdtd3D.m:2-5); layout [nz][ny][pitch].
+// Six components at their Yee positions (fdtd3D.m:2-5); every array is
+// [nz][ny][pitch] with x fastest.  Component c of E/H: 0 = x, 1 = y, 2 = z.
 template <class R>
 struct Inst3D {
     int n[3];
     int pitch;
     int per[3];
-    int np[3];              // CPML cells per end per axis
-    int idx16;
-    R C;
-    R* E[2][3];
+    int idxw;               // material index width in bytes: 1, 2 or 4
+    R C;                    // courant number
+    R* E[2][3];             // ping-pong
     R* H[2][3];
     const void* idx[3];     // material index of Ex, Ey, Ez
-    const R* lutc;          // C / eps
-    const double* lute;
-    // CPML profiles per axis: integer (E derivative) and half (H derivative)
+    const R* lutc;          // C / eps per material index
+    const double* lute;     // eps per material index
+    // CPML per axis q: (b, a, 1/kappa) at integer (E-derivative) and half
+    // (H-derivative) positions, n[q] entries each; slab index per coordinate
+    // (-1 outside the absorbing layer)
     const R* pmlI[3];
     const R* pmlH[3];
-    // psi per (component c, derivative axis q), compact along q:
-    // index [k][j][i] with the q coordinate replaced by its slab index
+    const int* slabI[3];
+    const int* slabH[3];
+    int nslabI[3], nslabH[3];
+    // psi of (component c, derivative axis q != c), compact along q, ping-pong
     R* psiE[2][3][3];
     R* psiH[2][3][3];
-    int nslabI[3], nslabH[3];
-    const int* slabI[3];    // slab index per coordinate along axis q, -1 outside
-    const int* slabH[3];
-    // source plane (axis sa, index ss): profiles Na x Nb (a fastest)
+    // TF/SF plane normal to axis sa at index ss (a = sa+1, b = sa+2 cyclic):
+    // H_a[ss-1] += sHa*gE, H_b[ss-1] += sHb*gE, E_a[ss] += sEa*gH, E_b[ss] += sEb*gH
     int sa, ss, na, nb;
-    const R* sEa;           // C * Ea * (per-E coefficient folded in at use)
-    const R* sEb;
-    const R* sHa;
-    const R* sHb;
+    const R* sHa;           // -C * Eb profile
+    const R* sHb;           // +C * Ea profile
+    const R* sEa;           // +(C/eps_a) * Hb profile
+    const R* sEb;           // -(C/eps_b) * Ha profile
     const double* gE;
     const double* gH;
     long long nsrc;
     int nmon;
-    int sstride;
+    int sstride;            // samples per step
     int mon_axis[kMaxMon];
     int mon_index[kMaxMon];
-    int mon_off[kMaxMon];   // offset of the monitor's 4 planes in one step's samples
+    int mon_off[kMaxMon];   // offset of the monitor's Ea, Eb, Ha, Hb planes in one step's samples
     R* samples;
     JobState* st;
 };
 
 struct Tile3D {
     int inst;
-    int oi0, oj0;           // output origin in x, y
-    short ow, oh;           // output extent in x, y (z is marched in full)
+    int i0, j0;             // output origin in x, y (z is marched in full)
+    short tw, th;           // output extent in x, y
 };
 
 // ------------------------------------------------------------- launchers --
@@ -213,10 +215,9 @@ cudaError_t launch_fast2d(bool fp64, bool te, bool idx16, int variant, const Fas
 int fast2d_blocks_per_sm(bool fp64, bool te, bool idx16, int variant);
 int step2d_blocks_per_sm(bool fp64, bool te, bool idx16, bool pml, int variant);
 
-cudaError_t launch_step3d(bool fp64, bool idx16, const void* insts, const Tile3D* tiles, int ntiles,
-                          int launch_off, int par, int want_energy, int grid, cudaStream_t s);
-int step3d_tile(bool fp64, int* tx, int* ty);
-int step3d_blocks_per_sm(bool fp64, bool idx16);
+constexpr int kTile3X = 32, kTile3Y = 8;   // 3D CTA tile (x, y)
+cudaError_t launch_step3d(bool fp64, int idxw, const void* insts, const Tile3D* tiles, int ntiles, int launch_off,
+                          int par, int want_energy, cudaStream_t s);
 
 cudaError_t launch_flush(bool fp64, const DftStream* streams, const FlushItem* items, int nitems,
                          cudaStream_t s);

@@ -1,8 +1,6 @@
 // temporary: 3D, batch and serving paths are added next
 #include "engine.cuh"
 namespace orf {
-int validate3d(const orf_sim3d*) { return ORF_OK; }
-int make_job3d(orf_ctx*, const orf_sim3d*, orf_job** out) { *out = nullptr; set_error("3D engine not built yet"); return ORF_EINVAL; }
 int batch2d_run(orf_ctx*, int, const orf_sim2d*, orf_out2d*, orf_progress_fn, void*) { set_error("batch not built yet"); return ORF_EINVAL; }
 }
 extern "C" {

@@ -97,3 +97,44 @@ def mixed_te_sim(nx=150, nz=90, steps=400, precision="double", seed=0, pol="TE",
         sim["epsX"], sim["epsZ"] = e["x"], e["z"]
     sim["source"] = dict(ix=30, profile=prof, neff=1.8, lambda0=1.55, bw=0.25)
     return sim
+
+
+def box3d_sim(n=(28, 24, 36), axis=3, per=(False, False, False), steps=150, precision="double", seed=0,
+              npml=(6, 5, 7), mons=None):
+    """Small 3D run touching every code path: CPML or wrap per axis, a few
+    random boxes, a TF/SF plane normal to `axis` with a smooth profile, and a
+    monitor plane normal to each axis."""
+    from opticrcwafdtd_b200 import epsComponents3D
+    rng = np.random.default_rng(seed)
+    d = 0.04
+    x, y, z = (np.arange(m) * d for m in n)
+    shapes = []
+    for _ in range(4):
+        lo = [rng.uniform(0.2, m * d - 0.5) for m in n]
+        hi = [a + rng.uniform(0.1, 0.4) for a in lo]
+        shapes.append(["box", [lo[0], hi[0], lo[1], hi[1], lo[2], hi[2], rng.uniform(1.3, 2.6)]])
+    e = epsComponents3D(x, y, z, 1.0, shapes)
+    ax = axis - 1
+    a, b = (ax + 1) % 3, (ax + 2) % 3
+    ca = np.arange(n[a]) * d
+    cb = np.arange(n[b]) * d
+    prof = np.exp(-((ca[:, None] - ca.mean()) / (0.3 * n[a] * d)) ** 2 - ((cb[None, :] - cb.mean()) / (0.3 * n[b] * d)) ** 2)
+    np_ = [0 if per[q] else npml[q] for q in range(3)]
+    src = dict(axis=axis, index=np_[ax] + 3, Ea=prof, Eb=0.3 * prof, Ha=-0.2 * prof, Hb=1.2 * prof, neff=1.2,
+               lambda0=0.6, bw=0.3)
+    if mons is None:
+        mons = [dict(axis=q + 1, index=np_[q] + 5 + (2 if q == ax else 0)) for q in range(3)]
+        mons.append(dict(axis=axis, index=n[ax] - np_[ax] - 3))
+    S = 0.99 / np.sqrt(3) * d
+    return dict(x=x, y=y, z=z, eps=e, npml=list(np_), periodic=list(per), source=src, monitors=mons,
+                lambdas=[0.55, 0.6, 0.65], maxTime=steps * S, shutoff=0.0, precision=precision)
+
+
+def plane_wave_3d(x, y, z, d, lam, lambda0, bw, zSrc, zR, zT):
+    """TestFDTD3D.planeWaveSim (tests/TestFDTD3D.m:179-189)."""
+    izOf = lambda zz: int(round((zz - z[0]) / d)) + 1
+    Na, Nb = x.size, y.size
+    src = dict(axis=3, index=izOf(zSrc), Ea=np.ones((Na, Nb)), Eb=np.zeros((Na, Nb)), Ha=np.zeros((Na, Nb)),
+               Hb=np.ones((Na, Nb)), neff=1, lambda0=lambda0, bw=bw)
+    return dict(x=x, y=y, z=z, npml=[0, 0, round(0.3 / d)], periodic=[True, True, False], source=src,
+                lambdas=lam, monitors=[dict(axis=3, index=izOf(zR)), dict(axis=3, index=izOf(zT))])

@@ -135,3 +135,24 @@ def test_pulse_definition():
         u = (t - 5 * tau) / tau
         assert abs(oracle.pulse(lam, bw, t) - np.exp(-u * u) * np.sin(k0 * (t - 5 * tau))) < 1e-15
     assert oracle.pulse(lam, bw, -1.0) == 0.0 and oracle.pulse(lam, bw, 10.01 * tau) == 0.0
+
+
+def test_3d_slab_matches_tmm_oracle():
+    # tests/TestFDTD3D.m:216-228 on the oracle
+    from opticrcwafdtd_b200 import epsComponents3D
+    d = 0.01
+    x = np.arange(2) * d
+    y = x.copy()
+    z = np.round(np.arange(0, 6 + d / 2, d), 12)
+    lam = np.linspace(1.2, 1.8, 7)
+    sim = cases.plane_wave_3d(x, y, z, d, lam, 1.5, 0.3, 1, 0.6, 5)
+    sim["eps"] = epsComponents3D(x, y, z, 1, [])
+    o0 = oracle.fdtd3D(sim)
+    sim["eps"] = epsComponents3D(x, y, z, 1, [["box", [-np.inf, np.inf, -np.inf, np.inf, 3, 3.5, 2]]])
+    o1 = oracle.fdtd3D(sim)
+    R = -o1["flux"][0] / o0["flux"][1]
+    T = o1["flux"][1] / o0["flux"][1]
+    tm = oracle.tmm(lam, [1, 2, 1], [0.5], 0, "s")
+    assert np.max(np.abs(R - tm["R"].ravel())) < 2e-3
+    assert np.max(np.abs(R + T - 1)) < 2e-5
+    assert np.max(np.abs(o0["flux"][0] / o0["flux"][1])) < 1e-8
