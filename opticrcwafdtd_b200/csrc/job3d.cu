@@ -4,8 +4,8 @@
 // into material indices (uint8/16/32) plus a table of C/eps (exact), build the
 // CPML profiles and slab maps of every axis, the TF/SF plane tables, the DFT
 // streams of the monitor planes (Ea, Eb, Ha, Hb) and the column tiles, and
-// upload everything into one device arena.  One z-marching launch advances
-// one step; the shared ChunkEngine runs the loop.
+// upload everything into one device arena.  A time step is the in-place H
+// then E half-step kernel (step3d.cu); the shared ChunkEngine runs the loop.
 #include <algorithm>
 #include <unordered_map>
 
@@ -64,7 +64,7 @@ template <class R>
 struct Job3D : orf_job {
     int n[3] = {0, 0, 0};
     bool per[3] = {false, false, false};
-    int pitch = 0, nM = 0, nL = 0, idxw = 1;
+    int pitch = 0, nM = 0, nL = 0, idxw = 1, zc = 4;
     double d = 0, Cc = 0, S = 0, src_end = 0, shutoff = 0;
     int64_t nmax = 0, nsrc = 0, enq_steps = 0;
     Arena arena;
@@ -72,8 +72,9 @@ struct Job3D : orf_job {
     Inst3D<R>* d_inst = nullptr;
     JobState* d_st = nullptr;
     JobState** d_states = nullptr;
-    std::vector<Tile3D> tiles;
+    std::vector<Tile3D> tiles, tiles_pml;   // interior / CPML tiles
     Tile3D* d_tiles = nullptr;
+    Tile3D* d_tiles_pml = nullptr;
     DftStream* d_streams = nullptr;
     std::vector<DftStream> host_streams;
     FlushItem* d_items = nullptr;
@@ -249,35 +250,49 @@ int Job3D<R>::create(const orf_sim3d* s) {
         pairs.push_back({4 * m, 4 * m + 3, 4 * m + 1, 4 * m + 2, m, nM, 0.5 * d * d});
     npairs = (int)pairs.size();
 
-    // ---- tiles: kTile3X x kTile3Y columns, full z
+    // ---- tiles: kTile3X x kTile3Y columns, zc planes each; a tile is "CPML" if
+    // any cell lies within one cell of an absorbing slab along any axis
     tiles.clear();
-    for (int j0 = 0; j0 < n[1]; j0 += kTile3Y)
-        for (int i0 = 0; i0 < n[0]; i0 += kTile3X) {
-            Tile3D t;
-            t.inst = 0;
-            t.i0 = i0;
-            t.j0 = j0;
-            t.tw = (short)std::min(kTile3X, n[0] - i0);
-            t.th = (short)std::min(kTile3Y, n[1] - j0);
-            tiles.push_back(t);
-        }
+    tiles_pml.clear();
+    auto near_pml = [&](int q, int lo, int hi) {   // cells [lo, hi) along axis q
+        const int np = per[q] ? 0 : s->npml[q];
+        if (np <= 0) return false;
+        return lo < np + 1 || hi > n[q] - np - 2;
+    };
+    zc = ctx->tuning.variant == 2 ? 8 : 4;   // planes per thread (compiled unroll depths)
+    for (int k0 = 0; k0 < n[2]; k0 += zc)
+        for (int j0 = 0; j0 < n[1]; j0 += kTile3Y)
+            for (int i0 = 0; i0 < n[0]; i0 += kTile3X) {
+                Tile3D t;
+                t.inst = 0;
+                t.i0 = i0;
+                t.j0 = j0;
+                t.tw = (short)std::min(kTile3X, n[0] - i0);
+                t.th = (short)std::min(kTile3Y, n[1] - j0);
+                t.k0 = k0;
+                t.k1 = std::min(n[2], k0 + zc);
+                const bool pm = near_pml(0, t.i0, t.i0 + t.tw) || near_pml(1, t.j0, t.j0 + t.th) ||
+                                near_pml(2, t.k0, t.k1);
+                (pm ? tiles_pml : tiles).push_back(t);
+            }
 
     // ---- device arena
+    // the H and E half-step kernels update in place: one buffer (index 0)
     Arena ar;
-    for (int b = 0; b < 2; ++b)
-        for (int c = 0; c < 3; ++c) {
-            ar.add(&h.E[b][c], NP());
-            ar.add(&h.H[b][c], NP());
-        }
-    for (int b = 0; b < 2; ++b)
-        for (int c = 0; c < 3; ++c)
-            for (int q = 0; q < 3; ++q) {
+    for (int c = 0; c < 3; ++c) {
+        ar.add(&h.E[0][c], NP());
+        ar.add(&h.H[0][c], NP());
+    }
+    for (int c = 0; c < 3; ++c)
+        for (int q = 0; q < 3; ++q) {
+            for (int b = 0; b < 2; ++b) {
                 h.psiE[b][c][q] = nullptr;
                 h.psiH[b][c][q] = nullptr;
-                if (q == c) continue;
-                if (nsI[q] > 0) ar.add(&h.psiE[b][c][q], N() / n[q] * nsI[q]);
-                if (nsH[q] > 0) ar.add(&h.psiH[b][c][q], N() / n[q] * nsH[q]);
             }
+            if (q == c) continue;
+            if (nsI[q] > 0) ar.add(&h.psiE[0][c][q], N() / n[q] * nsI[q]);
+            if (nsH[q] > 0) ar.add(&h.psiH[0][c][q], N() / n[q] * nsH[q]);
+        }
     unsigned char* d_ix[3];
     for (int c = 0; c < 3; ++c) ar.add(&d_ix[c], NP() * idxw);
     R *d_lutc, *d_pI[3], *d_pH[3], *d_sHa, *d_sHb, *d_sEa, *d_sEb, *d_samples;
@@ -311,7 +326,8 @@ int Job3D<R>::create(const orf_sim3d* s) {
     ar.add(&d_inst, 1);
     ar.add(&d_st, 1);
     ar.add(&d_states, 1);
-    ar.add(&d_tiles, tiles.size());
+    ar.add(&d_tiles, tiles.size() + 1);
+    ar.add(&d_tiles_pml, tiles_pml.size() + 1);
     ar.add(&d_streams, nstreams + 1);
     ar.add(&d_items, nitems + 1);
     ar.add(&d_pairs, npairs + 1);
@@ -361,9 +377,14 @@ int Job3D<R>::create(const orf_sim3d* s) {
     for (int l = 0; l < nL; ++l) om[l] = 2.0 * kPi / s->lambdas[l];
     ORF_TRY(up(d_omega, om.data(), nL * sizeof(double)));
 
+    for (int c = 0; c < 3; ++c) {
+        h.E[1][c] = h.E[0][c];
+        h.H[1][c] = h.H[0][c];
+    }
     for (int q = 0; q < 3; ++q) {
         h.n[q] = n[q];
         h.per[q] = per[q] ? 1 : 0;
+        h.np[q] = per[q] ? 0 : s->npml[q];
         h.pmlI[q] = d_pI[q];
         h.pmlH[q] = d_pH[q];
         h.slabI[q] = d_slI[q];
@@ -391,6 +412,7 @@ int Job3D<R>::create(const orf_sim3d* s) {
     h.st = d_st;
     ORF_TRY(up(d_inst, &h, sizeof(h)));
     ORF_TRY(up(d_tiles, tiles.data(), tiles.size() * sizeof(Tile3D)));
+    ORF_TRY(up(d_tiles_pml, tiles_pml.data(), tiles_pml.size() * sizeof(Tile3D)));
     std::vector<DftStream> hs(nstreams);
     size_t aoff = 0;
     for (int q = 0; q < nstreams; ++q) {
@@ -425,9 +447,15 @@ int Job3D<R>::create(const orf_sim3d* s) {
     const int64_t ncell = (int64_t)N();
     eng.step = [this, ncell](int off, int nsub, int par, int we, cudaStream_t stream, KernelTimer* tm) -> cudaError_t {
         (void)nsub;
+        (void)par;
         cudaEvent_t a = nullptr;
         if (tm && tm->begin(stream, &a) != ORF_OK) return cudaErrorUnknown;
-        cudaError_t e = launch_step3d(sizeof(R) == 8, idxw, d_inst, d_tiles, (int)tiles.size(), off, par, we, stream);
+        const bool f64 = sizeof(R) == 8;
+        cudaError_t e = launch_h3d(f64, zc, false, d_inst, d_tiles, (int)tiles.size(), off, stream);
+        if (e == cudaSuccess) e = launch_h3d(f64, zc, true, d_inst, d_tiles_pml, (int)tiles_pml.size(), off, stream);
+        if (e == cudaSuccess) e = launch_e3d(f64, zc, false, idxw, d_inst, d_tiles, (int)tiles.size(), off, we, stream);
+        if (e == cudaSuccess)
+            e = launch_e3d(f64, zc, true, idxw, d_inst, d_tiles_pml, (int)tiles_pml.size(), off, we, stream);
         if (e != cudaSuccess) return e;
         if (tm && tm->end(stream, 0, ncell, a) != ORF_OK) return cudaErrorUnknown;
         return e;
@@ -465,15 +493,14 @@ template <class R>
 int Job3D<R>::reset() {
     cudaStream_t st = ctx->stream;
     ORF_CUDA(cudaStreamSynchronize(st));
-    for (int b = 0; b < 2; ++b)
-        for (int c = 0; c < 3; ++c) {
-            ORF_CUDA(cudaMemsetAsync(h.E[b][c], 0, NP() * sizeof(R), st));
-            ORF_CUDA(cudaMemsetAsync(h.H[b][c], 0, NP() * sizeof(R), st));
-            for (int q = 0; q < 3; ++q) {
-                if (h.psiE[b][c][q]) ORF_CUDA(cudaMemsetAsync(h.psiE[b][c][q], 0, N() / n[q] * h.nslabI[q] * sizeof(R), st));
-                if (h.psiH[b][c][q]) ORF_CUDA(cudaMemsetAsync(h.psiH[b][c][q], 0, N() / n[q] * h.nslabH[q] * sizeof(R), st));
-            }
+    for (int c = 0; c < 3; ++c) {
+        ORF_CUDA(cudaMemsetAsync(h.E[0][c], 0, NP() * sizeof(R), st));
+        ORF_CUDA(cudaMemsetAsync(h.H[0][c], 0, NP() * sizeof(R), st));
+        for (int q = 0; q < 3; ++q) {
+            if (h.psiE[0][c][q]) ORF_CUDA(cudaMemsetAsync(h.psiE[0][c][q], 0, N() / n[q] * h.nslabI[q] * sizeof(R), st));
+            if (h.psiH[0][c][q]) ORF_CUDA(cudaMemsetAsync(h.psiH[0][c][q], 0, N() / n[q] * h.nslabH[q] * sizeof(R), st));
         }
+    }
     size_t acc_elems = 0;
     for (auto& q : host_streams) acc_elems += (size_t)q.len * nL;
     ORF_CUDA(cudaMemsetAsync(d_acc, 0, acc_elems * 16, st));
@@ -545,7 +572,8 @@ int Job3D<R>::get_fields(double* const* f, int nf) {
     ORF_CUDA(cudaStreamSynchronize(ctx->stream));
     JobState js;
     ORF_CUDA(cudaMemcpy(&js, d_st, sizeof js, cudaMemcpyDeviceToHost));
-    const int b = js.cur;
+    const int b = 0;   // in-place update: one buffer
+    (void)js;
     std::vector<R> tmp(NP());
     for (int q = 0; q < 6; ++q) {
         if (!f[q]) continue;

@@ -147,6 +147,7 @@ struct Inst3D {
     int n[3];
     int pitch;
     int per[3];
+    int np[3];              // CPML cells per end per axis (0 on periodic axes)
     int idxw;               // material index width in bytes: 1, 2 or 4
     R C;                    // courant number
     R* E[2][3];             // ping-pong
@@ -186,8 +187,9 @@ struct Inst3D {
 
 struct Tile3D {
     int inst;
-    int i0, j0;             // output origin in x, y (z is marched in full)
-    short tw, th;           // output extent in x, y
+    int i0, j0;             // column origin in x, y
+    short tw, th;           // extent in x, y (<= kTile3X x kTile3Y)
+    int k0, k1;             // z planes [k0, k1) marched by the CTA
 };
 
 // ------------------------------------------------------------- launchers --
@@ -216,8 +218,13 @@ int fast2d_blocks_per_sm(bool fp64, bool te, bool idx16, int variant);
 int step2d_blocks_per_sm(bool fp64, bool te, bool idx16, bool pml, int variant);
 
 constexpr int kTile3X = 32, kTile3Y = 8;   // 3D CTA tile (x, y)
-cudaError_t launch_step3d(bool fp64, int idxw, const void* insts, const Tile3D* tiles, int ntiles, int launch_off,
-                          int par, int want_energy, cudaStream_t s);
+// H then E half step of one time step (in place).  zc = planes per thread (a
+// compiled unroll depth: 4 or 8); tiles span <= zc planes.  pml = false only
+// for tiles with no cell near a CPML slab.
+cudaError_t launch_h3d(bool fp64, int zc, bool pml, const void* insts, const Tile3D* tiles, int ntiles,
+                       int launch_off, cudaStream_t s);
+cudaError_t launch_e3d(bool fp64, int zc, bool pml, int idxw, const void* insts, const Tile3D* tiles, int ntiles,
+                       int launch_off, int want_energy, cudaStream_t s);
 
 cudaError_t launch_flush(bool fp64, const DftStream* streams, const FlushItem* items, int nitems,
                          cudaStream_t s);
