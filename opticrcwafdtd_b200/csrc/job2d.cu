@@ -165,10 +165,11 @@ int Job2D<R>::create(const orf_sim2d* s) {
 
     // ---- tiles
     ORF_TRY(pick_tiling(npx, npz));
-    int fast_wx = 1;
+    int lx_int = 32, lx_pml = 32;
     {
         Variant2D fv;
-        if (fast2d_info(fvariant, sizeof(R) == 8, &fv)) fast_wx = fv.wx;
+        if (fast2d_info(fvariant, sizeof(R) == 8, false, &fv)) lx_int = fv.lx();
+        if (fast2d_info(0, sizeof(R) == 8, true, &fv)) lx_pml = fv.lx();
     }
 
     // ---- DFT streams: x monitors (P, B lines), z monitors (P, A lines)
@@ -232,9 +233,7 @@ int Job2D<R>::create(const orf_sim2d* s) {
     ar.add(&d_inst, 1);
     ar.add(&d_st, 1);
     ar.add(&d_states, 1);
-    ar.add(&d_tint, tiles_int.size() + 1);
     ar.add(&d_ftiles, ftiles_host.size() + 1);
-    ar.add(&d_tpml, tiles_pml.size() + 1);
     ar.add(&d_streams, nstreams + 1);
     ar.add(&d_items, nitems + 1);
     ar.add(&d_pairs, npairs + 1);
@@ -305,8 +304,9 @@ int Job2D<R>::create(const orf_sim2d* s) {
     h.samples = d_samples;
     h.st = d_st;
     ORF_TRY(up(d_inst, &h, sizeof(h)));
-    ORF_TRY(up(d_tint, tiles_int.data(), tiles_int.size() * sizeof(Tile2D)));
-    for (auto& t : ftiles_host) {
+    for (size_t q = 0; q < ftiles_host.size(); ++q) {
+        FastTile2D& t = ftiles_host[q];
+        const int lxt = (int)q < nfast ? lx_int : lx_pml;
         for (int b = 0; b < 2; ++b) {
             t.f[b][0] = h.P[b];
             t.f[b][1] = h.A[b];
@@ -317,14 +317,13 @@ int Job2D<R>::create(const orf_sim2d* s) {
         t.st = d_st;
         t.inst = d_inst;
         t.flags = 0;
-        if ((sx - 1 >= t.li0 && sx - 1 < t.li0 + 32 * fast_wx) || (sx >= t.li0 && sx < t.li0 + 32 * fast_wx)) t.flags |= 1;
+        if ((sx - 1 >= t.li0 && sx - 1 < t.li0 + lxt) || (sx >= t.li0 && sx < t.li0 + lxt)) t.flags |= 1;
         for (int m = 0; m < nM; ++m)
             if (s->monitors[m] >= t.oi0 && s->monitors[m] < t.oi0 + t.ow) t.flags |= 2;
         for (int m = 0; m < nMZ; ++m)
             if (s->monitors_z[m] >= t.ok0 && s->monitors_z[m] < t.ok0 + t.oh) t.flags |= 4;
     }
     ORF_TRY(up(d_ftiles, ftiles_host.data(), ftiles_host.size() * sizeof(FastTile2D)));
-    ORF_TRY(up(d_tpml, tiles_pml.data(), tiles_pml.size() * sizeof(Tile2D)));
     std::vector<DftStream> hs(nstreams);
     size_t aoff = 0;
     for (int q = 0; q < nstreams; ++q) {
@@ -357,23 +356,22 @@ int Job2D<R>::create(const orf_sim2d* s) {
     eng.d_states = d_states;
     eng.nstates = 1;
     int64_t interior_cells = 0;
-    for (auto& t : ftiles_host) interior_cells += (int64_t)t.ow * t.oh;
+    for (int q = 0; q < nfast; ++q) interior_cells += (int64_t)ftiles_host[q].ow * ftiles_host[q].oh;
     eng.step = [this, interior_cells](int off, int nsub, int par, int we, cudaStream_t stream,
                                       KernelTimer* tm) -> cudaError_t {
         const bool f64 = sizeof(R) == 8;
         cudaError_t e = cudaSuccess;
         cudaEvent_t a = nullptr;
-        if (!ftiles_host.empty()) {
+        if (nfast) {
             if (tm && tm->begin(stream, &a) != ORF_OK) return cudaErrorUnknown;
-            e = launch_fast2d(f64, te, idx16, fvariant, d_ftiles, (int)ftiles_host.size(), off, nsub, par, we,
-                              grid_fast, stream);
+            e = launch_fast2d(f64, te, idx16, false, fvariant, d_ftiles, nfast, off, nsub, par, we, grid_fast, stream);
             if (e != cudaSuccess) return e;
             if (tm && tm->end(stream, 0, interior_cells * nsub, a) != ORF_OK) return cudaErrorUnknown;
         }
-        if (!tiles_pml.empty()) {
+        if (nframe) {
             if (tm && tm->begin(stream, &a) != ORF_OK) return cudaErrorUnknown;
-            e = launch_step2d(f64, te, idx16, true, variant, d_inst, d_tpml, (int)tiles_pml.size(), T, off,
-                              nsub, par, we, grid_pml, stream);
+            e = launch_fast2d(f64, te, idx16, true, 0, d_ftiles + nfast, nframe, off, nsub, par, we, grid_frame,
+                              stream);
             if (e != cudaSuccess) return e;
             if (tm && tm->end(stream, 1, ((int64_t)nx * nz - interior_cells) * nsub, a) != ORF_OK)
                 return cudaErrorUnknown;
@@ -387,19 +385,16 @@ int Job2D<R>::create(const orf_sim2d* s) {
 template <class R>
 int Job2D<R>::pick_tiling(int npx, int npz) {
     const bool f64 = sizeof(R) == 8;
-    // interior tiles: pipelined kernel; CPML / boundary frame: masked kernel
     fvariant = ctx->tuning.variant > 0 ? ctx->tuning.variant : 1;
-    Variant2D fv, bv;
-    if (!fast2d_info(fvariant, f64, &fv)) {
+    Variant2D fv, pv;
+    if (!fast2d_info(fvariant, f64, false, &fv)) {
         set_error("unknown 2D kernel variant %d", fvariant);
         return ORF_EINVAL;
     }
-    // frame strips (npml + T cells wide) use the 128 x 32 / 64 x 32 geometry
-    // (measured faster than 64 x 64 on the config-2 grid)
-    variant = 2;
-    variant2d_info(variant, f64, &bv);
-    const int tmax = std::min({kMaxSub, (bv.lz() - 1) / 2, (bv.lx() - 1) / 2, (fv.lz() - 1) / 2, (fv.lx() - 4) / 2});
-    T = ctx->tuning.tsteps > 0 ? ctx->tuning.tsteps : (f64 ? 6 : 6);
+    fast2d_info(0, f64, true, &pv);
+    // a tile's output keeps T cells (plus up to 3 of x alignment) from its edges
+    const int tmax = std::min({kMaxSub, (pv.lz() - 1) / 2, (pv.lx() - 4) / 2, (fv.lz() - 1) / 2, (fv.lx() - 4) / 2});
+    T = ctx->tuning.tsteps > 0 ? ctx->tuning.tsteps : 6;
     if (T > tmax) T = tmax;
     if (T < 1) T = 1;
 
@@ -411,61 +406,55 @@ int Job2D<R>::pick_tiling(int npx, int npz) {
     int ax = npx + T, bx = nx - npx - T;
     int az = per ? 0 : npz + T, bz = per ? nz : nz - npz - T;
     if (bx - ax < 8 || bz - az < 4) { ax = bx = 0; az = bz = 0; }   // everything is frame
-    ftiles_host.clear();
-    tiles_pml.clear();
-    tiles_int.clear();
-    const int FX = fv.lx(), FZ = fv.lz();
-    for (int ok0 = az; ok0 < bz;) {
-        const int oh = std::min(FZ - 2 * T, bz - ok0);
-        for (int oi0 = ax; oi0 < bx;) {
-            const int li0 = ((oi0 - T) / 4) * 4;   // oi0 - T >= cl - 1 >= 0
-            const int ow = std::min(li0 + FX - T - oi0, bx - oi0);
-            FastTile2D t{};
-            t.pitch = pitch;
-            t.nz = nz;
-            t.periodic = per ? 1 : 0;
-            t.li0 = li0;
-            t.lk0 = ok0 - T;
-            t.oi0 = oi0;
-            t.ok0 = ok0;
-            t.ow = ow;
-            t.oh = oh;
-            ftiles_host.push_back(t);
-            oi0 += ow;
-        }
-        ok0 += oh;
-    }
-    // frame strips: bottom, top (full width), left, right (between az and bz)
-    const int OX = bv.lx() - 2 * T, OZ = bv.lz() - 2 * T;
-    auto strip = [&](int x0, int x1, int z0, int z1) {
-        for (int ok0 = z0; ok0 < z1; ok0 += OZ)
-            for (int oi0 = x0; oi0 < x1; oi0 += OX) {
-                Tile2D t;
-                t.inst = 0;
+    std::vector<FastTile2D> inner, frame;
+    // tile the rectangle [x0,x1) x [z0,z1) with a geometry of LX x LZ cells;
+    // the loaded origin li0 is rounded down to a multiple of 4 cells
+    auto tile_rect = [&](std::vector<FastTile2D>& out, const Variant2D& v, int x0, int x1, int z0, int z1) {
+        for (int ok0 = z0; ok0 < z1;) {
+            const int oh = std::min(v.lz() - 2 * T, z1 - ok0);
+            for (int oi0 = x0; oi0 < x1;) {
+                const int a = oi0 - T;
+                const int li0 = a - ((a % 4) + 4) % 4;
+                const int ow = std::min(li0 + v.lx() - T - oi0, x1 - oi0);
+                FastTile2D t{};
+                t.pitch = pitch;
+                t.nz = nz;
+                t.nx = nx;
+                t.periodic = per ? 1 : 0;
+                t.li0 = li0;
+                t.lk0 = ok0 - T;
                 t.oi0 = oi0;
                 t.ok0 = ok0;
-                t.ow = (short)std::min(OX, x1 - oi0);
-                t.oh = (short)std::min(OZ, z1 - ok0);
-                tiles_pml.push_back(t);
+                t.ow = ow;
+                t.oh = oh;
+                out.push_back(t);
+                oi0 += ow;
             }
+            ok0 += oh;
+        }
     };
     if (bx > ax) {
-        strip(0, nx, 0, az);
-        strip(0, nx, bz, nz);
-        strip(0, ax, az, bz);
-        strip(bx, nx, az, bz);
+        tile_rect(inner, fv, ax, bx, az, bz);
+        tile_rect(frame, pv, 0, nx, 0, az);
+        tile_rect(frame, pv, 0, nx, bz, nz);
+        tile_rect(frame, pv, 0, ax, az, bz);
+        tile_rect(frame, pv, bx, nx, az, bz);
     } else {
-        strip(0, nx, 0, nz);
+        tile_rect(frame, pv, 0, nx, 0, nz);
     }
-    const int bps_f = ftiles_host.empty() ? 1 : fast2d_blocks_per_sm(f64, te, idx16, fvariant);
-    const int bps_p = step2d_blocks_per_sm(f64, te, idx16, true, variant);
+    nfast = (int)inner.size();
+    nframe = (int)frame.size();
+    ftiles_host = inner;
+    ftiles_host.insert(ftiles_host.end(), frame.begin(), frame.end());
+    const int bps_f = nfast ? fast2d_blocks_per_sm(f64, te, idx16, false, fvariant) : 1;
+    const int bps_p = nframe ? fast2d_blocks_per_sm(f64, te, idx16, true, 0) : 1;
     if (bps_f < 1 || bps_p < 1) {
         set_error("2D kernel variant %d cannot be resident on this device (%s)", fvariant,
                   cudaGetErrorString(cudaGetLastError()));
         return ORF_ECUDA;
     }
-    grid_fast = (int)std::min<size_t>(ftiles_host.size(), (size_t)ctx->sm_count * bps_f);
-    grid_pml = (int)std::min<size_t>(tiles_pml.size(), (size_t)ctx->sm_count * bps_p);
+    grid_fast = (int)std::min<size_t>(nfast, (size_t)ctx->sm_count * bps_f);
+    grid_frame = (int)std::min<size_t>(nframe, (size_t)ctx->sm_count * bps_p);
     return ORF_OK;
 }
 

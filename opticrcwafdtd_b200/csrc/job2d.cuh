@@ -19,12 +19,12 @@ struct Job2D : orf_job {
     Inst2D<R>* d_inst = nullptr;
     JobState* d_st = nullptr;
     JobState** d_states = nullptr;
-    Tile2D* d_tint = nullptr;
-    Tile2D* d_tpml = nullptr;
-    std::vector<Tile2D> tiles_int, tiles_pml;
+    // interior tiles (pipelined kernel without CPML) and frame tiles (CPML /
+    // boundary instantiation), one descriptor array: [interior | frame]
     std::vector<FastTile2D> ftiles_host;
+    int nfast = 0, nframe = 0;
     FastTile2D* d_ftiles = nullptr;
-    int variant = 2, fvariant = 1, T = 1, grid_int = 0, grid_pml = 0, grid_fast = 0;
+    int fvariant = 1, T = 1, grid_fast = 0, grid_frame = 0;
     DftStream* d_streams = nullptr;
     std::vector<DftStream> host_streams;
     FlushItem* d_items = nullptr;

@@ -116,13 +116,7 @@ struct Inst2D {
     JobState* st;
 };
 
-struct Tile2D {
-    int inst;
-    int oi0, ok0;           // output origin (global cell coordinates)
-    short ow, oh;           // output extent
-};
-
-// Self-contained descriptor of an interior tile for the pipelined kernel
+// Self-contained descriptor of a tile for the pipelined kernel
 // (step2d_fast.cuh): everything its prefetch needs, 128 bytes, copied into
 // shared memory with cp.async two tiles ahead.
 struct alignas(16) FastTile2D {
@@ -130,12 +124,13 @@ struct alignas(16) FastTile2D {
     const void* idx0;
     const void* idx1;
     JobState* st;
-    const void* inst;       // Inst2D<R>* (source, monitors, tables)
+    const void* inst;       // Inst2D<R>* (source, monitors, tables, CPML state)
     int pitch, nz, periodic;
-    int li0, lk0;           // loaded origin; li0 is a multiple of 4 cells
+    int li0, lk0;           // loaded origin; li0 is a multiple of 4 cells (may be negative)
     int oi0, ok0, ow, oh;   // output rectangle
     int flags;              // 1: TF/SF plane in the loaded columns, 2: x monitor, 4: z monitor
-    int pad[2];
+    int nx;
+    int pad;
 };
 static_assert(sizeof(FastTile2D) == 128, "FastTile2D must stay 128 bytes");
 
@@ -200,21 +195,14 @@ struct Variant2D {
     int lx() const { return 32 * wx; }
     int lz() const { return ks * wz; }
 };
-
-// Returns the tile geometry of a compiled 2D variant (false if id unknown).
-bool variant2d_info(int id, bool fp64, Variant2D* v);
 int variant2d_count();
 
-cudaError_t launch_step2d(bool fp64, bool te, bool idx16, bool pml, int variant, const void* insts,
-                          const Tile2D* tiles, int ntiles, int halo, int launch_off, int nsub,
-                          int par, int want_energy, int grid, cudaStream_t s);
-size_t step2d_smem(bool fp64, bool te, bool pml, int variant);
-
-// Pipelined interior kernel (step2d_fast.cuh).
-bool fast2d_info(int id, bool fp64, Variant2D* v);
-cudaError_t launch_fast2d(bool fp64, bool te, bool idx16, int variant, const FastTile2D* tiles, int ntiles,
+// Pipelined kernel (step2d_fast.cuh).  pml = false: interior tiles (no CPML
+// or boundary cell in reach); pml = true: CPML / boundary tiles.
+bool fast2d_info(int id, bool fp64, bool pml, Variant2D* v);
+cudaError_t launch_fast2d(bool fp64, bool te, bool idx16, bool pml, int variant, const FastTile2D* tiles, int ntiles,
                           int launch_off, int nsub, int par, int want_energy, int grid, cudaStream_t s);
-int fast2d_blocks_per_sm(bool fp64, bool te, bool idx16, int variant);
+int fast2d_blocks_per_sm(bool fp64, bool te, bool idx16, bool pml, int variant);
 int step2d_blocks_per_sm(bool fp64, bool te, bool idx16, bool pml, int variant);
 
 constexpr int kTile3X = 32, kTile3Y = 8;   // 3D CTA tile (x, y)

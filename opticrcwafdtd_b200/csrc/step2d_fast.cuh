@@ -1,18 +1,30 @@
-// step2d_fast.cuh -- pipelined interior 2D Yee step kernel for sm_100a.
+// step2d_fast.cuh -- pipelined, temporally blocked 2D Yee step kernel (sm_100a).
 //
-// Same update as step2d_impl.cuh (toolbox/+orf/fdtd2D.m:3-7 P/A/B form, with
-// the TF/SF corrections and DFT sampling of fdtd2DTE.m:11-18), for tiles whose
-// whole dependency cone lies outside the CPML and inside the grid ("interior"
-// tiles): no psi state and no boundary masks.
+// Replaces the time loop of toolbox/+orf/fdtd2D.m:3-7 (P/A/B form):
+//   A += cA dP/dz,  B -= cB dP/dx,  P += cP (dA/dz - dB/dx)
+// with CPML (cpmlCoefficients.m:4-8), the one-sided TF/SF plane
+// (fdtd2DTE.m:11-15, fdtd2D.m:21-23) and DFT sampling of the monitor lines
+// (fdtd2DTE.m:16-18), advancing up to T time steps per launch.
 //
-// Persistent CTA, software-pipelined over its tiles:
-//   wait for tile t in shared memory -> move it to registers (fields) and to
-//   a coefficient plane (material index -> C/eps through the table) ->
-//   issue the cp.async prefetch of tile t+1 into the same shared buffer ->
-//   run the T fused time steps of tile t from registers -> store its output.
-// The prefetch of tile t+1 and the descriptor/state loads of tile t+2 are in
-// flight while tile t computes, so the DRAM latency that bounded the simple
-// kernel is hidden behind the stencil arithmetic.
+// Layout and work split:
+//   - a CTA owns a tile of LX = 32*WX columns by LZ = KS*WZ rows; each thread
+//     keeps a vertical strip of KS cells of P, A and B in registers for the
+//     whole launch, so the T fused steps read and write HBM once per field;
+//   - x neighbours come from warp shuffles, neighbours across warps from small
+//     shared exchange buffers (one __syncthreads per half step);
+//   - tiles overlap by T cells (trapezoidal temporal blocking): after T steps
+//     only the inner output rectangle is valid and written back; fields
+//     ping-pong between two buffers so overlapping tiles never race;
+//   - the update coefficients come from a uint8/uint16 material index and a
+//     table of C/eps (exact), expanded into a shared coefficient plane;
+//   - the CTA is persistent and software-pipelined over its tiles: while tile
+//     t computes, the cp.async prefetch of tile t+1 (fields, material index)
+//     and the descriptor and job-state snapshot of tile t+2 are in flight.
+// Two instantiations per geometry: interior tiles (PML = false: every cell of
+// the tile's dependency cone is a plain cell, no masks and no CPML code) and
+// frame tiles (PML = true: CPML psi in a shared working plane, boundary
+// masks, zero fill outside the grid).  Both perform, cell by cell, the same
+// floating-point operations, so results do not depend on the tiling.
 #pragma once
 #include "orf_internal.cuh"
 
@@ -24,33 +36,58 @@ __device__ __forceinline__ int pmod(int a, int n) {
     return r < 0 ? r + n : r;
 }
 
-__device__ __forceinline__ void cp_async4(void* sdst, const void* gsrc) {
+// cp.async of 4 / 8 bytes; when valid is false the destination is zero-filled
+// (src-size 0) and src is not read.
+__device__ __forceinline__ void cp_async4(void* sdst, const void* gsrc, bool valid = true) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gsrc) : "memory");
+    const unsigned n = valid ? 4u : 0u;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gsrc), "r"(n) : "memory");
 }
-__device__ __forceinline__ void cp_async8(void* sdst, const void* gsrc) {
+__device__ __forceinline__ void cp_async8(void* sdst, const void* gsrc, bool valid = true) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc) : "memory");
+    const unsigned n = valid ? 8u : 0u;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gsrc), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gsrc) : "memory");
 }
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 template <class R>
-__device__ __forceinline__ void cp_field(R* sdst, const R* gsrc) {
-    if constexpr (sizeof(R) == 4) cp_async4(sdst, gsrc);
-    else cp_async8(sdst, gsrc);
+__device__ __forceinline__ void cp_field(R* sdst, const R* gsrc, bool valid = true) {
+    if constexpr (sizeof(R) == 4) cp_async4(sdst, gsrc, valid);
+    else cp_async8(sdst, gsrc, valid);
 }
 
-// Dynamic shared memory of one instantiation: prefetch planes of P, A, B and
-// the material index (one or two), then the coefficient planes.
-template <class R, class IT, bool TE, int KS, int WX, int WZ>
+// compact CPML slab index (-1 outside the absorbing layer)
+__device__ __forceinline__ int slab_int(int u, int n, int np) {
+    if (np <= 0 || u < 0 || u >= n) return -1;
+    if (u < np) return u;
+    if (u >= n - np) return np + u - (n - np);
+    return -1;
+}
+__device__ __forceinline__ int slab_half(int u, int n, int np) {   // positions u+1/2, u < n-1
+    if (np <= 0 || u < 0 || u >= n - 1) return -1;
+    if (u < np) return u;
+    if (u >= n - 1 - np) return np + u - (n - 1 - np);
+    return -1;
+}
+
+// Dynamic shared memory: prefetch planes of P, A, B and the material index,
+// coefficient planes, then (PML) four psi planes and the row / column CPML
+// profiles of the tile.
+template <class R, class IT, bool TE, bool PML, int KS, int WX, int WZ>
 constexpr size_t dyn_smem() {
-    constexpr size_t cells = (size_t)32 * WX * KS * WZ;
+    constexpr size_t LX = 32 * WX, LZ = (size_t)KS * WZ, cells = LX * LZ;
     constexpr size_t idxb = ((cells * sizeof(IT) * (TE ? 1 : 2)) + 15) & ~size_t(15);
-    return cells * sizeof(R) * 3 + idxb + cells * sizeof(R) * (TE ? 1 : 2);
+    size_t b = cells * sizeof(R) * 3 + idxb + cells * sizeof(R) * (TE ? 1 : 2);
+    if (PML) b += cells * sizeof(R) * 4 + (LZ + LX) * 6 * sizeof(R);
+    return b;
 }
 
-template <class R, class IT, bool TE, int KS, int WX, int WZ>
+template <class R, class IT, bool TE, bool PML, int KS, int WX, int WZ>
 __global__ void __launch_bounds__(32 * WX * WZ, 1)
 k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, int nsub_max, int par,
               int want_energy) {
@@ -70,6 +107,12 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
     constexpr size_t idxb = ((CELLS * sizeof(IT) * NIDX) + 15) & ~size_t(15);
     R* c0s = reinterpret_cast<R*>(reinterpret_cast<unsigned char*>(pfI) + idxb);
     R* c1s = c0s + CELLS;                                // TM only
+    R* psA = c0s + (TE ? 1 : 2) * CELLS;                 // PML only: psi of A (z), B (x), P (x), P (z)
+    R* psB = psA + CELLS;
+    R* psPx = psB + CELLS;
+    R* psPz = psPx + CELLS;
+    R* prz = psPz + CELLS;                               // PML only: [LZ][6] rows: zP b,a,k ; zA b,a,k
+    R* prx = prz + LZ * 6;                               // PML only: [LX][6] cols: xP b,a,k ; xB b,a,k
 
     __shared__ R xPc[NW][KS];
     __shared__ R xPr[NW][32];
@@ -82,7 +125,7 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
     // descriptor ring (tiles t, t+G, t+2G) and snapshots of their job state,
     // both filled by cp.async so no thread waits on a dependent global load
     __shared__ __align__(16) FastTile2D s_desc[3];
-    __shared__ __align__(16) long long s_state[3][4];   // step, nmax, chunk, (done | converged << 32)
+    __shared__ __align__(16) long long s_state[3][4];   // step, nmax, chunk, done | converged << 32
 
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
@@ -96,16 +139,20 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
         const R* gP = reinterpret_cast<const R*>(d.f[par][0]);
         const R* gA = reinterpret_cast<const R*>(d.f[par][1]);
         const R* gB = reinterpret_cast<const R*>(d.f[par][2]);
-        const int col = min(d.li0 + cx, d.pitch - 1);
+        const int i = d.li0 + cx;
+        const bool cv = !PML || (i >= 0 && i < d.nx);
+        const int col = PML ? min(max(i, 0), d.nx - 1) : min(i, d.pitch - 1);
 #pragma unroll
         for (int j = 0; j < KS; ++j) {
             const int row = d.lk0 + ck0 + j;
+            const bool rv = d.periodic || (row >= 0 && row < d.nz);
             const int kk = d.periodic ? pmod(row, d.nz) : min(max(row, 0), d.nz - 1);
             const size_t off = (size_t)kk * d.pitch + col;
             const int c = (ck0 + j) * LX + cx;
-            cp_field(pfP + c, gP + off);
-            cp_field(pfA + c, gA + off);
-            cp_field(pfB + c, gB + off);
+            const bool v = !PML || (cv && rv);
+            cp_field(pfP + c, gP + off, v);
+            cp_field(pfA + c, gA + off, v);
+            cp_field(pfB + c, gB + off, v);
         }
         // material index rows: 4-byte copies (li0 and pitch are multiples of 4 cells)
         constexpr int W4 = LX * (int)sizeof(IT) / 4;
@@ -114,29 +161,30 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
             const int r = (q / W4) % LZ;
             const int c4 = q % W4;
             const int row = d.lk0 + r;
+            const bool rv = d.periodic || (row >= 0 && row < d.nz);
             const int kk = d.periodic ? pmod(row, d.nz) : min(max(row, 0), d.nz - 1);
-            size_t boff = ((size_t)kk * d.pitch + d.li0) * sizeof(IT) + 4 * (size_t)c4;
-            const size_t rowend = ((size_t)kk * d.pitch + d.pitch) * sizeof(IT);
+            const int c0 = d.li0 + 4 * c4 / (int)sizeof(IT);     // first cell of the word
+            const bool v = rv && c0 >= 0 && c0 < d.pitch;
+            const size_t base = (size_t)kk * d.pitch * sizeof(IT);
+            size_t boff = base + (size_t)max(c0, 0) * sizeof(IT);
+            const size_t rowend = base + (size_t)d.pitch * sizeof(IT);
             if (boff + 4 > rowend) boff = rowend - 4;
             const unsigned char* src = reinterpret_cast<const unsigned char*>(plane ? d.idx1 : d.idx0) + boff;
             cp_async4(reinterpret_cast<unsigned char*>(pfI) + (size_t)plane * CELLS * sizeof(IT) +
                           ((size_t)r * LX) * sizeof(IT) + 4 * (size_t)c4,
-                      src);
+                      src, v);
         }
     };
     auto fetch_desc = [&](int tile, int slot) {   // threads 0..7: 8 x 16 B
-        if (threadIdx.x < 8 && tile < ntiles) {
-            const unsigned s = (unsigned)__cvta_generic_to_shared(reinterpret_cast<char*>(&s_desc[slot]) + 16 * threadIdx.x);
-            const char* g = reinterpret_cast<const char*>(tiles + tile) + 16 * threadIdx.x;
-            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(g) : "memory");
-        }
+        if (threadIdx.x < 8 && tile < ntiles)
+            cp_async16(reinterpret_cast<char*>(&s_desc[slot]) + 16 * threadIdx.x,
+                       reinterpret_cast<const char*>(tiles + tile) + 16 * threadIdx.x);
     };
     auto fetch_state = [&](int slot) {            // threads 8..9: 2 x 16 B of JobState
         if (threadIdx.x >= 8 && threadIdx.x < 10) {
             const int q = threadIdx.x - 8;
-            const unsigned s = (unsigned)__cvta_generic_to_shared(reinterpret_cast<char*>(&s_state[slot][0]) + 16 * q);
-            const char* g = reinterpret_cast<const char*>(s_desc[slot].st) + 16 * q;
-            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(g) : "memory");
+            cp_async16(reinterpret_cast<char*>(&s_state[slot][0]) + 16 * q,
+                       reinterpret_cast<const char*>(s_desc[slot].st) + 16 * q);
         }
     };
 
@@ -184,6 +232,73 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
             sg[0][q] = n < I->nsrc ? I->gE[n] : 0.0;
             sg[1][q] = n < I->nsrc ? I->gH[n] : 0.0;
         }
+        const int i = d.li0 + cx;
+        const int kb = d.lk0 + ck0;
+        const int nz = d.nz;
+        // boundary masks (frame tiles): cells outside the grid, and the A row
+        // nz-1 / B column nx-1 that do not exist, keep zero and are not updated
+        unsigned mP = ~0u, mA = ~0u, mB = ~0u;
+        int sxP = -1, sxB = -1;
+        if (PML) {
+            const int nzA = d.periodic ? nz : nz - 1;
+            const bool cv = i >= 0 && i < d.nx, cvB = i >= 0 && i < d.nx - 1;
+            mP = mA = mB = 0;
+#pragma unroll
+            for (int j = 0; j < KS; ++j) {
+                const int k = kb + j;
+                const bool rv = d.periodic || (k >= 0 && k < nz);
+                const int kk = d.periodic ? pmod(k, nz) : k;
+                if (rv && cv) mP |= 1u << j;
+                if (rv && cv && kk < nzA) mA |= 1u << j;
+                if (rv && cvB) mB |= 1u << j;
+            }
+            // CPML state of the tile: psi planes (zero outside the slabs) and
+            // the row / column profiles (identity outside the slabs)
+            const int npx = I->npx, npz = I->npz, nx = d.nx;
+            sxP = cv ? slab_int(i, nx, npx) : -1;
+            sxB = cvB ? slab_half(i, nx, npx) : -1;
+            const R* gA = I->psiA[par];
+            const R* gB = I->psiB[par];
+            const R* gPx = I->psiPx[par];
+            const R* gPz = I->psiPz[par];
+#pragma unroll
+            for (int j = 0; j < KS; ++j) {
+                const int c = (ck0 + j) * LX + cx;
+                const int k = kb + j;
+                const int kk = d.periodic ? pmod(k, nz) : k;
+                R a = R(0), b = R(0), px = R(0), pz = R(0);
+                if ((mP >> j) & 1u) {
+                    const int szA = slab_half(kk, nz, npz);
+                    const int szP = slab_int(kk, nz, npz);
+                    if (szA >= 0) a = gA[(size_t)szA * nx + i];
+                    if (szP >= 0) pz = gPz[(size_t)szP * nx + i];
+                    if (sxP >= 0) px = gPx[(size_t)kk * (2 * npx) + sxP];
+                }
+                if (((mB >> j) & 1u) && sxB >= 0) b = gB[(size_t)kk * (2 * npx) + sxB];
+                psA[c] = a;
+                psB[c] = b;
+                psPx[c] = px;
+                psPz[c] = pz;
+            }
+            for (int q = threadIdx.x; q < LZ; q += NT) {
+                const int k = d.lk0 + q;
+                const int kk = d.periodic ? pmod(k, nz) : k;
+                const bool rv = kk >= 0 && kk < nz;
+                for (int cc = 0; cc < 3; ++cc) {
+                    const R id = R(cc == 1 ? 0 : 1);
+                    prz[q * 6 + cc] = rv ? I->pmlz[3 * kk + cc] : id;
+                    prz[q * 6 + 3 + cc] = (rv && kk < nzA) ? I->pmlzh[3 * kk + cc] : id;
+                }
+            }
+            for (int q = threadIdx.x; q < LX; q += NT) {
+                const int ii = d.li0 + q;
+                for (int cc = 0; cc < 3; ++cc) {
+                    const R id = R(cc == 1 ? 0 : 1);
+                    prx[q * 6 + cc] = (ii >= 0 && ii < nx) ? I->pmlx[3 * ii + cc] : id;
+                    prx[q * 6 + 3 + cc] = (ii >= 0 && ii < nx - 1) ? I->pmlxh[3 * ii + cc] : id;
+                }
+            }
+        }
         // shared buffer -> registers / coefficient planes
         R P[KS], A[KS], B[KS];
 #pragma unroll
@@ -199,7 +314,7 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
                 c1s[c] = sizeof(IT) == 1 ? slut[v1] : __ldg(I->lutc + v1);
             }
         }
-        __syncthreads();   // shared buffer free; coefficient planes and sg ready
+        __syncthreads();   // shared buffer free; coefficient planes, sg and CPML state ready
         if (tn < ntiles) {
             prefetch(s_desc[ns]);
             fetch_state(ns);
@@ -207,8 +322,6 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
         }
         cp_commit();
 
-        const int i = d.li0 + cx;
-        const int kb = d.lk0 + ck0;
         if (nsub > 0) {
             const bool colown = i >= d.oi0 && i < d.oi0 + d.ow;
             unsigned own = 0;
@@ -230,59 +343,100 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
                         if (I->monz[m] == kk) zmask |= ((own >> j) & 1u) << j;
                 }
             }
-            const int nz = d.nz;
+            R pxb = R(1), pxa = R(0), pxk = R(1), phb = R(1), pha = R(0), phk = R(1);
+            if (PML) {
+                pxb = prx[cx * 6 + 0]; pxa = prx[cx * 6 + 1]; pxk = prx[cx * 6 + 2];
+                phb = prx[cx * 6 + 3]; pha = prx[cx * 6 + 4]; phk = prx[cx * 6 + 5];
+            }
             for (int s = 0; s < nsub; ++s) {
-                // ----- H half step
+                // ----- H half step: A (d/dz P), B (d/dx P)
                 if (lane == 0) {
 #pragma unroll
                     for (int j = 0; j < KS; ++j) xPc[warp][j] = P[j];
                 }
                 xPr[warp][lane] = P[0];
                 __syncthreads();
-                const R Pdn = (wz + 1 < WZ) ? xPr[warp + WX][lane] : P[KS - 1];
+                const R Pdn = (wz + 1 < WZ) ? xPr[warp + WX][lane] : (PML ? R(0) : P[KS - 1]);
 #pragma unroll
                 for (int j = 0; j < KS; ++j) {
+                    const int c = (ck0 + j) * LX + cx;
                     R pr = __shfl_down_sync(FULL, P[j], 1);
-                    const R pe = (wx + 1 < WX) ? xPc[warp + 1][j] : pr;
+                    const R pe = (wx + 1 < WX) ? xPc[warp + 1][j] : (PML ? R(0) : pr);
                     pr = (lane == 31) ? pe : pr;
                     const R pk = (j + 1 < KS) ? P[j + 1] : Pdn;
-                    const R ca = TE ? C : c0s[(ck0 + j) * LX + cx];
-                    A[j] += ca * (pk - P[j]);
-                    const R cb = TE ? C : c1s[(ck0 + j) * LX + cx];
-                    B[j] -= cb * (pr - P[j]);
+                    R dz = pk - P[j];
+                    R dx = pr - P[j];
+                    if (PML) {
+                        const R* pz = prz + (ck0 + j) * 6;
+                        const R ps = pz[3] * psA[c] + pz[4] * dz;
+                        psA[c] = ps;
+                        dz = dz * pz[5] + ps;
+                        const R qs = phb * psB[c] + pha * dx;
+                        psB[c] = qs;
+                        dx = dx * phk + qs;
+                    }
+                    const R ca = TE ? C : c0s[c];
+                    const R cb = TE ? C : c1s[c];
+                    if (PML) {
+                        if ((mA >> j) & 1u) A[j] += ca * dz;
+                        if ((mB >> j) & 1u) B[j] -= cb * dx;
+                    } else {
+                        A[j] += ca * dz;
+                        B[j] -= cb * dx;
+                    }
                 }
-                if (hs && i == six - 1) {
+                if (hs && i == six - 1) {   // TF/SF: the B column left of the plane is scattered field
                     const R ge = (R)sg[0][s];
 #pragma unroll
                     for (int j = 0; j < KS; ++j) {
-                        const int kk = d.periodic ? pmod(kb + j, nz) : kb + j;
-                        B[j] += __ldg(I->srcB + kk) * ge;
+                        if ((mB >> j) & 1u) {
+                            const int kk = d.periodic ? pmod(kb + j, nz) : kb + j;
+                            B[j] += __ldg(I->srcB + kk) * ge;
+                        }
                     }
                 }
-                // ----- E half step (branch-free stencil loop)
+                // ----- E half step: P (branch-free stencil loop)
                 if (lane == 31) {
 #pragma unroll
                     for (int j = 0; j < KS; ++j) xBc[warp][j] = B[j];
                 }
                 xAr[warp][lane] = A[KS - 1];
                 __syncthreads();
-                const R Aup = (wz > 0) ? xAr[warp - WX][lane] : A[0];
+                const R Aup = (wz > 0) ? xAr[warp - WX][lane] : (PML ? R(0) : A[0]);
 #pragma unroll
                 for (int j = 0; j < KS; ++j) {
+                    const int c = (ck0 + j) * LX + cx;
                     R bl = __shfl_up_sync(FULL, B[j], 1);
-                    const R be = (wx > 0) ? xBc[warp - 1][j] : bl;
+                    const R be = (wx > 0) ? xBc[warp - 1][j] : (PML ? R(0) : bl);
                     bl = (lane == 0) ? be : bl;
                     const R am = (j > 0) ? A[j - 1] : Aup;
-                    const R cp = TE ? c0s[(ck0 + j) * LX + cx] : C;
-                    P[j] += cp * ((A[j] - am) - (B[j] - bl));
+                    R da = A[j] - am;
+                    R db = B[j] - bl;
+                    if (PML) {
+                        const R* pz = prz + (ck0 + j) * 6;
+                        const R ps = pz[0] * psPz[c] + pz[1] * da;
+                        psPz[c] = ps;
+                        da = da * pz[2] + ps;
+                        const R qs = pxb * psPx[c] + pxa * db;
+                        psPx[c] = qs;
+                        db = db * pxk + qs;
+                    }
+                    const R cp = TE ? c0s[c] : C;
+                    if (PML) {
+                        if ((mP >> j) & 1u) P[j] += cp * (da - db);
+                    } else {
+                        P[j] += cp * (da - db);
+                    }
                 }
                 // rare paths, each behind a tile-uniform flag
                 if (hs && i == six) {   // TF/SF: the plane is total field
                     const R gh = (R)sg[1][s];
 #pragma unroll
                     for (int j = 0; j < KS; ++j) {
-                        const int kk = d.periodic ? pmod(kb + j, nz) : kb + j;
-                        P[j] += __ldg(I->srcP + kk) * gh;
+                        if ((mP >> j) & 1u) {
+                            const int kk = d.periodic ? pmod(kb + j, nz) : kb + j;
+                            P[j] += __ldg(I->srcP + kk) * gh;
+                        }
                     }
                 }
                 if (d.flags & 6) {      // DFT monitor samples of this step
@@ -291,7 +445,7 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
 #pragma unroll
                     for (int j = 0; j < KS; ++j) {
                         R bl = __shfl_up_sync(FULL, B[j], 1);
-                        const R be = (wx > 0) ? xBc[warp - 1][j] : bl;
+                        const R be = (wx > 0) ? xBc[warp - 1][j] : (PML ? R(0) : bl);
                         bl = (lane == 0) ? be : bl;
                         if (xm >= 0 && ((own >> j) & 1u)) {
                             R* smp = smp0 + (size_t)xm * 2 * nz;
@@ -302,9 +456,9 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
                             const R am = (j > 0) ? A[j - 1] : Aup;
                             for (int m = 0; m < I->nmonz; ++m) {
                                 if (I->monz[m] != kb + j) continue;
-                                R* smp = smp0 + (size_t)I->nmon * 2 * nz + (size_t)m * 2 * I->nx;
+                                R* smp = smp0 + (size_t)I->nmon * 2 * nz + (size_t)m * 2 * d.nx;
                                 smp[i] = P[j];
-                                smp[I->nx + i] = R(0.5) * (am + A[j]);
+                                smp[d.nx + i] = R(0.5) * (am + A[j]);
                             }
                         }
                     }
@@ -323,7 +477,8 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
                             e += I->lute[v0] * p * p + a * a + b * b;
                         } else {
                             const int v1 = (int)reinterpret_cast<const IT*>(d.idx1)[o];
-                            e += p * p + I->lute[v0] * a * a + I->lute[v1] * b * b;
+                            e += p * p + (((mA >> j) & 1u) ? I->lute[v0] * a * a : 0.0) +
+                                 (((mB >> j) & 1u) ? I->lute[v1] * b * b : 0.0);
                         }
                     }
                 }
@@ -337,7 +492,7 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
                     atomicAdd(&d.st->energy, tot);
                 }
             }
-            // ----- store the output rectangle
+            // ----- store the output rectangle (owned rows never wrap)
             R* __restrict__ Pout = reinterpret_cast<R*>(const_cast<void*>(d.f[par ^ 1][0]));
             R* __restrict__ Aout = reinterpret_cast<R*>(const_cast<void*>(d.f[par ^ 1][1]));
             R* __restrict__ Bout = reinterpret_cast<R*>(const_cast<void*>(d.f[par ^ 1][2]));
@@ -348,6 +503,25 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
                     Pout[o] = P[j];
                     Aout[o] = A[j];
                     Bout[o] = B[j];
+                }
+            }
+            if (PML) {
+                const int npx = I->npx, npz = I->npz, nx = d.nx;
+                R* __restrict__ gA = I->psiA[par ^ 1];
+                R* __restrict__ gB = I->psiB[par ^ 1];
+                R* __restrict__ gPx = I->psiPx[par ^ 1];
+                R* __restrict__ gPz = I->psiPz[par ^ 1];
+#pragma unroll
+                for (int j = 0; j < KS; ++j) {
+                    if (!((own >> j) & 1u)) continue;
+                    const int c = (ck0 + j) * LX + cx;
+                    const int kk = kb + j;
+                    const int szA = slab_half(kk, nz, npz);
+                    const int szP = slab_int(kk, nz, npz);
+                    if (szA >= 0) gA[(size_t)szA * nx + i] = psA[c];
+                    if (szP >= 0) gPz[(size_t)szP * nx + i] = psPz[c];
+                    if (sxP >= 0) gPx[(size_t)kk * (2 * npx) + sxP] = psPx[c];
+                    if (sxB >= 0) gB[(size_t)kk * (2 * npx) + sxB] = psB[c];
                 }
             }
             if (threadIdx.x == 0) d.st->cur = par ^ 1;

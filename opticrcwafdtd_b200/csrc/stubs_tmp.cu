@@ -1,7 +1,6 @@
 // temporary: 3D, batch and serving paths are added next
 #include "engine.cuh"
 namespace orf {
-int batch2d_run(orf_ctx*, int, const orf_sim2d*, orf_out2d*, orf_progress_fn, void*) { set_error("batch not built yet"); return ORF_EINVAL; }
 }
 extern "C" {
 int32_t orf_serve_open(orf_ctx*, const orf_serve_cfg*, orf_server**) { return ORF_EINVAL; }

@@ -106,6 +106,34 @@ def fdtd3D(sim, ctx: Context | None = None) -> dict:
     return out
 
 
+def fdtd2D_batch(sims, ctx: Context | None = None, progress=None) -> list[dict]:
+    """Run many 2D sims (same pol and precision) together: one persistent
+    kernel per fused step block advances every instance (orf_batch2d_run).
+    Returns the list of out structs, in order."""
+    lib = _lib.load()
+    ms = [_abi.marshal_sim2d(s) for s in sims]
+    if not ms:
+        return []
+    arr = (_abi.OrfSim2D * len(ms))(*[m.struct for m in ms])
+    outs = [_abi.alloc_out2d(m) for m in ms]
+    oarr = (_abi.OrfOut2D * len(ms))(*[o for o, _ in outs])
+    own = ctx is None
+    if own:
+        ctx = Context(0)
+    cb, box = _abi.make_progress(progress)
+    st = lib.orf_batch2d_run(ctx.handle, len(ms), arr, oarr, cb or _abi.PROGRESS_FN(0), None)
+    if own:
+        ctx.close()
+    if box and "exc" in box:
+        raise box["exc"]
+    _lib.check(st, "fdtd2D_batch")
+    res = []
+    for q, m in enumerate(ms):
+        out = _abi.finish_out2d(m, oarr[q], outs[q][1])
+        res.append(out)
+    return res
+
+
 class Job:
     """Device-resident run: fields and DFT sums stay on the GPU between
     advance() calls (orf_job_* in include/orf_fdtd.h)."""
