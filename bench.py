@@ -1,5 +1,5 @@
 #!/usr/bin/env python
-"""Benchmark of the B200 Yee-FDTD engine on the configuration-2 workload.
+"""Benchmark of the B200 Yee-FDTD engine on the 2D TM 4000 x 1500 pixel-region workload.
 
 Workload (one bench "step" = one whole FDTD job): 2D TM, 4000 x 1500 cells at
 dx = 10 nm with 20-cell CPML, a seeded Bernoulli Si/SiO2 pixel design region
@@ -40,7 +40,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="single", choices=["single", "double"])
-    ap.add_argument("--time-steps", type=int, default=30000, help="FDTD time steps per job (config 2: 30000)")
+    ap.add_argument("--time-steps", type=int, default=30000, help="FDTD time steps per job (the workload: 30000)")
     ap.add_argument("--cpu-sample-steps", type=int, default=300)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -66,7 +66,7 @@ def measured_peaks():
 
 def ncu_traffic_per_cell_update():
     """DRAM bytes per cell update of the interior kernel from the committed ncu summary."""
-    p = os.path.join(HERE, "profiles", "interior_kernel_config2.json")
+    p = os.path.join(HERE, "profiles", "interior_kernel_tm_pixel_4000x1500.json")
     try:
         with open(p) as f:
             d = json.load(f)
@@ -140,7 +140,7 @@ def cpu_baseline(sim, sample_steps):
     dt = time.perf_counter() - t
     cells = s["epsX"].shape[0] * (s["epsZ"].shape[1])
     return {"value": cells * sample_steps / dt / 1e6, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"config-2 grid {cells} cells, {sample_steps} of 30000 time steps, "
+            "sample": f"TM pixel-region grid {cells} cells, {sample_steps} of 30000 time steps, "
                       f"{s['precision']} fields, {dt:.1f} s"}
 
 
@@ -149,7 +149,7 @@ def run_reference(args):
     if rank != 0:
         return
     from opticrcwafdtd_b200 import workloads
-    sim = workloads.config2_sim(precision=args.precision)
+    sim = workloads.pixel_region_sim(precision=args.precision)
     vals = []
     for i in range(args.warmup + args.steps):
         r = cpu_baseline(sim, max(20, args.cpu_sample_steps // 2))
@@ -159,8 +159,8 @@ def run_reference(args):
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
         "warmup": args.warmup, "higher_is_better": True, "dtype": "f32" if args.precision == "single" else "f64",
-        "data": "synthetic (seeded pixel map with config-2 shapes)",
-        "config": {"workload": "config2: 2D TM 4000x1500 dx=10nm, 101-lambda DFT, 30000 steps (bounded sample)"},
+        "data": "synthetic (seeded Bernoulli Si/SiO2 pixel map, 4000x1500)",
+        "config": {"workload": "2D TM pixel region 4000x1500 dx=10nm, 101-lambda DFT, 30000 steps (bounded sample)"},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": r["cores"], "kind": "port", "sample": r["sample"]},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "reference (MATLAB P-code) cannot run on this box; CPU oracle restatement timed instead",
@@ -183,7 +183,7 @@ def main():
                                 device_id=torch.device("cuda", local))
     from opticrcwafdtd_b200 import Context, Job, fdtd2D, workloads
 
-    sim = workloads.config2_sim(precision=args.precision, steps=args.time_steps)
+    sim = workloads.pixel_region_sim(precision=args.precision, steps=args.time_steps)
     nx, nz = sim["epsX"].shape[0], sim["epsZ"].shape[1]
     cells = nx * nz
     stream = torch.cuda.current_stream()
@@ -278,8 +278,8 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32" if args.precision == "single" else "f64",
-            "data": "synthetic (seeded Bernoulli Si/SiO2 pixel map, config-2 shapes)",
-            "config": {"workload": "config2: 2D TM 4000x1500 dx=10nm 20-cell CPML, TM0 source, "
+            "data": "synthetic (seeded Bernoulli Si/SiO2 pixel map, 4000x1500)",
+            "config": {"workload": "2D TM pixel region 4000x1500 dx=10nm 20-cell CPML, TM0 source, "
                                    "101-lambda DFT (3 x-lines, 2 z-lines), 30000 time steps per job",
                        "cells": cells, "time_steps_per_job": nsteps,
                        "precision": "FP32 fields, FP32+Kahan DFT, FP64 phases" if args.precision == "single"

@@ -229,7 +229,7 @@ ORF_API int32_t orf_job_destroy(orf_job* job);
  * allocating routine.  All device state lives in one 64 MiB static
  * __device__ array that every GPU loading this library reserves until exit.
  * Runs needing more return ORF_ETOOLARGE, before any device work (the
- * config-1 grating coupler, 800 x 300 FP64 with 51 wavelengths, needs
+ * 800 x 300 FP64 grating coupler with 51 wavelengths needs
  * about 20 MiB).  The first
  * call on a device looks up the array's address and should come before any
  * stream capture.  Calls share the array: calls that overlap on the GPU race,
@@ -248,9 +248,10 @@ ORF_API int32_t orf_fdtd3d_run_ctx(orf_ctx* ctx, const orf_sim3d* sim, orf_out3d
                            orf_progress_fn progress, void* user);
 
 /* ------------------------------------------------------------ batches --- */
-/* Many independent 2D runs advanced together by one persistent kernel per
- * launch, the time loop captured in CUDA graphs.  All sims of one call must
- * share pol and precision.  Replaces the sequential orf.fdtd2D calls of the
+/* Many independent 2D runs advanced together: runs of one kernel
+ * configuration share each persistent-kernel launch, and the time loop is
+ * captured in CUDA graphs.  All sims of one call must share the precision
+ * (ORF_EINVAL otherwise); TE and TM runs may be mixed.  Replaces the sequential orf.fdtd2D calls of the
  * sweeps (examples/cpo_box_scan.m:23-31, optimizeGratingCoupler.m:1-12). */
 ORF_API int32_t orf_batch2d_run(orf_ctx* ctx, int32_t n, const orf_sim2d* sims,
                         orf_out2d* outs, orf_progress_fn progress, void* user);
@@ -266,13 +267,16 @@ typedef struct orf_serve_job_info {
     double t_submit, t_admit, t_done;   /* seconds on the server's clock       */
     int64_t steps;
     int64_t cells;
-    int32_t status;
-    int32_t dims;
+    int32_t status;            /* the job's orf_status                        */
+    int32_t dims;              /* 2 or 3                                       */
+    int64_t device_bytes;      /* device memory the job held while resident    */
 } orf_serve_job_info;
 
 ORF_API int32_t orf_serve_open(orf_ctx* ctx, const orf_serve_cfg* cfg, orf_server** srv);
-/* The sim and its arrays are copied at submit; out arrays must stay valid
- * until the ticket completes. */
+/* The sim and its arrays are copied at submit.  The out struct, the arrays
+ * it points to (and, in 3D, its per-monitor pointer arrays) must stay valid
+ * until the ticket completes: the server writes them when it retires the
+ * job, and sets out->wall_time to the job's latency (done - submit). */
 ORF_API int32_t orf_serve_submit2d(orf_server* srv, const orf_sim2d* sim, orf_out2d* out,
                            int64_t* ticket);
 ORF_API int32_t orf_serve_submit3d(orf_server* srv, const orf_sim3d* sim, orf_out3d* out,

@@ -13,4 +13,4 @@ from .geometry import epsCellMean, epsComponents2D, epsComponents3D, epsFromBoxe
 from .modes import slabModes  # noqa: F401
 
 __version__ = "0.1.0"
-from .fdtd import Context, Job, device_count, fdtd2D, fdtd2D_batch, fdtd2DTE, fdtd3D  # noqa: F401,E402
+from .fdtd import Context, Job, Server, device_count, fdtd2D, fdtd2D_batch, fdtd2DTE, fdtd3D  # noqa: F401,E402

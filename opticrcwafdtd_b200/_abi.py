@@ -21,6 +21,7 @@ c_int32_p = C.POINTER(C.c_int32)
 
 ORF_TE, ORF_TM = 0, 1
 ORF_DOUBLE, ORF_SINGLE = 0, 1
+ORF_EBUSY, ORF_ETOOLARGE = 7, 8
 
 STATUS_NAMES = {
     0: "ORF_OK", 1: "ORF_EINVAL", 2: "ORF_ENOMEM_DEVICE", 3: "ORF_ECANCELLED",
@@ -110,7 +111,7 @@ class OrfServeCfg(C.Structure):
 class OrfServeJobInfo(C.Structure):
     _fields_ = [("t_submit", C.c_double), ("t_admit", C.c_double), ("t_done", C.c_double),
                 ("steps", C.c_int64), ("cells", C.c_int64), ("status", C.c_int32),
-                ("dims", C.c_int32)]
+                ("dims", C.c_int32), ("device_bytes", C.c_int64)]
 
 
 class OrfError(RuntimeError):

@@ -3,15 +3,17 @@
 // The reference runs its sweeps (examples/cpo_box_scan.m:23-31,
 // optimizeGratingCoupler.m:1-12, the app's period sweep) as sequential
 // orf.fdtd2D calls.  Here every instance is set up as a device-resident job,
-// and their tile descriptors (self-contained, FastTile2D), DFT streams and
-// state pointers are concatenated: one persistent interior launch and one
-// frame launch advance all instances per fused step block, one flush and one
-// check launch close each chunk, and the chunk sequence is captured as a
-// CUDA graph.  Instances of uneven size and step budget coexist: a finished
-// instance's tiles turn into no-ops.
+// and instances of one kernel configuration form a group (group.cuh): their
+// tile descriptors (self-contained, FastTile2D), DFT streams and state
+// pointers are concatenated, so one persistent interior launch and one frame
+// launch advance all of them per fused step block, one flush and one check
+// launch close each chunk, and the chunk sequence is captured as a CUDA
+// graph.  Instances of uneven size and step budget coexist: a finished
+// instance's tiles turn into no-ops.  Instances of both polarisations, or
+// with more than 256 distinct permittivities, fall into further groups.
 #include <algorithm>
 
-#include "job2d.cuh"
+#include "group.cuh"
 
 namespace orf {
 namespace {
@@ -32,104 +34,25 @@ int run_batch(orf_ctx* ctx, int n, const orf_sim2d* sims, orf_out2d* outs, orf_p
         }
         jobs.push_back(std::move(j));
     }
-    // all instances share the kernel variant and the fused step count T
-    const int T = jobs[0]->T, fv = jobs[0]->fvariant;
-    const bool te = jobs[0]->te;
-    bool idx16 = false;
+    // instances sharing a kernel configuration (precision, index width,
+    // fused step count, interior variant) form one group: one launch per
+    // kernel advances all of its members
+    std::vector<std::unique_ptr<Group2D<R>>> groups;
+    int64_t nmax = 0;
     for (auto& j : jobs) {
-        if (j->T != T || j->fvariant != fv) {
-            set_error("batch instances picked different tilings");
-            return ORF_EINVAL;
+        Group2D<R>* g = nullptr;
+        for (auto& c : groups)
+            if (Group2D<R>::compatible(c->jobs[0], j.get())) g = c.get();
+        if (!g) {
+            groups.push_back(std::make_unique<Group2D<R>>());
+            g = groups.back().get();
+            g->ctx = ctx;
         }
-        idx16 = idx16 || j->idx16;
-    }
-    if (idx16) {
-        for (auto& j : jobs)
-            if (!j->idx16) {
-                set_error("mixing instances with <= 256 and > 256 distinct permittivities is not supported");
-                return ORF_EINVAL;
-            }
-    }
-    std::vector<FastTile2D> inner, frame;
-    std::vector<DftStream> streams;
-    std::vector<FlushItem> items;
-    std::vector<JobState*> states;
-    int64_t interior_cells = 0, cells = 0, nmax = 0;
-    for (auto& j : jobs) {
-        inner.insert(inner.end(), j->ftiles_host.begin(), j->ftiles_host.begin() + j->nfast);
-        frame.insert(frame.end(), j->ftiles_host.begin() + j->nfast, j->ftiles_host.end());
-        for (int q = 0; q < j->nfast; ++q) interior_cells += (int64_t)j->ftiles_host[q].ow * j->ftiles_host[q].oh;
-        cells += j->cells();
-        const int s0 = (int)streams.size();
-        streams.insert(streams.end(), j->host_streams.begin(), j->host_streams.end());
-        for (int q = 0; q < j->nstreams; ++q)
-            for (int e0 = 0; e0 < j->host_streams[q].len; e0 += 128)
-                for (int l0 = 0; l0 < j->nL; l0 += 8) items.push_back({s0 + q, e0, l0, 0});
-        states.push_back(j->d_st);
+        g->add(j.get());
         nmax = std::max<int64_t>(nmax, j->nmax);
     }
-    Arena ar;
-    FastTile2D *d_inner = nullptr, *d_frame = nullptr;
-    DftStream* d_streams = nullptr;
-    FlushItem* d_items = nullptr;
-    JobState** d_states = nullptr;
-    ar.add(&d_inner, inner.size() + 1);
-    ar.add(&d_frame, frame.size() + 1);
-    ar.add(&d_streams, streams.size() + 1);
-    ar.add(&d_items, items.size() + 1);
-    ar.add(&d_states, states.size() + 1);
-    ORF_TRY(ar.alloc());
-    struct Guard {
-        Arena* a;
-        ~Guard() { a->release(); }
-    } guard{&ar};
     cudaStream_t st = ctx->stream;
-    auto up = [&](void* d, const void* h, size_t b) -> int {
-        if (!b) return ORF_OK;
-        ORF_CUDA(cudaMemcpyAsync(d, h, b, cudaMemcpyHostToDevice, st));
-        ctx->stats.h2d_bytes += (int64_t)b;
-        return ORF_OK;
-    };
-    ORF_TRY(up(d_inner, inner.data(), inner.size() * sizeof(FastTile2D)));
-    ORF_TRY(up(d_frame, frame.data(), frame.size() * sizeof(FastTile2D)));
-    ORF_TRY(up(d_streams, streams.data(), streams.size() * sizeof(DftStream)));
-    ORF_TRY(up(d_items, items.data(), items.size() * sizeof(FlushItem)));
-    ORF_TRY(up(d_states, states.data(), states.size() * sizeof(JobState*)));
-    ORF_CUDA(cudaStreamSynchronize(st));
-
-    const bool f64 = sizeof(R) == 8;
-    const int bps_f = fast2d_blocks_per_sm(f64, te, idx16, false, fv);
-    const int bps_p = fast2d_blocks_per_sm(f64, te, idx16, true, 0);
-    const int grid_f = (int)std::min<size_t>(inner.size(), (size_t)ctx->sm_count * std::max(1, bps_f));
-    const int grid_p = (int)std::min<size_t>(frame.size(), (size_t)ctx->sm_count * std::max(1, bps_p));
-    const int ni = (int)inner.size(), nf = (int)frame.size();
-    ChunkEngine eng;
-    eng.ctx = ctx;
-    eng.fp64 = f64;
-    eng.T = T;
-    eng.par = 0;
-    eng.d_streams = d_streams;
-    eng.d_items = d_items;
-    eng.nitems = (int)items.size();
-    eng.d_states = d_states;
-    eng.nstates = n;
-    eng.step = [&](int off, int nsub, int par, int we, cudaStream_t s, KernelTimer* tm) -> cudaError_t {
-        cudaError_t e = cudaSuccess;
-        cudaEvent_t a = nullptr;
-        if (ni) {
-            if (tm && tm->begin(s, &a) != ORF_OK) return cudaErrorUnknown;
-            e = launch_fast2d(f64, te, idx16, false, fv, d_inner, ni, off, nsub, par, we, grid_f, s);
-            if (e != cudaSuccess) return e;
-            if (tm && tm->end(s, 0, interior_cells * nsub, a) != ORF_OK) return cudaErrorUnknown;
-        }
-        if (nf) {
-            if (tm && tm->begin(s, &a) != ORF_OK) return cudaErrorUnknown;
-            e = launch_fast2d(f64, te, idx16, true, 0, d_frame, nf, off, nsub, par, we, grid_p, s);
-            if (e != cudaSuccess) return e;
-            if (tm && tm->end(s, 1, (cells - interior_cells) * nsub, a) != ORF_OK) return cudaErrorUnknown;
-        }
-        return e;
-    };
+    for (auto& g : groups) ORF_TRY(g->build(st));
 
     // time loop: graph replays in batches; every instance's status ring is
     // read after each batch (progress = mean fraction, stop when all are done)
@@ -167,7 +90,7 @@ int run_batch(orf_ctx* ctx, int n, const orf_sim2d* sims, orf_out2d* outs, orf_p
     while (!all_done()) {
         while (enq < chunks && evs.size() - head < (size_t)kInFlight) {
             const int nb = (int)std::min<int64_t>(kBatch, chunks - enq);
-            ORF_TRY(eng.enqueue(nb, st));
+            for (auto& g : groups) ORF_TRY(g->enqueue(nb, st));
             enq += nb;
             cudaEvent_t e;
             ORF_CUDA(cudaEventCreateWithFlags(&e, cudaEventBlockingSync | cudaEventDisableTiming));
@@ -185,7 +108,7 @@ int run_batch(orf_ctx* ctx, int n, const orf_sim2d* sims, orf_out2d* outs, orf_p
     cudaError_t se = cudaStreamSynchronize(st);
     for (auto e : evs) cudaEventDestroy(e);
     ORF_CUDA(se);
-    eng.collect_timing();
+    for (auto& g : groups) g->eng.collect_timing();
     if (rc != ORF_OK) return rc;
     for (int q = 0; q < n; ++q) {
         ctx->stats.cell_updates += jobs[q]->pl.last_step * jobs[q]->cells();
@@ -207,8 +130,8 @@ int batch2d_run(orf_ctx* ctx, int n, const orf_sim2d* sims, orf_out2d* outs, orf
             set_error("%s", buf);
             return st;
         }
-        if (sims[q].pol != sims[0].pol || sims[q].precision != sims[0].precision) {
-            set_error("all instances of a batch share pol and precision (instance %d differs)", q + 1);
+        if (sims[q].precision != sims[0].precision) {
+            set_error("all instances of a batch share the precision (instance %d differs)", q + 1);
             return ORF_EINVAL;
         }
     }

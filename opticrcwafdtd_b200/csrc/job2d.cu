@@ -237,6 +237,7 @@ int Job2D<R>::create(const orf_sim2d* s) {
     ar.add(&d_streams, nstreams + 1);
     ar.add(&d_items, nitems + 1);
     ar.add(&d_pairs, npairs + 1);
+    ORF_TRY(ar.check_budget(budget, &need));
     if (ext_base) {
         ORF_TRY(ar.place(ext_base, ext_cap));
     } else {

@@ -9,7 +9,7 @@
 #include <algorithm>
 #include <unordered_map>
 
-#include "engine.cuh"
+#include "job3d.cuh"
 
 namespace orf {
 
@@ -60,62 +60,6 @@ int validate3d(const orf_sim3d* s) {
 
 namespace {
 
-template <class R>
-struct Job3D : orf_job {
-    int n[3] = {0, 0, 0};
-    bool per[3] = {false, false, false};
-    int pitch = 0, nM = 0, nL = 0, idxw = 1, zc = 4;
-    double d = 0, Cc = 0, S = 0, src_end = 0, shutoff = 0;
-    int64_t nmax = 0, nsrc = 0, enq_steps = 0;
-    Arena arena;
-    Inst3D<R> h{};
-    Inst3D<R>* d_inst = nullptr;
-    JobState* d_st = nullptr;
-    JobState** d_states = nullptr;
-    std::vector<Tile3D> tiles, tiles_pml;   // interior / CPML tiles
-    Tile3D* d_tiles = nullptr;
-    Tile3D* d_tiles_pml = nullptr;
-    DftStream* d_streams = nullptr;
-    std::vector<DftStream> host_streams;
-    FlushItem* d_items = nullptr;
-    FluxPair* d_pairs = nullptr;
-    int nstreams = 0, nitems = 0, npairs = 0;
-    void* d_acc = nullptr;
-    double* d_omega = nullptr;
-    double* d_flux = nullptr;
-    double2* d_stage = nullptr;
-    size_t stage_elems = 0;
-    std::vector<std::pair<int, int>> planes;   // (Na, Nb) per monitor
-    ChunkStatus* ring_h = nullptr;
-    ChunkStatus* ring_d = nullptr;
-    volatile int* cancel_h = nullptr;
-    int* cancel_d = nullptr;
-    ChunkEngine eng;
-    ProgressLoop pl;
-
-    Job3D() { dims = 3; }
-    ~Job3D() override {
-        if (arena.base) {
-            cudaStreamSynchronize(ctx->stream);
-            arena.release();
-        }
-        if (ring_h) cudaFreeHost(ring_h);
-        if (cancel_h) cudaFreeHost((void*)cancel_h);
-    }
-    size_t N() const { return (size_t)n[0] * n[1] * n[2]; }
-    size_t NP() const { return (size_t)pitch * n[1] * n[2]; }
-    int64_t cells() const override { return (int64_t)N(); }
-    int64_t step_budget() const override { return nmax; }
-
-    int create(const orf_sim3d* s);
-    int init_state();
-    int advance(int64_t nsteps, orf_progress_fn progress, void* user) override;
-    int64_t steps_done() override;
-    int reset() override;
-    int get_fields(double* const* f, int nf) override;
-    int finish3d(orf_out3d* o) override;
-};
-
 struct Lut3 {
     std::unordered_map<uint64_t, uint32_t> map;
     std::vector<double> vals;
@@ -139,6 +83,8 @@ struct Lut3 {
         return id;
     }
 };
+
+}  // namespace
 
 template <class R>
 int Job3D<R>::create(const orf_sim3d* s) {
@@ -331,6 +277,7 @@ int Job3D<R>::create(const orf_sim3d* s) {
     ar.add(&d_streams, nstreams + 1);
     ar.add(&d_items, nitems + 1);
     ar.add(&d_pairs, npairs + 1);
+    ORF_TRY(ar.check_budget(budget, &need));
     ORF_TRY(ar.alloc());
     arena = ar;
     ORF_CUDA(cudaMemsetAsync(arena.base, 0, arena.total, st));
@@ -588,7 +535,8 @@ int Job3D<R>::get_fields(double* const* f, int nf) {
     return ORF_OK;
 }
 
-}  // namespace
+template struct Job3D<float>;
+template struct Job3D<double>;
 
 int make_job3d(orf_ctx* ctx, const orf_sim3d* sim, orf_job** out) {
     *out = nullptr;

@@ -1,0 +1,64 @@
+// job3d.cuh -- device-resident 3D run (orf.fdtd3D).
+#pragma once
+#include "engine.cuh"
+
+namespace orf {
+
+template <class R>
+struct Job3D : orf_job {
+    int n[3] = {0, 0, 0};
+    bool per[3] = {false, false, false};
+    int pitch = 0, nM = 0, nL = 0, idxw = 1, zc = 4;
+    double d = 0, Cc = 0, S = 0, src_end = 0, shutoff = 0;
+    int64_t nmax = 0, nsrc = 0, enq_steps = 0;
+    Arena arena;
+    Inst3D<R> h{};
+    Inst3D<R>* d_inst = nullptr;
+    JobState* d_st = nullptr;
+    JobState** d_states = nullptr;
+    std::vector<Tile3D> tiles, tiles_pml;   // interior / CPML tiles
+    Tile3D* d_tiles = nullptr;
+    Tile3D* d_tiles_pml = nullptr;
+    DftStream* d_streams = nullptr;
+    std::vector<DftStream> host_streams;
+    FlushItem* d_items = nullptr;
+    FluxPair* d_pairs = nullptr;
+    int nstreams = 0, nitems = 0, npairs = 0;
+    void* d_acc = nullptr;
+    double* d_omega = nullptr;
+    double* d_flux = nullptr;
+    double2* d_stage = nullptr;
+    size_t stage_elems = 0;
+    std::vector<std::pair<int, int>> planes;   // (Na, Nb) per monitor
+    ChunkStatus* ring_h = nullptr;
+    ChunkStatus* ring_d = nullptr;
+    volatile int* cancel_h = nullptr;
+    int* cancel_d = nullptr;
+    ChunkEngine eng;
+    ProgressLoop pl;
+
+    Job3D() { dims = 3; }
+    ~Job3D() override {
+        if (arena.base) {
+            cudaStreamSynchronize(ctx->stream);
+            arena.release();
+        }
+        if (ring_h) cudaFreeHost(ring_h);
+        if (cancel_h) cudaFreeHost((void*)cancel_h);
+    }
+    size_t N() const { return (size_t)n[0] * n[1] * n[2]; }
+    size_t NP() const { return (size_t)pitch * n[1] * n[2]; }
+    int64_t cells() const override { return (int64_t)N(); }
+    int64_t step_budget() const override { return nmax; }
+
+    int create(const orf_sim3d* s);
+    int init_state();
+    int advance(int64_t nsteps, orf_progress_fn progress, void* user) override;
+    int64_t steps_done() override;
+    int reset() override;
+    int get_fields(double* const* f, int nf) override;
+    int finish3d(orf_out3d* o) override;
+};
+
+
+}  // namespace orf

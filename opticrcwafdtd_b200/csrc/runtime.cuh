@@ -113,6 +113,15 @@ struct Arena {
     }
     // Carve the requests from caller-provided device memory instead of
     // cudaMalloc (no allocation); fails with ORF_ETOOLARGE if they do not fit.
+    int check_budget(size_t budget, size_t* need) const {
+        *need = bytes();
+        if (*need > budget) {
+            set_error("run needs %.1f MB of device memory, above the %.1f MB left in the budget", *need / 1048576.0,
+                      budget / 1048576.0);
+            return ORF_ETOOLARGE;
+        }
+        return ORF_OK;
+    }
     int place(void* ext, size_t cap) {
         total = bytes();
         if (total > cap) {
@@ -154,6 +163,10 @@ struct orf_job {
     virtual ~orf_job() = default;
     orf_ctx* ctx = nullptr;
     int dims = 2;
+    // admission: create() fails with ORF_ETOOLARGE, before allocating, when
+    // the job's device arena would exceed `budget`; `need` holds its size
+    size_t budget = ~size_t(0);
+    size_t need = 0;
     virtual int advance(int64_t nsteps, orf_progress_fn progress, void* user) = 0;
     virtual int64_t steps_done() = 0;
     virtual int64_t step_budget() const = 0;

@@ -107,8 +107,9 @@ def fdtd3D(sim, ctx: Context | None = None) -> dict:
 
 
 def fdtd2D_batch(sims, ctx: Context | None = None, progress=None) -> list[dict]:
-    """Run many 2D sims (same pol and precision) together: one persistent
-    kernel per fused step block advances every instance (orf_batch2d_run).
+    """Run many 2D sims (same precision; TE and TM may mix) together: one
+    persistent-kernel launch per fused step block advances every instance of
+    a kernel configuration (orf_batch2d_run).
     Returns the list of out structs, in order."""
     lib = _lib.load()
     ms = [_abi.marshal_sim2d(s) for s in sims]
@@ -190,6 +191,95 @@ class Job:
     def close(self) -> None:
         if self.handle:
             self.lib.orf_job_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Continuous-batching server (orf_serve_* in include/orf_fdtd.h).
+
+    submit() copies a 2D or 3D sim into the queue and returns a ticket; each
+    step() admits queued jobs while their device memory fits the budget,
+    advances every resident job by up to macro_steps time steps (jobs of one
+    kernel configuration share launches) and retires finished jobs.  result()
+    returns the out struct of a finished ticket, info() its timing record
+    (submit/admit/done on the server clock, seconds)."""
+
+    def __init__(self, ctx: Context | None = None, max_device_bytes: int = 0, max_jobs: int = 0,
+                 macro_steps: int = 0):
+        self.lib = _lib.load()
+        self.ctx = ctx or Context(0)
+        cfg = _abi.OrfServeCfg(int(max_device_bytes), int(max_jobs), int(macro_steps))
+        h = C.c_void_p()
+        _lib.check(self.lib.orf_serve_open(self.ctx.handle, C.byref(cfg), C.byref(h)), "orf_serve_open")
+        self.handle = h
+        self._jobs: dict[int, tuple] = {}
+
+    def submit(self, sim, dims: int = 2) -> int:
+        t = C.c_int64()
+        if dims == 2:
+            m = _abi.marshal_sim2d(sim)
+            o, bufs = _abi.alloc_out2d(m)
+            _lib.check(self.lib.orf_serve_submit2d(self.handle, C.byref(m.struct), C.byref(o), C.byref(t)),
+                       "serve submit")
+        else:
+            m = _abi.marshal_sim3d(sim)
+            o, bufs = _abi.alloc_out3d(m)
+            _lib.check(self.lib.orf_serve_submit3d(self.handle, C.byref(m.struct), C.byref(o), C.byref(t)),
+                       "serve submit")
+        # the out struct and its buffers must outlive the job
+        self._jobs[int(t.value)] = (dims, m, o, bufs)
+        return int(t.value)
+
+    def step(self) -> None:
+        _lib.check(self.lib.orf_serve_step(self.handle), "serve step")
+
+    def pending(self) -> tuple[int, int]:
+        q, r = C.c_int32(), C.c_int32()
+        _lib.check(self.lib.orf_serve_pending(self.handle, C.byref(q), C.byref(r)))
+        return int(q.value), int(r.value)
+
+    def clock(self) -> float:
+        return float(self.lib.orf_serve_clock(self.handle))
+
+    def info(self, ticket: int) -> dict | None:
+        """Timing record of a finished ticket, None while it is queued or resident."""
+        i = _abi.OrfServeJobInfo()
+        st = self.lib.orf_serve_poll(self.handle, int(ticket), C.byref(i))
+        if st == _abi.ORF_EBUSY:
+            return None
+        _lib.check(st, "serve poll")
+        return {k: getattr(i, k) for k, _ in i._fields_}
+
+    def result(self, ticket: int) -> dict:
+        """out struct of a finished ticket (raises the job's error if it failed)."""
+        inf = self.info(ticket)
+        if inf is None:
+            raise _abi.OrfError("orf:busy", f"ticket {ticket} has not finished", _abi.ORF_EBUSY)
+        dims, m, o, bufs = self._jobs[int(ticket)]
+        st = int(inf["status"])
+        if st != 0:
+            raise _abi.OrfError(_abi.STATUS_IDS.get(st, "orf:error"),
+                                f"served job {ticket} failed with {_abi.STATUS_NAMES.get(st, st)}", st)
+        return _abi.finish_out2d(m, o, bufs) if dims == 2 else _abi.finish_out3d(m, o, bufs)
+
+    def drain(self, max_rounds: int = 10**7) -> None:
+        """step() until nothing is queued or resident."""
+        for _ in range(max_rounds):
+            q, r = self.pending()
+            if q == 0 and r == 0:
+                return
+            self.step()
+        raise RuntimeError("serve drain did not finish")
+
+    def close(self) -> None:
+        if self.handle:
+            self.lib.orf_serve_close(self.handle)
             self.handle = None
 
     def __del__(self):

@@ -1,15 +1,15 @@
-"""Seeded synthetic inputs with the shapes of the benchmark configurations.
+"""Seeded synthetic inputs with the shapes of the benchmark workloads.
 
 No dataset is involved: every structure is generated from a seed, with the
-sizes, materials and value distributions the configurations name.
+sizes, materials and value distributions the workloads name.
 
-  config1   2D TE SOI grating coupler, 800 x 300 at 20 nm, FP64, 8000 steps
-  config2   2D TM Si/SiO2 pixel design region, 4000 x 1500 at 10 nm, 30000 steps
-  config3   3D TiO2 pillar lattice on SiO2, 600 x 600 x 300 at 20 nm, 6000 steps
-  config4   256 2D TE grating couplers of uneven size, 10000 steps each (batch)
-  config5   Poisson stream of mixed 2D / 3D jobs (serving)
+  coupler_sim          2D TE SOI grating coupler, 800 x 300 at 20 nm, FP64, 8000 steps
+  pixel_region_sim     2D TM Si/SiO2 pixel design region, 4000 x 1500 at 10 nm, 30000 steps
+  pillar_lattice_sim   3D TiO2 pillar lattice on SiO2, 600 x 600 x 300 at 20 nm, 6000 steps
+  coupler_batch_sims   256 2D TE grating couplers of uneven size, 10000 steps each (batch)
+  serve_stream         Poisson stream of mixed 2D / 3D jobs (serving)
 
-The 100 nm source bandwidth of the configurations is read as a 1/e spectral
+The 100 nm source bandwidth of the workloads is read as a 1/e spectral
 half-width of 50 nm, i.e. bw = 0.05 / 1.55 in the reference's relative units
 (fdtd2DTE.m:14-15).
 """
@@ -54,7 +54,7 @@ def _runs_to_boxes(mask: np.ndarray, x0: float, z0: float, px: float, pz: float,
     return boxes
 
 
-def config2_sim(seed: int = 0, steps: int = 30000, precision: str = "single", nx: int = 4000, nz: int = 1500,
+def pixel_region_sim(seed: int = 0, steps: int = 30000, precision: str = "single", nx: int = 4000, nz: int = 1500,
                 n_lambda: int = 101) -> dict:
     """2D TM, dx = 10 nm, 20-cell CPML: SOI waveguide (220 nm Si in SiO2) whose
     middle 10 um x 0.22 um is a Bernoulli(0.5) Si/SiO2 pixel map (20 nm pixels,
@@ -109,7 +109,7 @@ def core_mode(z, n, lambda0, pol="TE", core=(0.0, 0.22), n_modes=8, eps_half=Non
     return float(np.real(m["neff"][q])), m["field"][:, q]
 
 
-def config1_sim(precision: str = "double", steps: int = 8000, n_lambda: int = 51, period=0.63, ff=0.5, etch=0.07,
+def coupler_sim(precision: str = "double", steps: int = 8000, n_lambda: int = 51, period=0.63, ff=0.5, etch=0.07,
                 nx: int = 800, nz: int = 300) -> dict:
     """2D TE SOI grating coupler, 800 x 300 at 20 nm with 20-cell CPML.  The
     grating starts 1.5 um after the source (the reference's x = 4 um start does
@@ -132,7 +132,7 @@ def config1_sim(precision: str = "double", steps: int = 8000, n_lambda: int = 51
     return sim
 
 
-def config4_sims(n: int = 256, seed: int = 4, steps: int = 10000, precision: str = "single", n_lambda: int = 51):
+def coupler_batch_sims(n: int = 256, seed: int = 4, steps: int = 10000, precision: str = "single", n_lambda: int = 51):
     """n uneven grating couplers: period U[0.56, 0.70], fill U[0.3, 0.7], etch
     U[0.05, 0.12] um, domain width U[12, 24] um (600-1200 cells), height
     250-350 cells, dx = 20 nm."""

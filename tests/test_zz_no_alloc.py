@@ -39,7 +39,7 @@ def _same(a, b):
 @pytest.mark.parametrize("make", [
     lambda: cases.mixed_te_sim(nx=300, nz=160, steps=300, seed=21),
     lambda: cases.mixed_te_sim(nx=300, nz=160, steps=300, seed=22, pol="TM", precision="single"),
-    lambda: workloads.config1_sim(steps=600),
+    lambda: workloads.coupler_sim(steps=600),
 ])
 def test_noalloc_matches_allocating_run_twice(make):
     sim = make()
