@@ -233,6 +233,14 @@ class _Shape:
             return ok & zin & (r > 0) & ((X - cx) ** 2 + (Y - cy) ** 2 < r * r)
         raise AssertionError
 
+    def z_extruded(self) -> bool:
+        """True when the cross-section does not change with z inside [z1, z2)."""
+        if self.kind in ("cyl", "cone"):
+            return self.r1 == self.r2
+        if self.kind == "lattice":
+            return self.dRdz == 0.0
+        return True
+
     def band(self, X, Y, Z, h):
         """Cells (centres X, Y, Z, half-size h) that the shape boundary may cross."""
         near = ((X >= self.lo[0] - h) & (X <= self.hi[0] + h) & (Y >= self.lo[1] - h)
@@ -252,17 +260,23 @@ class _Shape:
                 side = (rho >= rlo - hd) & (rho <= rhi + hd)
                 return near & (zface | side)
             if k == "lattice":
-                ix = np.clip(np.rint((X - self.x0) / self.P).astype(np.int64), 0, self.R.shape[0] - 1)
-                iy = np.clip(np.rint((Y - self.y0) / self.P).astype(np.int64), 0, self.R.shape[1] - 1)
+                # a pillar whose rim passes through the cell has its centre at
+                # one of the 3 x 3 lattice sites around the cell's nearest site
+                # (radii stay below P/2)
                 dz = abs(self.dRdz) * h
-                r = self.R[ix, iy] + self.dRdz * (Z - self.z1)
-                rho = np.sqrt((X - (self.x0 + ix * self.P)) ** 2 + (Y - (self.y0 + iy * self.P)) ** 2)
-                side = np.abs(rho - r) <= hd + dz
-                # pillar boundaries near a lattice-cell edge: also flag cells within
-                # reach of the neighbouring pillar by testing the cell as a whole
-                edge = (np.abs(np.mod(X - self.x0 + self.P / 2, self.P) - self.P / 2) > self.P / 2 - self.rmax - hd) | \
-                       (np.abs(np.mod(Y - self.y0 + self.P / 2, self.P) - self.P / 2) > self.P / 2 - self.rmax - hd)
-                return near & (zface | side | edge)
+                ix0 = np.rint((X - self.x0) / self.P).astype(np.int64)
+                iy0 = np.rint((Y - self.y0) / self.P).astype(np.int64)
+                side = np.zeros(np.broadcast(X, Y, Z if self.dRdz else 0.0).shape, dtype=bool)
+                for di in (-1, 0, 1):
+                    for dj in (-1, 0, 1):
+                        ix, iy = ix0 + di, iy0 + dj
+                        ok = (ix >= 0) & (ix < self.R.shape[0]) & (iy >= 0) & (iy < self.R.shape[1])
+                        ixc = np.clip(ix, 0, self.R.shape[0] - 1)
+                        iyc = np.clip(iy, 0, self.R.shape[1] - 1)
+                        r = self.R[ixc, iyc] + (self.dRdz * (Z - self.z1) if self.dRdz else 0.0)
+                        rho = np.sqrt((X - (self.x0 + ixc * self.P)) ** 2 + (Y - (self.y0 + iyc * self.P)) ** 2)
+                        side |= ok & (np.abs(rho - r) <= hd + dz)
+                return near & (zface | side)
             # polygon: distance to any edge
             xs, ys = self.xy[:, 0], self.xy[:, 1]
             dmin = np.full(np.broadcast(X, Y).shape, np.inf)
@@ -310,46 +324,92 @@ def epsComponents3D(x, y, z, nBg: float, shapes, NSub: int = 4, Period=None,
         shift[c] = h
         X = (x + shift[0])[:, None, None]
         Y = (y + shift[1])[None, :, None]
-        Z = (z + shift[2])[None, None, :]
-        Xf, Yf = _fold(X, Lx), _fold(Y, Ly)
-        shape3 = (x.size, y.size, z.size)
-        # material at the cell centres
-        e = np.full(shape3, float(nBg) ** 2)
-        band = np.zeros(shape3, dtype=bool)
-        for s in sh:
-            Xb, Yb, Zb = np.broadcast_arrays(Xf, Yf, Z)
-            e[s.inside(Xb, Yb, Zb)] = s.n ** 2
-            band |= s.band(Xb, Yb, Zb, h)
-        if NSub > 1 and band.any():
-            ii, jj, kk = np.nonzero(band)
-            cx, cy, cz = X.ravel()[ii], Y.ravel()[jj], Z.ravel()[kk]
-            m = ii.size
+        Zall = z + shift[2]
+        # planes whose cells no shape face crosses and that lie inside the
+        # same z-ranges of z-extruded shapes carry the same x-y map: compute
+        # one representative of each such class, and every other plane alone
+        rep, inv = _z_classes(Zall, sh, h)
+        e = _component(c, X, Y, Zall[rep][None, None, :], sh, nBg, h, d, off, NSub, Lx, Ly, Method)
+        out[name] = np.ascontiguousarray(e[:, :, inv]) if rep.size < Zall.size else e
+    return out
+
+
+def _z_classes(Z: np.ndarray, sh: list, h: float):
+    """(representative plane indices, plane -> representative map)."""
+    n = Z.size
+    everything = (np.arange(n), np.arange(n))
+    zb = []
+    for s in sh:
+        if not s.z_extruded():
+            return everything
+        for v in (s.lo[2], s.hi[2]):
+            if np.isfinite(v):
+                zb.append(float(v))
+    zb = np.array(sorted(set(zb)))
+    if zb.size == 0:
+        face = np.zeros(n, dtype=bool)
+        keys = np.zeros((n, 0), dtype=bool)
+    else:
+        face = (np.abs(Z[:, None] - zb[None, :]) <= h).any(axis=1)
+        keys = Z[:, None] >= zb[None, :]
+    rep, inv, seen = [], np.empty(n, dtype=np.int64), {}
+    for k in range(n):
+        key = None if face[k] else keys[k].tobytes()
+        if key is not None and key in seen:
+            inv[k] = seen[key]
+            continue
+        inv[k] = len(rep)
+        if key is not None:
+            seen[key] = len(rep)
+        rep.append(k)
+    return np.array(rep, dtype=np.int64), inv
+
+
+def _component(c, X, Y, Z, sh, nBg, h, d, off, NSub, Lx, Ly, Method):
+    """One eps component at cell centres X (nx,1,1), Y (1,ny,1), Z (1,1,nz)."""
+    Xf, Yf = _fold(X, Lx), _fold(Y, Ly)
+    shape3 = (X.shape[0], Y.shape[1], Z.shape[2])
+    # material at the cell centres
+    e = np.full(shape3, float(nBg) ** 2)
+    band = np.zeros(shape3, dtype=bool)
+    for s in sh:
+        e[np.broadcast_to(s.inside(Xf, Yf, Z), shape3)] = s.n ** 2
+        band |= np.broadcast_to(s.band(Xf, Yf, Z, h), shape3)
+    if NSub > 1 and band.any():
+        ii, jj, kk = np.nonzero(band)
+        cx, cy, cz = X.ravel()[ii], Y.ravel()[jj], Z.ravel()[kk]
+        m = ii.size
+        val = np.empty(m)
+        # sub-sample in bounded chunks of band cells (memory: chunk x NSub^3)
+        step = max(1, (1 << 22) // (NSub ** 3))
+        for q0 in range(0, m, step):
+            q1 = min(m, q0 + step)
             # samples s[m, a, b, c] with a along x, b along y, c along z
-            sx = cx[:, None] + off[None, :] * d
-            sy = cy[:, None] + off[None, :] * d
-            sz = cz[:, None] + off[None, :] * d
+            sx = cx[q0:q1, None] + off[None, :] * d
+            sy = cy[q0:q1, None] + off[None, :] * d
+            sz = cz[q0:q1, None] + off[None, :] * d
             SX = _fold(sx[:, :, None, None], Lx)
             SY = _fold(sy[:, None, :, None], Ly)
             SZ = sz[:, None, None, :]
             SXb, SYb, SZb = np.broadcast_arrays(SX, SY, SZ)
             es = np.full(SXb.shape, float(nBg) ** 2)
             for s in sh:
-                es[s.inside(SXb, SYb, SZb)] = s.n ** 2
+                es[np.broadcast_to(s.inside(SXb, SYb, SZb), es.shape)] = s.n ** 2
+            mq = q1 - q0
             if Method == "directional":
                 inv_along = (1.0 / es).mean(axis=1 + c)                 # harmonic along c
-                val = (1.0 / inv_along).reshape(m, -1).mean(axis=1)
+                val[q0:q1] = (1.0 / inv_along).reshape(mq, -1).mean(axis=1)
             elif Method == "kottke":
-                mean_e = es.reshape(m, -1).mean(axis=1)
-                mean_inv = (1.0 / es).reshape(m, -1).mean(axis=1)
+                mean_e = es.reshape(mq, -1).mean(axis=1)
+                mean_inv = (1.0 / es).reshape(mq, -1).mean(axis=1)
                 grads = []
                 for ax in range(3):
                     w = off.reshape([-1 if a == ax else 1 for a in range(3)])
-                    grads.append((es * w[None]).reshape(m, -1).sum(axis=1))
+                    grads.append((es * w[None]).reshape(mq, -1).sum(axis=1))
                 gn = np.sqrt(sum(g * g for g in grads))
                 nc2 = np.where(gn > 0, (grads[c] / np.where(gn > 0, gn, 1.0)) ** 2, 0.0)
-                val = 1.0 / (nc2 * mean_inv + (1.0 - nc2) / mean_e)
+                val[q0:q1] = 1.0 / (nc2 * mean_inv + (1.0 - nc2) / mean_e)
             else:
                 raise ValueError('Method must be "directional" or "kottke"')
-            e[ii, jj, kk] = val
-        out[name] = e
-    return out
+        e[ii, jj, kk] = val
+    return e

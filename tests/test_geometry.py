@@ -79,3 +79,45 @@ def test_slab_modes_te_tm():
     assert abs(np.sqrt(w[0]) / k0 - m["neff"][0]) < 1e-12
     mt = slabModes(z, np.sqrt(epsw[0, :]), 1.55, "TM")
     assert 2.0 < mt["neff"][0] < m["neff"][0]
+
+
+def _eps3d_every_cell_sampled(x, y, z, nBg, shapes, c, NSub=4):
+    """Directional average with every cell sub-sampled (no interface band)."""
+    from opticrcwafdtd_b200.geometry import _Shape, _offsets, _shape_list
+    sh = [_Shape(k, p) for k, p in _shape_list(shapes)]
+    d = x[1] - x[0]
+    off = _offsets(NSub) * d
+    shift = np.zeros(3)
+    shift[c] = d / 2
+    X = (x + shift[0])[:, None] + off[None, :]
+    Y = (y + shift[1])[:, None] + off[None, :]
+    Z = (z + shift[2])[:, None] + off[None, :]
+    SX = X[:, None, None, :, None, None]
+    SY = Y[None, :, None, None, :, None]
+    SZ = Z[None, None, :, None, None, :]
+    SX, SY, SZ = np.broadcast_arrays(SX, SY, SZ)
+    es = np.full(SX.shape, float(nBg) ** 2)
+    for s in sh:
+        es[s.inside(SX, SY, SZ)] = s.n ** 2
+    inv_along = (1.0 / es).mean(axis=3 + c)
+    return (1.0 / inv_along).reshape(x.size, y.size, z.size, -1).mean(axis=3)
+
+
+def test_eps_components_3d_band_covers_every_interface():
+    """Cells outside the interface band are homogeneous: the band-limited
+    average equals sub-sampling every cell (pillar lattice, cylinder, cone,
+    boxes), and extruded planes shared between z classes stay exact."""
+    rng = np.random.default_rng(7)
+    d = 0.02
+    x = (np.arange(26) + 0.5) * d
+    y = (np.arange(24) + 0.5) * d
+    z = np.arange(30) * d
+    shapes = [["box", [-np.inf, np.inf, -np.inf, np.inf, -np.inf, 0.17, 1.46]],
+              ["lattice", dict(x0=0.1, y0=0.1, period=0.2, R=rng.uniform(0.03, 0.09, (3, 3)), z1=0.17, z2=0.43,
+                               n=2.4)],
+              ["cyl", [0.25, 0.2, 0.07, 0.45, 0.55, 3.0]],
+              ["cone", [0.3, 0.25, 0.03, 0.1, 0.05, 0.3, 1.8]]]
+    e = epsComponents3D(x, y, z, 1.0, shapes)
+    for c, k in enumerate("xyz"):
+        ref = _eps3d_every_cell_sampled(x, y, z, 1.0, shapes, c)
+        np.testing.assert_allclose(e[k], ref, rtol=1e-13, atol=0)
