@@ -9,6 +9,14 @@ sums.  The fields (2 x 72 MB ping-pong + 12 MB material index) exceed the
 126 MB L2, so no flush is needed between timed steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload pixel2d|pillar3d|coupler_batch|serve]
+
+pixel2d (the default) is the headline above.  The other workloads measure
+the remaining paths, each printing its own JSON line: pillar3d (3D TiO2
+pillar lattice, 600 x 600 x 300, 6000 steps), coupler_batch (256 uneven 2D
+grating couplers, 10000 steps each, one batched call per step) and serve (a
+Poisson stream of mixed 2D / 3D jobs through the serving loop: jobs/s, p50 /
+p99 latency, flux error of sampled jobs against the FP64 form).
 
 Under torchrun every rank runs its own replica of the job on its GPU (a
 single job fits one GPU: "replicas only", weak scaling); rank 0 prints one
@@ -44,6 +52,14 @@ def parse():
     ap.add_argument("--cpu-sample-steps", type=int, default=300)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--workload", default="pixel2d", choices=["pixel2d", "pillar3d", "coupler_batch", "serve"],
+                    help="pixel2d is the headline; the others measure the 3D, batched and served paths")
+    ap.add_argument("--batch", type=int, default=256)
+    ap.add_argument("--serve-jobs", type=int, default=32)
+    ap.add_argument("--serve-rate", type=float, default=0.5)
+    ap.add_argument("--serve-max-cells", type=float, default=5e7)
+    ap.add_argument("--serve-macro", type=int, default=500)
+    ap.add_argument("--serve-check", type=int, default=4)
     return ap.parse_args()
 
 
@@ -167,20 +183,49 @@ def run_reference(args):
     }), flush=True)
 
 
-def main():
-    args = parse()
-    if args.impl == "reference":
-        run_reference(args)
-        return
-    rank, world, local = dist_env()
+def _init_dist(local, world):
     import torch
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
+    if world <= 1:
+        return None
+    import torch.distributed as dist
+    from datetime import timedelta
+    dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    return dist
+
+
+def _max_over_ranks(dist, v):
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([v], device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def _roofline(st, bpc, kernel, kind="interior"):
+    """Roofline of the dominant step kernel from its per-launch CUDA events."""
+    peak, peak_kind = measured_peaks()
+    ms, launches, cu = st[f"{kind}_ms"], st[f"{kind}_launches"], st[f"{kind}_cell_updates"]
+    if ms <= 0 or launches <= 0:
+        return None
+    per_launch_bytes = bpc * cu / launches
+    launch_s = ms / 1e3 / launches
+    achieved = per_launch_bytes / launch_s / 1e9
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
+            "traffic": None, "kernel": kernel, "algorithmic_bytes_per_cell_update": bpc,
+            "cell_updates_per_launch": cu / launches, "avg_launch_ms": launch_s * 1e3}
+
+
+def bench_pixel2d(args, rank, world, local, dist):
+    """Headline: whole 2D TM pixel-region jobs, device-resident inputs."""
+    import torch
     from opticrcwafdtd_b200 import Context, Job, fdtd2D, workloads
 
     sim = workloads.pixel_region_sim(precision=args.precision, steps=args.time_steps)
@@ -197,14 +242,8 @@ def main():
 
     for _ in range(args.warmup):
         one_job()
-    ctx.reset_stats()
-    ctx.set_timing(True)
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    barrier()
+    # timed region: the production path (chunk sequence replayed as CUDA graphs)
+    _barrier(dist)
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
@@ -213,34 +252,27 @@ def main():
             one_job()
         ev1.record(stream)
         torch.cuda.synchronize()
-    barrier()
-    ms = ev0.elapsed_time(ev1)
+    _barrier(dist)
+    ms = _max_over_ranks(dist, ev0.elapsed_time(ev1))
+    value = cells * nsteps * args.steps * world / (ms / 1e3) / 1e6
+    launches_per_job = None
+
+    # one more job with CUDA events around every launch (graphs off): per-kernel
+    # durations for the roofline and the launch count
+    ctx.reset_stats()
+    ctx.set_timing(True)
+    one_job()
+    torch.cuda.synchronize()
     st = ctx.stats()
     ctx.set_timing(False)
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = cells * nsteps * args.steps * world / (ms / 1e3) / 1e6
-    launches = st["interior_launches"] + st["frame_launches"] + st["flush_launches"]
-
-    # ---- roofline of the dominant (interior) kernel
-    peak, peak_kind = measured_peaks()
+    launches_per_job = st["interior_launches"] + st["frame_launches"] + st["flush_launches"]
     bpc = BYTES_PER_CELL_UPDATE[("TM", args.precision)]
-    roof = None
-    if st["interior_ms"] > 0:
-        per_launch_bytes = bpc * st["interior_cell_updates"] / st["interior_launches"]
-        launch_s = st["interior_ms"] / 1e3 / st["interior_launches"]
-        achieved = per_launch_bytes / launch_s / 1e9
+    roof = _roofline(st, bpc, "k_step2d_fast (interior tiles, PML=false)")
+    if roof:
         tpc = ncu_traffic_per_cell_update()
-        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
-                "traffic": (tpc * st["interior_cell_updates"] / st["interior_launches"]) if tpc else None,
-                "kernel": "k_step2d_fast (interior tiles)",
-                "algorithmic_bytes_per_cell_update": bpc,
-                "avg_launch_ms": launch_s * 1e3,
-                "share_of_step_kernels": st["interior_ms"] / max(1e-9, st["interior_ms"] + st["frame_ms"]),
-                "frame_kernel_avg_launch_ms": st["frame_ms"] / max(1, st["frame_launches"])}
+        roof["traffic"] = tpc * roof["cell_updates_per_launch"] if tpc else None
+        roof["share_of_step_kernels"] = st["interior_ms"] / max(1e-9, st["interior_ms"] + st["frame_ms"])
+        roof["frame_kernel_avg_launch_ms"] = st["frame_ms"] / max(1, st["frame_launches"])
 
     # ---- end to end through the public API (host arrays in, host arrays out)
     e2e = None
@@ -251,18 +283,15 @@ def main():
             warnings.simplefilter("ignore")
             fdtd2D(sim, ctx=ectx)   # warm
             ectx.reset_stats()
-            barrier()
+            _barrier(dist)
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             for _ in range(args.steps):
-                out = fdtd2D(sim, ctx=ectx)
+                fdtd2D(sim, ctx=ectx)
             torch.cuda.synchronize()
             te = time.perf_counter() - t0
         es = ectx.stats()
-        if dist is not None:
-            t = torch.tensor([te], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            te = float(t.item())
+        te = _max_over_ranks(dist, te)
         e2e = {"value": cells * nsteps * args.steps * world / te / 1e6, "unit": UNIT,
                "h2d_bytes_per_step": es["h2d_bytes"] // args.steps, "d2h_bytes_per_step": es["d2h_bytes"] // args.steps,
                "note": "orf.fdtd2D(sim): host eps arrays -> material index + tables -> device, "
@@ -272,7 +301,7 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(sim, args.cpu_sample_steps)
-
+    line = None
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -284,14 +313,194 @@ def main():
                        "cells": cells, "time_steps_per_job": nsteps,
                        "precision": "FP32 fields, FP32+Kahan DFT, FP64 phases" if args.precision == "single"
                        else "FP64", "parallelism": f"replicas x{world}",
-                       "l2": "inputs larger than L2 (156 MB working set > 126 MB)"},
-            "gpu_launches": launches,
+                       "l2": "inputs larger than L2 (156 MB working set > 126 MB)",
+                       "timed_path": "CUDA-graph chunk replays, timing events off"},
+            "gpu_launches": launches_per_job * args.steps,
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
-            "kernel_ms": {"interior": st["interior_ms"], "frame": st["frame_ms"], "flush_check": st["flush_ms"]},
+            "kernel_ms_one_job": {"interior": st["interior_ms"], "frame": st["frame_ms"],
+                                  "flush_check": st["flush_ms"]},
         }
-        print(json.dumps(line), flush=True)
     job.close()
     ctx.close()
+    return line
+
+
+def bench_pillar3d(args, rank, world, local, dist):
+    """3D TiO2 pillar lattice, 600 x 600 x 300 at 20 nm, 3 DFT planes."""
+    import torch
+    from opticrcwafdtd_b200 import Context, Job, workloads
+    nsteps = args.time_steps if args.time_steps != 30000 else 6000
+    sim = workloads.pillar_lattice_sim(steps=nsteps, precision=args.precision)
+    cells = sim["x"].size * sim["y"].size * sim["z"].size
+    stream = torch.cuda.current_stream()
+    ctx = Context(local, stream=stream.cuda_stream)
+    job = Job(sim, ctx, dims=3)
+
+    def one_job():
+        job.reset()
+        job.advance(nsteps)
+
+    for _ in range(args.warmup):
+        one_job()
+    _barrier(dist)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            one_job()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    _barrier(dist)
+    ms = _max_over_ranks(dist, ev0.elapsed_time(ev1))
+    ctx.reset_stats()
+    ctx.set_timing(True)
+    job.reset()
+    job.advance(min(nsteps, 1000))
+    torch.cuda.synchronize()
+    st = ctx.stats()
+    ctx.set_timing(False)
+    bpc = 51 if args.precision == "single" else 99
+    roof = _roofline(st, bpc, "k_h3d + k_e3d (one time step, interior and CPML tiles)")
+    line = None
+    if rank == 0:
+        line = {"metric": METRIC, "value": cells * nsteps * args.steps * world / (ms / 1e3) / 1e6, "unit": UNIT,
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32" if args.precision == "single" else "f64",
+                "data": "synthetic (seeded TiO2 pillar radii U[60,180] nm)",
+                "config": {"workload": "3D pillar lattice 600x600x300 dx=20nm, periodic x/y, 20-cell CPML z, "
+                                       "532 nm plane wave, 3 DFT planes", "cells": cells,
+                           "time_steps_per_job": nsteps, "parallelism": f"replicas x{world}",
+                           "l2": "inputs larger than L2"},
+                "roofline": roof, "clocks": clk.summary(),
+                "hbm_gbs_algorithmic": bpc * cells * nsteps * args.steps / (ms / 1e3) / 1e9}
+    job.close()
+    ctx.close()
+    return line
+
+
+def bench_coupler_batch(args, rank, world, local, dist):
+    """256 uneven 2D TE grating couplers advanced together (orf_batch2d_run)."""
+    import torch
+    from opticrcwafdtd_b200 import Context, fdtd2D_batch, workloads
+    nsteps = args.time_steps if args.time_steps != 30000 else 10000
+    sims = workloads.coupler_batch_sims(n=args.batch, steps=nsteps, precision=args.precision)
+    cu = sum(s["x"].size * s["z"].size for s in sims) * nsteps
+    stream = torch.cuda.current_stream()
+    ctx = Context(local, stream=stream.cuda_stream)
+    import warnings
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        for _ in range(args.warmup):
+            fdtd2D_batch(sims, ctx)
+        _barrier(dist)
+        torch.cuda.synchronize()
+        with ClockSampler(local) as clk:
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                fdtd2D_batch(sims, ctx)
+            torch.cuda.synchronize()
+            te = time.perf_counter() - t0
+    _barrier(dist)
+    te = _max_over_ranks(dist, te)
+    line = None
+    if rank == 0:
+        line = {"metric": METRIC, "value": cu * args.steps * world / te / 1e6, "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": te * 1e3 / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32" if args.precision == "single" else "f64",
+                "data": "synthetic (seeded grating parameters)",
+                "config": {"workload": f"{args.batch} 2D TE grating couplers 600-1200 x 250-350 dx=20nm, "
+                                       f"51-lambda DFT, {nsteps} steps each, one orf_batch2d_run per step",
+                           "jobs_per_s": args.batch * args.steps * world / te, "parallelism": f"replicas x{world}",
+                           "timed_path": "host sims -> device -> results on host (end to end)"},
+                "clocks": clk.summary()}
+    ctx.close()
+    return line
+
+
+def bench_serve(args, rank, world, local, dist):
+    """Poisson stream of mixed 2D / 3D jobs through the serving loop."""
+    import numpy as np
+    import torch
+    from opticrcwafdtd_b200 import Context, Server, fdtd2D, fdtd3D, workloads
+    stream_jobs = workloads.serve_stream(n_jobs=args.serve_jobs, rate=args.serve_rate, seed=5 + rank,
+                                         cells=(2e5, args.serve_max_cells))
+    ctx = Context(local, stream=torch.cuda.current_stream().cuda_stream)
+    import warnings
+    warnings.simplefilter("ignore")
+    # warm the kernels once on a small job of each kind
+    warm = workloads.serve_stream(n_jobs=4, seed=99, cells=(2e5, 4e5), steps=(200, 300), frac3d=0.5)
+    srv = Server(ctx, macro_steps=args.serve_macro)
+    for j in warm:
+        srv.submit(j["sim"], dims=j["dims"])
+    srv.drain()
+    srv.close()
+    srv = Server(ctx, macro_steps=args.serve_macro)
+    _barrier(dist)
+    torch.cuda.synchronize()
+    tickets = []
+    nxt = 0
+    with ClockSampler(local) as clk:
+        t0 = srv.clock()
+        while True:
+            now = srv.clock() - t0
+            while nxt < len(stream_jobs) and stream_jobs[nxt]["t"] <= now:
+                tickets.append(srv.submit(stream_jobs[nxt]["sim"], dims=stream_jobs[nxt]["dims"]))
+                nxt += 1
+            q, r = srv.pending()
+            if q == 0 and r == 0:
+                if nxt >= len(stream_jobs):
+                    break
+                time.sleep(max(0.0, min(0.05, stream_jobs[nxt]["t"] - now)))
+                continue
+            srv.step()
+        span = srv.clock() - t0
+    infos = [srv.info(t) for t in tickets]
+    lat = np.array([i["t_done"] - i["t_submit"] for i in infos])
+    cu = sum(j["cells"] * j["steps"] for j in stream_jobs)
+    # per-job error of the FP32 results against the FP64 plain form, on a sample
+    errs = []
+    for q in range(min(args.serve_check, len(tickets))):
+        j = stream_jobs[q]
+        s64 = dict(j["sim"], precision="double")
+        o32 = srv.result(tickets[q])
+        o64 = fdtd2D(s64, ctx) if j["dims"] == 2 else fdtd3D(s64, ctx)
+        f32, f64 = np.asarray(o32["flux"]), np.asarray(o64["flux"])
+        errs.append(float(np.max(np.abs(f32 - f64)) / max(1e-300, np.max(np.abs(f64)))))
+    srv.close()
+    ctx.close()
+    if rank != 0:
+        return None
+    return {"metric": "jobs/s", "value": len(tickets) * world / span, "unit": "jobs/s", "n_gpus": world,
+            "steps": 1, "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded Poisson stream, random grating / pillar geometries)",
+            "config": {"workload": f"served stream of {len(tickets)} jobs, Poisson rate {args.serve_rate}/s, "
+                                   f"80% 2D grating couplers / 20% 3D pillar lattices, cells log-uniform "
+                                   f"[2e5, {args.serve_max_cells:.0e}], steps U[2000, 20000], FP32",
+                       "macro_steps": args.serve_macro, "parallelism": f"replicas x{world}"},
+            "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                          "max": float(lat.max())},
+            "mcell_updates_per_s": cu / span / 1e6, "makespan_s": span,
+            "flux_rel_err_vs_fp64": {"jobs": len(errs), "max": max(errs) if errs else None},
+            "clocks": clk.summary()}
+
+
+WORKLOADS = {"pixel2d": bench_pixel2d, "pillar3d": bench_pillar3d, "coupler_batch": bench_coupler_batch,
+             "serve": bench_serve}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    rank, world, local = dist_env()
+    dist = _init_dist(local, world)
+    line = WORKLOADS[args.workload](args, rank, world, local, dist)
+    if rank == 0 and line is not None:
+        print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
 

@@ -183,6 +183,10 @@ ORF_API int32_t     orf_device_count(void);
 /* Creates a context on `device`.  `stream` is a cudaStream_t or NULL (the
  * context then creates its own non-blocking stream). */
 ORF_API int32_t orf_ctx_create(int32_t device, void* stream, orf_ctx** out);
+/* Releases the caller's reference.  Every job and server built on the
+ * context holds one more, so the context (its stream, tuning and counters)
+ * lives until the last of them is destroyed: contexts, jobs and servers may
+ * be destroyed in any order. */
 ORF_API int32_t orf_ctx_destroy(orf_ctx* ctx);
 ORF_API int32_t orf_ctx_set_tuning(orf_ctx* ctx, const orf_tuning* t);
 ORF_API int32_t orf_ctx_set_timing(orf_ctx* ctx, int32_t on);

@@ -26,6 +26,15 @@ orf_ctx* default_ctx(int* status) {
     return ctxs[dev];
 }
 
+void ctx_retain(orf_ctx* c) { c->refs.fetch_add(1); }
+
+void ctx_release(orf_ctx* c) {
+    if (c->refs.fetch_sub(1) != 1) return;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
 }  // namespace orf
 
 extern "C" {
@@ -86,9 +95,7 @@ int32_t orf_ctx_create(int32_t device, void* stream, orf_ctx** out) {
 
 int32_t orf_ctx_destroy(orf_ctx* c) {
     if (!c) return ORF_EINVAL;
-    if (c->stream) cudaStreamSynchronize(c->stream);
-    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
-    delete c;
+    ctx_release(c);
     return ORF_OK;
 }
 
@@ -150,12 +157,16 @@ int32_t orf_fdtd2d_run(const orf_sim2d* sim, orf_out2d* out, orf_progress_fn pro
 
 int32_t orf_job2d_create(orf_ctx* ctx, const orf_sim2d* sim, orf_job** job) {
     if (!ctx || !job) return ORF_EINVAL;
-    return make_job2d(ctx, sim, job);
+    const int st = make_job2d(ctx, sim, job);
+    if (st == ORF_OK) ctx_retain(ctx);
+    return st;
 }
 
 int32_t orf_job3d_create(orf_ctx* ctx, const orf_sim3d* sim, orf_job** job) {
     if (!ctx || !job) return ORF_EINVAL;
-    return make_job3d(ctx, sim, job);
+    const int st = make_job3d(ctx, sim, job);
+    if (st == ORF_OK) ctx_retain(ctx);
+    return st;
 }
 
 int32_t orf_job_advance(orf_job* job, int64_t nsteps) {
@@ -178,7 +189,10 @@ int32_t orf_job_get_fields(orf_job* job, double* const* f, int32_t nf) {
     return (job && f) ? job->get_fields(f, nf) : ORF_EINVAL;
 }
 int32_t orf_job_destroy(orf_job* job) {
+    if (!job) return ORF_OK;
+    orf_ctx* c = job->ctx;
     delete job;
+    ctx_release(c);
     return ORF_OK;
 }
 

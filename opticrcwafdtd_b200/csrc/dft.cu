@@ -67,13 +67,21 @@ k_flush(const DftStream* __restrict__ streams, const FlushItem* __restrict__ ite
         const long long n0 = s_n0;
         const double dt = S.st->S;
         const int nlg = min(kFlushLambdas, S.nl - w.l0);
-        for (int q = threadIdx.x; q < nlg * count; q += blockDim.x) {
-            const int l = q / count, j = q % count;
-            const double t = ((double)(n0 + j) + (S.half ? 0.5 : 1.0)) * dt;
-            double sn, cs;
-            sincos(S.omega[w.l0 + l] * t, &sn, &cs);
-            ph[l][j][0] = (R)(cs * dt);
-            ph[l][j][1] = (R)(sn * dt);
+        // phases of the chunk's steps; zero past the last step of a partial
+        // chunk, since those slots are multiplied by zero samples below and
+        // shared memory may hold any bit pattern (0 * NaN = NaN)
+        for (int q = threadIdx.x; q < nlg * kChunk; q += blockDim.x) {
+            const int l = q / kChunk, j = q % kChunk;
+            R c = R(0), s = R(0);
+            if (j < count) {
+                const double t = ((double)(n0 + j) + (S.half ? 0.5 : 1.0)) * dt;
+                double sn, cs;
+                sincos(S.omega[w.l0 + l] * t, &sn, &cs);
+                c = (R)(cs * dt);
+                s = (R)(sn * dt);
+            }
+            ph[l][j][0] = c;
+            ph[l][j][1] = s;
         }
         __syncthreads();
         const int e = w.e0 + threadIdx.x;

@@ -8,6 +8,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <atomic>
 #include <memory>
 #include <string>
 #include <vector>
@@ -156,7 +157,15 @@ struct orf_ctx {
     bool timing = false;
     orf_kernel_stats stats{};
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // references: the creator's, plus one per job or server built on the
+    // context; the context is freed when the last one is released
+    std::atomic<int> refs{1};
 };
+
+namespace orf {
+void ctx_retain(orf_ctx* c);
+void ctx_release(orf_ctx* c);
+}  // namespace orf
 
 // A device-resident run (2D or 3D).  Implemented in job2d.cu / job3d.cu.
 struct orf_job {

@@ -339,6 +339,7 @@ int32_t orf_serve_open(orf_ctx* ctx, const orf_serve_cfg* cfg, orf_server** srv)
     // whole chunks; at most half the status ring between two reads of it
     s->chunks_per_step = std::max(1, std::min(kStatusRing / 2, (macro + kChunk - 1) / kChunk));
     s->t0 = now_s();
+    ctx_retain(ctx);
     *srv = s.release();
     return ORF_OK;
 }
@@ -419,7 +420,10 @@ int32_t orf_serve_pending(orf_server* srv, int32_t* queued, int32_t* resident) {
 double orf_serve_clock(orf_server* srv) { return srv ? srv->clock() : 0.0; }
 
 int32_t orf_serve_close(orf_server* srv) {
+    if (!srv) return ORF_OK;
+    orf_ctx* c = srv->ctx;
     delete srv;
+    ctx_release(c);
     return ORF_OK;
 }
 

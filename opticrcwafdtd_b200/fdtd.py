@@ -45,6 +45,7 @@ class Context:
 
     def close(self) -> None:
         if self.handle:
+            # releases this reference; jobs and servers keep the context alive
             self._lib.orf_ctx_destroy(self.handle)
             self.handle = None
 

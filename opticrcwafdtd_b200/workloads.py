@@ -187,3 +187,57 @@ def pillar_lattice_sim(nx: int = 600, ny: int = 600, nz: int = 300, d: float = 0
                monitors=mons, lambdas=np.linspace(0.52, 0.545, n_lambda) if n_lambda > 1 else [0.532],
                maxTime=steps * S, shutoff=0.0, precision=precision)
     return sim
+
+
+def _coupler_instance(nx: int, nz: int, period: float, ff: float, etch: float, steps: int, precision: str,
+                      n_lambda: int) -> dict:
+    """One uniform SOI grating coupler on an nx x nz grid at 20 nm (the
+    coupler_batch_sims layout)."""
+    dx = 0.02
+    width = nx * dx
+    n_per = max(4, int((width - 4.0) / period))
+    x = np.arange(nx) * dx
+    z = np.arange(nz) * dx - 0.4 * nz * dx + dx / 2
+    boxes = grating_coupler_geometry(period, ff, etch, n_per=n_per, x_start=2.5, n_clad=1.444,
+                                     box=min(2.0, 0.35 * nz * dx))
+    e = epsComponents2D(x, z, N_SIO2, boxes)
+    ix = 51
+    neff, prof = core_mode(z, np.sqrt(e["y"][ix - 1, :]), 1.55)
+    S = 0.99 / math.sqrt(2) * dx
+    kup = int(np.argmin(np.abs(z - 1.22))) + 1
+    sim = dict(pol="TE", x=x, z=z, eps=e["y"], npml=[20, 20], lambdas=np.linspace(1.5, 1.6, n_lambda),
+               monitors=[ix - 25, ix + 10, nx - 30], monitorsZ=[kup], maxTime=steps * S, shutoff=0.0,
+               precision=precision)
+    sim["source"] = dict(ix=ix, profile=prof, neff=neff, lambda0=1.55, bw=BW_100NM)
+    return sim
+
+
+def serve_stream(n_jobs: int = 32, seed: int = 5, rate: float = 1.0, cells=(2e5, 5e7), steps=(2000, 20000),
+                 frac3d: float = 0.2, precision: str = "single", n_lambda: int = 21) -> list[dict]:
+    """A served stream: Poisson arrivals (rate jobs/s) of mixed jobs, frac3d
+    of them 3D pillar lattices and the rest 2D grating couplers, cell counts
+    log-uniform in [cells], step budgets uniform in [steps] (shutoff off, so
+    every job runs its budget).  Returns [{"t", "dims", "cells", "steps",
+    "sim"}] in arrival order."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    jobs = []
+    for _ in range(n_jobs):
+        t += rng.exponential(1.0 / rate)
+        is3d = rng.random() < frac3d
+        nc = math.exp(rng.uniform(math.log(cells[0]), math.log(cells[1])))
+        st = int(rng.integers(steps[0], steps[1] + 1))
+        if is3d:
+            # nx = ny = 2 nz, lattice-commensurate (20 cells per 400 nm period), nz >= 120
+            nz = max(120, int(round((nc / 4) ** (1 / 3))))
+            nxy = max(20, int(round(math.sqrt(nc / nz) / 20)) * 20)
+            sim = pillar_lattice_sim(nx=nxy, ny=nxy, nz=nz, seed=int(rng.integers(1 << 30)), steps=st,
+                                     precision=precision, n_lambda=3)
+            jobs.append(dict(t=t, dims=3, cells=nxy * nxy * nz, steps=st, sim=sim))
+        else:
+            nz = max(150, int(round(math.sqrt(nc / 3))))
+            nx = max(400, int(round(nc / nz)))
+            period, ff, etch = rng.uniform(0.56, 0.70), rng.uniform(0.3, 0.7), rng.uniform(0.05, 0.12)
+            sim = _coupler_instance(nx, nz, period, ff, etch, st, precision, n_lambda)
+            jobs.append(dict(t=t, dims=2, cells=nx * nz, steps=st, sim=sim))
+    return jobs

@@ -204,3 +204,39 @@ def test_fp32_many_tiles_against_fp64_oracle():
     assert np.max(np.abs(out["flux"] - ref["flux"])) / scale < 1e-4
     for a, b in zip(out["fields"], ref["fields"]):
         assert rel_l2(a, b) < 1e-4
+
+
+@pytest.mark.parametrize("precision", ["double", "single"])
+def test_partial_last_chunk_large_grid_is_finite(precision):
+    """A step budget that ends inside a chunk (1344 = 26 x 50 + 44 steps) on a
+    grid with tens of DFT flush blocks: every DFT line stays finite, whatever
+    shared memory held before (the flush weights steps past the budget by
+    exact zeros), and FP32 agrees with FP64."""
+    from opticrcwafdtd_b200 import workloads
+    sim = workloads._coupler_instance(3213, 1071, 0.63, 0.5, 0.07, 1344, precision, 21)
+    out = orf.fdtd2D(sim)
+    for k in ("flux", "fluxZ", "P", "B", "PZ", "AZ"):
+        assert np.isfinite(out[k]).all(), k
+    assert out["steps"] == 1344
+    if precision == "single":
+        ref = orf.fdtd2D(dict(sim, precision="double"))
+        assert np.max(np.abs(out["flux"] - ref["flux"])) / np.max(np.abs(ref["flux"])) < 1e-4
+
+
+def test_context_may_be_released_before_its_job_and_server():
+    """Jobs and servers hold a reference to their context: releasing the
+    context first (as a garbage collector may do) leaves them working."""
+    sim = cases.mixed_te_sim(nx=200, nz=100, steps=150, precision="single")
+    ref = orf.fdtd2D(sim)
+    ctx = Context(0)
+    job = Job(sim, ctx)
+    srv = orf.Server(ctx)
+    ctx.close()
+    job.advance(150)
+    out = job.finish()
+    job.close()
+    t = srv.submit(sim)
+    srv.drain()
+    assert np.array_equal(srv.result(t)["flux"], ref["flux"])
+    assert np.array_equal(out["flux"], ref["flux"])
+    srv.close()
