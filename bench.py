@@ -56,7 +56,7 @@ def parse():
                     help="pixel2d is the headline; the others measure the 3D, batched and served paths")
     ap.add_argument("--batch", type=int, default=256)
     ap.add_argument("--serve-jobs", type=int, default=32)
-    ap.add_argument("--serve-rate", type=float, default=0.5)
+    ap.add_argument("--serve-rate", type=float, default=0.33)
     ap.add_argument("--serve-max-cells", type=float, default=5e7)
     ap.add_argument("--serve-macro", type=int, default=500)
     ap.add_argument("--serve-check", type=int, default=4)

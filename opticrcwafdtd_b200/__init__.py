@@ -11,6 +11,7 @@ a GPU is missing.
 from ._abi import NotConvergedWarning, OrfError  # noqa: F401
 from .geometry import epsCellMean, epsComponents2D, epsComponents3D, epsFromBoxes  # noqa: F401
 from .modes import slabModes  # noqa: F401
+from .coupler import fiberCoupling, gratingCouplerTE, gratingCouplerTE_batch  # noqa: F401
 
 __version__ = "0.1.0"
 from .fdtd import Context, Job, Server, device_count, fdtd2D, fdtd2D_batch, fdtd2DTE, fdtd3D  # noqa: F401,E402

@@ -16,7 +16,10 @@
 //     only the inner output rectangle is valid and written back; fields
 //     ping-pong between two buffers so overlapping tiles never race;
 //   - the update coefficients come from a uint8/uint16 material index and a
-//     table of C/eps (exact), expanded into a shared coefficient plane;
+//     table of C/eps (exact), looked up once per tile into registers;
+//   - no memory access depends on a runtime branch inside the stencil loop:
+//     neighbour-warp columns are read with 16-byte vector loads from a valid
+//     slot (a tile-edge warp reads its own, a halo value) and selected;
 //   - the CTA is persistent and software-pipelined over its tiles: while tile
 //     t computes, the cp.async prefetch of tile t+1 (fields, material index)
 //     and the descriptor and job-state snapshot of tile t+2 are in flight.
@@ -76,15 +79,40 @@ __device__ __forceinline__ int slab_half(int u, int n, int np) {   // positions 
 }
 
 // Dynamic shared memory: prefetch planes of P, A, B and the material index,
-// coefficient planes, then (PML) four psi planes and the row / column CPML
-// profiles of the tile.
+// then (PML) four psi planes and the row / column CPML profiles of the tile.
 template <class R, class IT, bool TE, bool PML, int KS, int WX, int WZ>
 constexpr size_t dyn_smem() {
     constexpr size_t LX = 32 * WX, LZ = (size_t)KS * WZ, cells = LX * LZ;
     constexpr size_t idxb = ((cells * sizeof(IT) * (TE ? 1 : 2)) + 15) & ~size_t(15);
-    size_t b = cells * sizeof(R) * 3 + idxb + cells * sizeof(R) * (TE ? 1 : 2);
+    size_t b = cells * sizeof(R) * 3 + idxb;
     if (PML) b += cells * sizeof(R) * 4 + (LZ + LX) * 6 * sizeof(R);
     return b;
+}
+
+// 16 bytes of an exchange row (16-byte aligned) into registers
+template <class R>
+__device__ __forceinline__ void load16(R (&dst)[16 / sizeof(R)], const R* src) {
+    if constexpr (sizeof(R) == 4) {
+        const float4 v = *reinterpret_cast<const float4*>(src);
+        dst[0] = v.x; dst[1] = v.y; dst[2] = v.z; dst[3] = v.w;
+    } else {
+        const double2 v = *reinterpret_cast<const double2*>(src);
+        dst[0] = v.x; dst[1] = v.y;
+    }
+}
+template <class R, int KS>
+__device__ __forceinline__ void store_row(R* dst, const R (&src)[KS]) {
+    if constexpr (sizeof(R) == 4 && KS % 4 == 0) {
+#pragma unroll
+        for (int q = 0; q < KS / 4; ++q)
+            reinterpret_cast<float4*>(dst)[q] = make_float4(src[4 * q], src[4 * q + 1], src[4 * q + 2], src[4 * q + 3]);
+    } else if constexpr (sizeof(R) == 8 && KS % 2 == 0) {
+#pragma unroll
+        for (int q = 0; q < KS / 2; ++q) reinterpret_cast<double2*>(dst)[q] = make_double2(src[2 * q], src[2 * q + 1]);
+    } else {
+#pragma unroll
+        for (int j = 0; j < KS; ++j) dst[j] = src[j];
+    }
 }
 
 template <class R, class IT, bool TE, bool PML, int KS, int WX, int WZ>
@@ -105,18 +133,16 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
     R* pfB = pfA + CELLS;
     IT* pfI = reinterpret_cast<IT*>(pfB + CELLS);     // NIDX planes
     constexpr size_t idxb = ((CELLS * sizeof(IT) * NIDX) + 15) & ~size_t(15);
-    R* c0s = reinterpret_cast<R*>(reinterpret_cast<unsigned char*>(pfI) + idxb);
-    R* c1s = c0s + CELLS;                                // TM only
-    R* psA = c0s + (TE ? 1 : 2) * CELLS;                 // PML only: psi of A (z), B (x), P (x), P (z)
+    R* psA = reinterpret_cast<R*>(reinterpret_cast<unsigned char*>(pfI) + idxb);   // PML only: psi of A (z), B (x), P (x), P (z)
     R* psB = psA + CELLS;
     R* psPx = psB + CELLS;
     R* psPz = psPx + CELLS;
     R* prz = psPz + CELLS;                               // PML only: [LZ][6] rows: zP b,a,k ; zA b,a,k
     R* prx = prz + LZ * 6;                               // PML only: [LX][6] cols: xP b,a,k ; xB b,a,k
 
-    __shared__ R xPc[NW][KS];
+    __shared__ __align__(16) R xPc[NW][KS];
     __shared__ R xPr[NW][32];
-    __shared__ R xBc[NW][KS];
+    __shared__ __align__(16) R xBc[NW][KS];
     __shared__ R xAr[NW][32];
     __shared__ R slut[256];
     __shared__ const R* s_lutsrc;
@@ -133,6 +159,10 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
     const int wz = warp / WX;
     const int cx = 32 * wx + lane;
     const int ck0 = KS * wz;
+    // neighbour warps in the tile; a warp on the tile edge names itself
+    const bool hasR = wx + 1 < WX, hasL = wx > 0, hasDn = wz + 1 < WZ, hasUp = wz > 0;
+    const int wR = hasR ? warp + 1 : warp, wL = hasL ? warp - 1 : warp;
+    const int wDn = hasDn ? warp + WX : warp, wUp = hasUp ? warp - WX : warp;
 
     // ---- prefetch one tile's fields and material index into the shared buffer
     auto prefetch = [&](const FastTile2D& d) {
@@ -299,8 +329,9 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
                 }
             }
         }
-        // shared buffer -> registers / coefficient planes
-        R P[KS], A[KS], B[KS];
+        // shared buffer -> registers: fields and update coefficients
+        // (TE: K0 = C/eps of P; TM: K0 = C/eps of A, K1 = C/eps of B)
+        R P[KS], A[KS], B[KS], K0[KS], K1[KS];
 #pragma unroll
         for (int j = 0; j < KS; ++j) {
             const int c = (ck0 + j) * LX + cx;
@@ -308,13 +339,15 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
             A[j] = pfA[c];
             B[j] = pfB[c];
             const int v0 = (int)pfI[c];
-            c0s[c] = sizeof(IT) == 1 ? slut[v0] : __ldg(I->lutc + v0);
+            K0[j] = sizeof(IT) == 1 ? slut[v0] : __ldg(I->lutc + v0);
             if (!TE) {
                 const int v1 = (int)pfI[CELLS + c];
-                c1s[c] = sizeof(IT) == 1 ? slut[v1] : __ldg(I->lutc + v1);
+                K1[j] = sizeof(IT) == 1 ? slut[v1] : __ldg(I->lutc + v1);
+            } else {
+                K1[j] = R(0);
             }
         }
-        __syncthreads();   // shared buffer free; coefficient planes, sg and CPML state ready
+        __syncthreads();   // shared buffer free; sg and CPML state ready
         if (tn < ntiles) {
             prefetch(s_desc[ns]);
             fetch_state(ns);
@@ -350,19 +383,21 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
             }
             for (int s = 0; s < nsub; ++s) {
                 // ----- H half step: A (d/dz P), B (d/dx P)
-                if (lane == 0) {
-#pragma unroll
-                    for (int j = 0; j < KS; ++j) xPc[warp][j] = P[j];
-                }
+                if (lane == 0) store_row<R, KS>(&xPc[warp][0], P);
                 xPr[warp][lane] = P[0];
                 __syncthreads();
-                const R Pdn = (wz + 1 < WZ) ? xPr[warp + WX][lane] : (PML ? R(0) : P[KS - 1]);
+                R Pdn = xPr[wDn][lane];
+                if (!hasDn) Pdn = PML ? R(0) : P[KS - 1];
+                constexpr int VEC = 16 / sizeof(R);
+                static_assert(KS % VEC == 0, "KS must be a multiple of 16 bytes of R");
+                R pe[VEC];
 #pragma unroll
                 for (int j = 0; j < KS; ++j) {
                     const int c = (ck0 + j) * LX + cx;
+                    if (j % VEC == 0) load16<R>(pe, &xPc[wR][j]);
                     R pr = __shfl_down_sync(FULL, P[j], 1);
-                    const R pe = (wx + 1 < WX) ? xPc[warp + 1][j] : (PML ? R(0) : pr);
-                    pr = (lane == 31) ? pe : pr;
+                    const R pej = (PML && !hasR) ? R(0) : pe[j % VEC];
+                    pr = (lane == 31) ? pej : pr;
                     const R pk = (j + 1 < KS) ? P[j + 1] : Pdn;
                     R dz = pk - P[j];
                     R dx = pr - P[j];
@@ -375,8 +410,8 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
                         psB[c] = qs;
                         dx = dx * phk + qs;
                     }
-                    const R ca = TE ? C : c0s[c];
-                    const R cb = TE ? C : c1s[c];
+                    const R ca = TE ? C : K0[j];
+                    const R cb = TE ? C : K1[j];
                     if (PML) {
                         if ((mA >> j) & 1u) A[j] += ca * dz;
                         if ((mB >> j) & 1u) B[j] -= cb * dx;
@@ -396,19 +431,19 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
                     }
                 }
                 // ----- E half step: P (branch-free stencil loop)
-                if (lane == 31) {
-#pragma unroll
-                    for (int j = 0; j < KS; ++j) xBc[warp][j] = B[j];
-                }
+                if (lane == 31) store_row<R, KS>(&xBc[warp][0], B);
                 xAr[warp][lane] = A[KS - 1];
                 __syncthreads();
-                const R Aup = (wz > 0) ? xAr[warp - WX][lane] : (PML ? R(0) : A[0]);
+                R Aup = xAr[wUp][lane];
+                if (!hasUp) Aup = PML ? R(0) : A[0];
+                R be[VEC];
 #pragma unroll
                 for (int j = 0; j < KS; ++j) {
                     const int c = (ck0 + j) * LX + cx;
+                    if (j % VEC == 0) load16<R>(be, &xBc[wL][j]);
                     R bl = __shfl_up_sync(FULL, B[j], 1);
-                    const R be = (wx > 0) ? xBc[warp - 1][j] : (PML ? R(0) : bl);
-                    bl = (lane == 0) ? be : bl;
+                    const R bej = (PML && !hasL) ? R(0) : be[j % VEC];
+                    bl = (lane == 0) ? bej : bl;
                     const R am = (j > 0) ? A[j - 1] : Aup;
                     R da = A[j] - am;
                     R db = B[j] - bl;
@@ -421,7 +456,7 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
                         psPx[c] = qs;
                         db = db * pxk + qs;
                     }
-                    const R cp = TE ? c0s[c] : C;
+                    const R cp = TE ? K0[j] : C;
                     if (PML) {
                         if ((mP >> j) & 1u) P[j] += cp * (da - db);
                     } else {
@@ -444,9 +479,10 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
                     R* smp0 = I->samples + (size_t)sslot * I->sstride;
 #pragma unroll
                     for (int j = 0; j < KS; ++j) {
+                        if (j % VEC == 0) load16<R>(be, &xBc[wL][j]);
                         R bl = __shfl_up_sync(FULL, B[j], 1);
-                        const R be = (wx > 0) ? xBc[warp - 1][j] : (PML ? R(0) : bl);
-                        bl = (lane == 0) ? be : bl;
+                        const R bej = (PML && !hasL) ? R(0) : be[j % VEC];
+                        bl = (lane == 0) ? bej : bl;
                         if (xm >= 0 && ((own >> j) & 1u)) {
                             R* smp = smp0 + (size_t)xm * 2 * nz;
                             smp[kb + j] = P[j];

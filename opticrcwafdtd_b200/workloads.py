@@ -99,9 +99,14 @@ def grating_coupler_geometry(period=0.63, ff=0.5, etch=0.07, n_per=20, box=2.0, 
     return boxes
 
 
-def core_mode(z, n, lambda0, pol="TE", core=(0.0, 0.22), n_modes=8, eps_half=None):
+def core_mode(z, n, lambda0, pol="TE", core=(0.0, 0.22), n_modes=8, eps_half=None, substrate_top=None):
     """The guided mode of the Si core (not a substrate mode): the slab mode
-    with the largest share of |field|^2 inside the core."""
+    with the largest share of |field|^2 inside the core.  With substrate_top
+    given, the Si substrate below it is replaced by oxide for the mode solve,
+    so a thick substrate's many guided modes cannot crowd the core mode out."""
+    n = np.asarray(n, dtype=float)
+    if substrate_top is not None:
+        n = np.where(np.asarray(z) < substrate_top, N_SIO2, n)
     m = slabModes(z, n, lambda0, pol, n_modes, EpsHalf=eps_half)
     inside = (z >= core[0]) & (z <= core[1])
     frac = [np.sum(m["field"][inside, q] ** 2) / np.sum(m["field"][:, q] ** 2) for q in range(n_modes)]
@@ -202,7 +207,7 @@ def _coupler_instance(nx: int, nz: int, period: float, ff: float, etch: float, s
                                      box=min(2.0, 0.35 * nz * dx))
     e = epsComponents2D(x, z, N_SIO2, boxes)
     ix = 51
-    neff, prof = core_mode(z, np.sqrt(e["y"][ix - 1, :]), 1.55)
+    neff, prof = core_mode(z, np.sqrt(e["y"][ix - 1, :]), 1.55, substrate_top=-min(2.0, 0.35 * nz * dx))
     S = 0.99 / math.sqrt(2) * dx
     kup = int(np.argmin(np.abs(z - 1.22))) + 1
     sim = dict(pol="TE", x=x, z=z, eps=e["y"], npml=[20, 20], lambdas=np.linspace(1.5, 1.6, n_lambda),
