@@ -55,6 +55,7 @@ def parse():
     ap.add_argument("--workload", default="pixel2d", choices=["pixel2d", "pillar3d", "coupler_batch", "serve"],
                     help="pixel2d is the headline; the others measure the 3D, batched and served paths")
     ap.add_argument("--batch", type=int, default=256)
+    ap.add_argument("--size3d", default="600,600,300", help="pillar3d grid NX,NY,NZ (smaller for profiling)")
     ap.add_argument("--serve-jobs", type=int, default=32)
     ap.add_argument("--serve-rate", type=float, default=0.33)
     ap.add_argument("--serve-max-cells", type=float, default=5e7)
@@ -330,7 +331,8 @@ def bench_pillar3d(args, rank, world, local, dist):
     import torch
     from opticrcwafdtd_b200 import Context, Job, workloads
     nsteps = args.time_steps if args.time_steps != 30000 else 6000
-    sim = workloads.pillar_lattice_sim(steps=nsteps, precision=args.precision)
+    nx3, ny3, nz3 = (int(v) for v in args.size3d.split(","))
+    sim = workloads.pillar_lattice_sim(nx=nx3, ny=ny3, nz=nz3, steps=nsteps, precision=args.precision)
     cells = sim["x"].size * sim["y"].size * sim["z"].size
     stream = torch.cuda.current_stream()
     ctx = Context(local, stream=stream.cuda_stream)
@@ -369,7 +371,7 @@ def bench_pillar3d(args, rank, world, local, dist):
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32" if args.precision == "single" else "f64",
                 "data": "synthetic (seeded TiO2 pillar radii U[60,180] nm)",
-                "config": {"workload": "3D pillar lattice 600x600x300 dx=20nm, periodic x/y, 20-cell CPML z, "
+                "config": {"workload": f"3D pillar lattice {nx3}x{ny3}x{nz3} dx=20nm, periodic x/y, 20-cell CPML z, "
                                        "532 nm plane wave, 3 DFT planes", "cells": cells,
                            "time_steps_per_job": nsteps, "parallelism": f"replicas x{world}",
                            "l2": "inputs larger than L2"},

@@ -187,15 +187,20 @@ def gratingCouplerTE(p: Any = None, ctx=None) -> dict:
 
 def gratingCouplerTE_batch(ps, ctx=None, progress=None) -> list[dict]:
     """gratingCouplerTE for many parameter sets, advanced together by one
-    orf_batch2d_run submission (all sets must share the precision)."""
+    orf_batch2d_run submission (all sets must share the precision).  Under an
+    initialised torch.distributed process group (one process per GPU) the
+    sets are sharded across ranks by grid size and every rank returns all
+    results."""
     from .fdtd import fdtd2D_batch
+    from .replicas import sharded_map
     built = [gratingCouplerTE_sim(p) for p in ps]
     sims = []
     for s, _ in built:
         s = dict(s)
         s.pop("progress", None)
         sims.append(s)
-    outs = fdtd2D_batch(sims, ctx, progress)
+    costs = [s["x"].size * s["z"].size for s in sims]
+    outs = sharded_map(lambda part: fdtd2D_batch(part, ctx, progress), sims, costs)
     return [coupler_budget(o, bd) for o, (_, bd) in zip(outs, built)]
 
 

@@ -1,7 +1,9 @@
 """Pins the CPU oracle against the reference's own FDTD tests, at the
 reference's tolerances.  The reference's implementation is closed P-code
-(toolbox/+orf/fdtd2D.p) and cannot run here, so these physics checks (and the
-golden fixtures in tests/golden/) are what ties the oracle to it."""
+(toolbox/+orf/fdtd2D.p) and cannot run here, and the reference stores no
+golden vectors, so these physics checks (TMM slab R/T, exact-Yee dispersion,
+unidirectional source, empty-domain reflection, single vs double) are what
+ties the oracle to it."""
 import numpy as np
 import pytest
 
