@@ -205,7 +205,10 @@ int Job3D<R>::create(const orf_sim3d* s) {
         if (np <= 0) return false;
         return lo < np + 1 || hi > n[q] - np - 2;
     };
-    zc = ctx->tuning.variant == 2 ? 8 : 4;   // planes per thread (compiled unroll depths)
+    // planes per thread (compiled depths 4 and 2): all loads of the planes are
+    // issued before the updates, which FP32 affords for 4 planes and FP64 for 2
+    const int zc_default = sizeof(R) == 4 ? 4 : 2;
+    zc = ctx->tuning.variant == 2 ? 6 - zc_default : zc_default;
     for (int k0 = 0; k0 < n[2]; k0 += zc)
         for (int j0 = 0; j0 < n[1]; j0 += kTile3Y)
             for (int i0 = 0; i0 < n[0]; i0 += kTile3X) {

@@ -207,7 +207,7 @@ int step2d_blocks_per_sm(bool fp64, bool te, bool idx16, bool pml, int variant);
 
 constexpr int kTile3X = 32, kTile3Y = 8;   // 3D CTA tile (x, y)
 // H then E half step of one time step (in place).  zc = planes per thread (a
-// compiled unroll depth: 4 or 8); tiles span <= zc planes.  pml = false only
+// compiled unroll depth: 4 or 2); tiles span <= zc planes.  pml = false only
 // for tiles with no cell near a CPML slab.
 cudaError_t launch_h3d(bool fp64, int zc, bool pml, const void* insts, const Tile3D* tiles, int ntiles,
                        int launch_off, cudaStream_t s);

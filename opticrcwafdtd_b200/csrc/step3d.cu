@@ -8,10 +8,12 @@
 // One time step = the H kernel then the E kernel, each updating its fields
 // in place (the H update reads only E, the E update only H, so no second
 // buffer is needed and the 3D state takes 6 arrays, not 12).  A thread owns
-// one (x, y) column and marches ZC planes of it (unrolled, so the loads of
-// several planes are in flight together); the z-neighbour of the previous
-// plane is carried in registers, x/y neighbours come from the L1 lines the
-// neighbouring threads of the same CTA load.  Tiles that touch no CPML slab
+// one (x, y) column and marches ZC planes of it: every load of the ZC planes
+// is issued before the first update (the kernel reads the other field set
+// only and each updated cell belongs to one thread, so the loads can all be
+// in flight), the z-neighbour of the previous plane comes from the same
+// register arrays, x/y neighbours from the L1 lines the neighbouring threads
+// of the same CTA load.  Tiles that touch no CPML slab
 // run an instantiation without any CPML code.  Every thread does the same
 // work, so neither kernel needs a barrier or shared memory.
 #include "orf_internal.cuh"
@@ -88,7 +90,6 @@ k_h3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, int
     const bool px = I->per[0] != 0, py = I->per[1] != 0, pz = I->per[2] != 0;
     const size_t plane = (size_t)ny * pitch;
     const R C = I->C;
-    const R gE = (R)(n < I->nsrc ? I->gE[n] : 0.0);
     const int sa = I->sa, sb = (sa + 1) % 3, sc = (sa + 2) % 3, ss = I->ss;
     const int i = tile.i0 + tx, j = tile.j0 + ty;
     bool iok, jok;
@@ -101,33 +102,50 @@ k_h3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, int
     R* __restrict__ H1 = I->H[0][1];
     R* __restrict__ H2 = I->H[0][2];
     const size_t cij = (size_t)j * pitch + i;
-    R ex = E0[(size_t)tile.k0 * plane + cij], ey = E1[(size_t)tile.k0 * plane + cij];
+    const size_t ci = (size_t)j * pitch + ip, cj = (size_t)jp * pitch + i;
+    // all loads of the ZC planes first (E is read-only in this kernel, and
+    // each H cell is read and written by its own thread), so they are in
+    // flight together; then the updates and stores
+    R ex[ZC + 1], ey[ZC + 1], ez[ZC], ezi[ZC], eyi[ZC], ezj[ZC], exj[ZC], h0[ZC], h1[ZC], h2[ZC];
+    ex[0] = __ldg(E0 + (size_t)tile.k0 * plane + cij);
+    ey[0] = __ldg(E1 + (size_t)tile.k0 * plane + cij);
+#pragma unroll
+    for (int kq = 0; kq < ZC; ++kq) {
+        const int k = tile.k0 + kq;
+        const bool kin = k < tile.k1;
+        bool kok;
+        const int kp = wrap(k + 1, nz, pz, &kok);
+        const size_t o = (size_t)k * plane;
+        const size_t ok = (size_t)kp * plane + cij;
+        ex[kq + 1] = (kin && kok) ? __ldg(E0 + ok) : R(0);
+        ey[kq + 1] = (kin && kok) ? __ldg(E1 + ok) : R(0);
+        ez[kq] = kin ? __ldg(E2 + o + cij) : R(0);
+        ezi[kq] = (kin && iok) ? __ldg(E2 + o + ci) : R(0);
+        eyi[kq] = (kin && iok) ? __ldg(E1 + o + ci) : R(0);
+        ezj[kq] = (kin && jok) ? __ldg(E2 + o + cj) : R(0);
+        exj[kq] = (kin && jok) ? __ldg(E0 + o + cj) : R(0);
+        h0[kq] = kin ? H0[o + cij] : R(0);
+        h1[kq] = kin ? H1[o + cij] : R(0);
+        h2[kq] = kin ? H2[o + cij] : R(0);
+    }
+    const R gE = (R)(n < I->nsrc ? I->gE[n] : 0.0);
 #pragma unroll
     for (int kq = 0; kq < ZC; ++kq) {
         const int k = tile.k0 + kq;
         if (k >= tile.k1) break;
-        bool kok;
-        const int kp = wrap(k + 1, nz, pz, &kok);
         const size_t o = (size_t)k * plane + cij;
-        const size_t oi = (size_t)k * plane + (size_t)j * pitch + ip;
-        const size_t oj = (size_t)k * plane + (size_t)jp * pitch + i;
-        const size_t ok = (size_t)kp * plane + cij;
-        const R ez = E2[o];
-        const R ex_k = kok ? E0[ok] : R(0), ey_k = kok ? E1[ok] : R(0);
-        const R ez_i = iok ? E2[oi] : R(0), ey_i = iok ? E1[oi] : R(0);
-        const R ez_j = jok ? E2[oj] : R(0), ex_j = jok ? E0[oj] : R(0);
         // Hx -= C ((Ez(j+1) - Ez) - (Ey(k+1) - Ey))
-        R d1 = cpml<PML>(I, true, 0, 1, j, i, j, k, ez_j - ez);
-        R d2 = cpml<PML>(I, true, 0, 2, k, i, j, k, ey_k - ey);
-        R hx = H0[o] - C * (d1 - d2);
+        R d1 = cpml<PML>(I, true, 0, 1, j, i, j, k, ezj[kq] - ez[kq]);
+        R d2 = cpml<PML>(I, true, 0, 2, k, i, j, k, ey[kq + 1] - ey[kq]);
+        R hx = h0[kq] - C * (d1 - d2);
         // Hy -= C ((Ex(k+1) - Ex) - (Ez(i+1) - Ez))
-        d1 = cpml<PML>(I, true, 1, 2, k, i, j, k, ex_k - ex);
-        d2 = cpml<PML>(I, true, 1, 0, i, i, j, k, ez_i - ez);
-        R hy = H1[o] - C * (d1 - d2);
+        d1 = cpml<PML>(I, true, 1, 2, k, i, j, k, ex[kq + 1] - ex[kq]);
+        d2 = cpml<PML>(I, true, 1, 0, i, i, j, k, ezi[kq] - ez[kq]);
+        R hy = h1[kq] - C * (d1 - d2);
         // Hz -= C ((Ey(i+1) - Ey) - (Ex(j+1) - Ex))
-        d1 = cpml<PML>(I, true, 2, 0, i, i, j, k, ey_i - ey);
-        d2 = cpml<PML>(I, true, 2, 1, j, i, j, k, ex_j - ex);
-        R hz = H2[o] - C * (d1 - d2);
+        d1 = cpml<PML>(I, true, 2, 0, i, i, j, k, eyi[kq] - ey[kq]);
+        d2 = cpml<PML>(I, true, 2, 1, j, i, j, k, exj[kq] - ex[kq]);
+        R hz = h2[kq] - C * (d1 - d2);
         // TF/SF: the H plane just below the source plane is scattered field
         if (sel3(sa, i, j, k) == ss - 1) {
             const size_t pq = (size_t)sel3(sb, i, j, k) + (size_t)I->na * sel3(sc, i, j, k);
@@ -139,8 +157,6 @@ k_h3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, int
         H0[o] = hx;
         H1[o] = hy;
         H2[o] = hz;
-        ex = ex_k;
-        ey = ey_k;
     }
 }
 
@@ -160,7 +176,6 @@ k_e3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, int
         const int nx = I->n[0], ny = I->n[1], nz = I->n[2], pitch = I->pitch;
         const bool px = I->per[0] != 0, py = I->per[1] != 0, pz = I->per[2] != 0;
         const size_t plane = (size_t)ny * pitch;
-        const R gH = (R)(n < I->nsrc ? I->gH[n] : 0.0);
         const int sa = I->sa, sb = (sa + 1) % 3, sc = (sa + 2) % 3, ss = I->ss;
         const int i = tile.i0 + tx, j = tile.j0 + ty;
         bool iok, jok, kok;
@@ -173,33 +188,55 @@ k_e3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, int
         const R* __restrict__ H1 = I->H[0][1];
         const R* __restrict__ H2 = I->H[0][2];
         const size_t cij = (size_t)j * pitch + i;
+        const size_t ci = (size_t)j * pitch + im, cj = (size_t)jm * pitch + i;
+        // loads of the ZC planes first (H is read-only here; each E cell is
+        // read and written by its own thread), then the updates
         const int km0 = wrap(tile.k0 - 1, nz, pz, &kok);
-        R hxm = kok ? H0[(size_t)km0 * plane + cij] : R(0);
-        R hym = kok ? H1[(size_t)km0 * plane + cij] : R(0);
+        R hx[ZC + 1], hy[ZC + 1], hz[ZC], hyi[ZC], hzi[ZC], hxj[ZC], hzj[ZC], e0[ZC], e1[ZC], e2[ZC];
+        int v0[ZC], v1[ZC], v2[ZC];
+        hx[0] = kok ? __ldg(H0 + (size_t)km0 * plane + cij) : R(0);
+        hy[0] = kok ? __ldg(H1 + (size_t)km0 * plane + cij) : R(0);
+#pragma unroll
+        for (int kq = 0; kq < ZC; ++kq) {
+            const int k = tile.k0 + kq;
+            const bool kin = k < tile.k1;
+            const size_t o = (size_t)k * plane;
+            hx[kq + 1] = kin ? __ldg(H0 + o + cij) : R(0);
+            hy[kq + 1] = kin ? __ldg(H1 + o + cij) : R(0);
+            hz[kq] = kin ? __ldg(H2 + o + cij) : R(0);
+            hyi[kq] = (kin && iok) ? __ldg(H1 + o + ci) : R(0);
+            hzi[kq] = (kin && iok) ? __ldg(H2 + o + ci) : R(0);
+            hxj[kq] = (kin && jok) ? __ldg(H0 + o + cj) : R(0);
+            hzj[kq] = (kin && jok) ? __ldg(H2 + o + cj) : R(0);
+            v0[kq] = kin ? ldx<IT>(I->idx[0], o + cij) : 0;
+            v1[kq] = kin ? ldx<IT>(I->idx[1], o + cij) : 0;
+            v2[kq] = kin ? ldx<IT>(I->idx[2], o + cij) : 0;
+            e0[kq] = kin ? E0[o + cij] : R(0);
+            e1[kq] = kin ? E1[o + cij] : R(0);
+            e2[kq] = kin ? E2[o + cij] : R(0);
+        }
+        const R gH = (R)(n < I->nsrc ? I->gH[n] : 0.0);
         R* smp0 = I->samples + (size_t)launch_off * I->sstride;
 #pragma unroll
         for (int kq = 0; kq < ZC; ++kq) {
             const int k = tile.k0 + kq;
             if (k >= tile.k1) break;
             const size_t o = (size_t)k * plane + cij;
-            const size_t oi = (size_t)k * plane + (size_t)j * pitch + im;
-            const size_t oj = (size_t)k * plane + (size_t)jm * pitch + i;
-            const R hx = H0[o], hy = H1[o], hz = H2[o];
-            const R hy_i = iok ? H1[oi] : R(0), hz_i = iok ? H2[oi] : R(0);
-            const R hx_j = jok ? H0[oj] : R(0), hz_j = jok ? H2[oj] : R(0);
-            const int v0 = ldx<IT>(I->idx[0], o), v1 = ldx<IT>(I->idx[1], o), v2 = ldx<IT>(I->idx[2], o);
+            const R hxk = hx[kq + 1], hyk = hy[kq + 1], hzk = hz[kq];
+            const R hxm = hx[kq], hym = hy[kq];
+            const R hy_i = hyi[kq], hz_i = hzi[kq], hx_j = hxj[kq], hz_j = hzj[kq];
             // Ex += cx ((Hz - Hz(j-1)) - (Hy - Hy(k-1)))
-            R d1 = cpml<PML>(I, false, 0, 1, j, i, j, k, hz - hz_j);
-            R d2 = cpml<PML>(I, false, 0, 2, k, i, j, k, hy - hym);
-            R ex = E0[o] + __ldg(I->lutc + v0) * (d1 - d2);
+            R d1 = cpml<PML>(I, false, 0, 1, j, i, j, k, hzk - hz_j);
+            R d2 = cpml<PML>(I, false, 0, 2, k, i, j, k, hyk - hym);
+            R ex = e0[kq] + __ldg(I->lutc + v0[kq]) * (d1 - d2);
             // Ey += cy ((Hx - Hx(k-1)) - (Hz - Hz(i-1)))
-            d1 = cpml<PML>(I, false, 1, 2, k, i, j, k, hx - hxm);
-            d2 = cpml<PML>(I, false, 1, 0, i, i, j, k, hz - hz_i);
-            R ey = E1[o] + __ldg(I->lutc + v1) * (d1 - d2);
+            d1 = cpml<PML>(I, false, 1, 2, k, i, j, k, hxk - hxm);
+            d2 = cpml<PML>(I, false, 1, 0, i, i, j, k, hzk - hz_i);
+            R ey = e1[kq] + __ldg(I->lutc + v1[kq]) * (d1 - d2);
             // Ez += cz ((Hy - Hy(i-1)) - (Hx - Hx(j-1)))
-            d1 = cpml<PML>(I, false, 2, 0, i, i, j, k, hy - hy_i);
-            d2 = cpml<PML>(I, false, 2, 1, j, i, j, k, hx - hx_j);
-            R ez = E2[o] + __ldg(I->lutc + v2) * (d1 - d2);
+            d1 = cpml<PML>(I, false, 2, 0, i, i, j, k, hyk - hy_i);
+            d2 = cpml<PML>(I, false, 2, 1, j, i, j, k, hxk - hx_j);
+            R ez = e2[kq] + __ldg(I->lutc + v2[kq]) * (d1 - d2);
             // TF/SF: the source plane is total field
             if (sel3(sa, i, j, k) == ss) {
                 const size_t pq = (size_t)sel3(sb, i, j, k) + (size_t)I->na * sel3(sc, i, j, k);
@@ -219,17 +256,17 @@ k_e3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, int
                 size_t p, npl;
                 if (ax == 2) {          // a = x, b = y
                     ea = ex; eb = ey;
-                    ha = R(0.5) * (hx + hxm); hb = R(0.5) * (hy + hym);
+                    ha = R(0.5) * (hxk + hxm); hb = R(0.5) * (hyk + hym);
                     p = (size_t)i + (size_t)nx * j;
                     npl = (size_t)nx * ny;
                 } else if (ax == 0) {   // a = y, b = z
                     ea = ey; eb = ez;
-                    ha = R(0.5) * (hy + hy_i); hb = R(0.5) * (hz + hz_i);
+                    ha = R(0.5) * (hyk + hy_i); hb = R(0.5) * (hzk + hz_i);
                     p = (size_t)j + (size_t)ny * k;
                     npl = (size_t)ny * nz;
                 } else {                // a = z, b = x
                     ea = ez; eb = ex;
-                    ha = R(0.5) * (hz + hz_j); hb = R(0.5) * (hx + hx_j);
+                    ha = R(0.5) * (hzk + hz_j); hb = R(0.5) * (hxk + hx_j);
                     p = (size_t)k + (size_t)nz * i;
                     npl = (size_t)nz * nx;
                 }
@@ -240,11 +277,10 @@ k_e3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, int
                 smp[3 * npl + p] = hb;
             }
             if (want_energy) {
-                energy += I->lute[v0] * (double)ex * ex + I->lute[v1] * (double)ey * ey +
-                          I->lute[v2] * (double)ez * ez + (double)hx * hx + (double)hy * hy + (double)hz * hz;
+                energy += I->lute[v0[kq]] * (double)ex * ex + I->lute[v1[kq]] * (double)ey * ey +
+                          I->lute[v2[kq]] * (double)ez * ez + (double)hxk * hxk + (double)hyk * hyk +
+                          (double)hzk * hzk;
             }
-            hxm = hx;
-            hym = hy;
         }
     }
     if (want_energy) {   // warp reduction, one atomic per warp (no block barrier)
@@ -261,7 +297,7 @@ cudaError_t launch_h3d(bool fp64, int zc, bool pml, const void* insts, const Til
     if (ntiles <= 0) return cudaSuccess;
 #define ORF_H3(R, Z, P) k_h3d<R, Z, P><<<ntiles, NT, 0, s>>>(reinterpret_cast<const Inst3D<R>*>(insts), tiles, launch_off)
 #define ORF_H3Z(R, P) \
-    if (zc == 4) ORF_H3(R, 4, P); else ORF_H3(R, 8, P)
+    if (zc == 4) ORF_H3(R, 4, P); else ORF_H3(R, 2, P)
     if (fp64) {
         if (pml) { ORF_H3Z(double, true); } else { ORF_H3Z(double, false); }
     } else {
@@ -278,8 +314,8 @@ cudaError_t launch_e3d(bool fp64, int zc, bool pml, int idxw, const void* insts,
 #define ORF_E3(R, IT, Z, P) \
     k_e3d<R, IT, Z, P><<<ntiles, NT, 0, s>>>(reinterpret_cast<const Inst3D<R>*>(insts), tiles, launch_off, want_energy)
 #define ORF_E3Z(R, IT) \
-    if (pml) { if (zc == 4) ORF_E3(R, IT, 4, true); else ORF_E3(R, IT, 8, true); } \
-    else { if (zc == 4) ORF_E3(R, IT, 4, false); else ORF_E3(R, IT, 8, false); }
+    if (pml) { if (zc == 4) ORF_E3(R, IT, 4, true); else ORF_E3(R, IT, 2, true); } \
+    else { if (zc == 4) ORF_E3(R, IT, 4, false); else ORF_E3(R, IT, 2, false); }
     if (fp64) {
         if (idxw == 1) { ORF_E3Z(double, uint8_t); }
         else if (idxw == 2) { ORF_E3Z(double, uint16_t); }
