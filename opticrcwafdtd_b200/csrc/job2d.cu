@@ -386,7 +386,8 @@ int Job2D<R>::create(const orf_sim2d* s) {
 template <class R>
 int Job2D<R>::pick_tiling(int npx, int npz) {
     const bool f64 = sizeof(R) == 8;
-    fvariant = ctx->tuning.variant > 0 ? ctx->tuning.variant : 1;
+    // defaults from the variant / depth sweeps on the 4000 x 1500 workload
+    fvariant = ctx->tuning.variant > 0 ? ctx->tuning.variant : (f64 ? 2 : 1);
     Variant2D fv, pv;
     if (!fast2d_info(fvariant, f64, false, &fv)) {
         set_error("unknown 2D kernel variant %d", fvariant);
@@ -395,7 +396,7 @@ int Job2D<R>::pick_tiling(int npx, int npz) {
     fast2d_info(0, f64, true, &pv);
     // a tile's output keeps T cells (plus up to 3 of x alignment) from its edges
     const int tmax = std::min({kMaxSub, (pv.lz() - 1) / 2, (pv.lx() - 4) / 2, (fv.lz() - 1) / 2, (fv.lx() - 4) / 2});
-    T = ctx->tuning.tsteps > 0 ? ctx->tuning.tsteps : 6;
+    T = ctx->tuning.tsteps > 0 ? ctx->tuning.tsteps : (f64 ? 6 : 8);
     if (T > tmax) T = tmax;
     if (T < 1) T = 1;
 

@@ -116,7 +116,7 @@ __device__ __forceinline__ void store_row(R* dst, const R (&src)[KS]) {
 }
 
 template <class R, class IT, bool TE, bool PML, int KS, int WX, int WZ>
-__global__ void __launch_bounds__(32 * WX * WZ, 1)
+__global__ void __launch_bounds__(32 * WX * WZ, (PML && sizeof(R) == 4) ? 2 : 1)
 k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, int nsub_max, int par,
               int want_energy) {
     constexpr int NW = WX * WZ;
