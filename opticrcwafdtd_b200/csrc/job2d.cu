@@ -213,8 +213,9 @@ int Job2D<R>::create(const orf_sim2d* s) {
     if (!te) ar.add(&d_ix1, cellsP * isz);
     R *d_lutc, *d_px, *d_pxh, *d_pz, *d_pzh, *d_srcB, *d_srcP, *d_samples;
     double *d_lute, *d_gE, *d_gH;
-    ar.add(&d_lutc, nlut);
-    ar.add(&d_lute, nlut);
+    // at least 256 entries: u8-index kernels copy the whole table to shared memory
+    ar.add(&d_lutc, std::max<size_t>(nlut, 256));
+    ar.add(&d_lute, std::max<size_t>(nlut, 256));
     ar.add(&d_px, px.size());
     ar.add(&d_pxh, pxh.size() + 3);
     ar.add(&d_pz, pz.size());

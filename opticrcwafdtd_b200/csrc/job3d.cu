@@ -247,8 +247,9 @@ int Job3D<R>::create(const orf_sim3d* s) {
     R *d_lutc, *d_pI[3], *d_pH[3], *d_sHa, *d_sHb, *d_sEa, *d_sEb, *d_samples;
     int *d_slI[3], *d_slH[3];
     double *d_lute, *d_gE, *d_gH;
-    ar.add(&d_lutc, nlut);
-    ar.add(&d_lute, nlut);
+    // at least 256 entries: u8-index kernels copy the whole table to shared memory
+    ar.add(&d_lutc, std::max<size_t>(nlut, 256));
+    ar.add(&d_lute, std::max<size_t>(nlut, 256));
     for (int q = 0; q < 3; ++q) {
         ar.add(&d_pI[q], pI[q].size());
         ar.add(&d_pH[q], pH[q].size());

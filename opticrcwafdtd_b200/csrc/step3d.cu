@@ -22,6 +22,7 @@ namespace orf {
 namespace {
 
 constexpr int TX = kTile3X, TY = kTile3Y, NT = TX * TY;
+static_assert(NT == 256, "the E kernel fills a 256-entry table with one entry per thread");
 
 __device__ __forceinline__ int wrap(int u, int n, bool per, bool* ok) {
     if (u >= 0 && u < n) {
@@ -68,6 +69,12 @@ __device__ __forceinline__ R cpml(const Inst3D<R>* __restrict__ I, bool half, in
     const R p = b * ps[o] + a * d;
     ps[o] = p;
     return d * ki + p;
+}
+
+template <class R, class IT>
+__device__ __forceinline__ R coef(const R* slut, const R* __restrict__ lutc, int v) {
+    if constexpr (sizeof(IT) == 1) return slut[v];
+    else return __ldg(lutc + v);
 }
 
 template <class IT>
@@ -171,6 +178,13 @@ k_e3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, int
     if (n >= st->nmax) return;
     const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
     const bool own = tx < tile.tw && ty < tile.th;
+    // u8 index: the 256-entry coefficient table in shared memory, so the
+    // coefficient lookup is not a second dependent global load
+    __shared__ R slut[sizeof(IT) == 1 ? 256 : 1];
+    if constexpr (sizeof(IT) == 1) {
+        slut[threadIdx.x] = I->lutc[threadIdx.x];
+        __syncthreads();
+    }
     double energy = 0.0;
     if (own) {
         const int nx = I->n[0], ny = I->n[1], nz = I->n[2], pitch = I->pitch;
@@ -228,15 +242,15 @@ k_e3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, int
             // Ex += cx ((Hz - Hz(j-1)) - (Hy - Hy(k-1)))
             R d1 = cpml<PML>(I, false, 0, 1, j, i, j, k, hzk - hz_j);
             R d2 = cpml<PML>(I, false, 0, 2, k, i, j, k, hyk - hym);
-            R ex = e0[kq] + __ldg(I->lutc + v0[kq]) * (d1 - d2);
+            R ex = e0[kq] + coef<R, IT>(slut, I->lutc, v0[kq]) * (d1 - d2);
             // Ey += cy ((Hx - Hx(k-1)) - (Hz - Hz(i-1)))
             d1 = cpml<PML>(I, false, 1, 2, k, i, j, k, hxk - hxm);
             d2 = cpml<PML>(I, false, 1, 0, i, i, j, k, hzk - hz_i);
-            R ey = e1[kq] + __ldg(I->lutc + v1[kq]) * (d1 - d2);
+            R ey = e1[kq] + coef<R, IT>(slut, I->lutc, v1[kq]) * (d1 - d2);
             // Ez += cz ((Hy - Hy(i-1)) - (Hx - Hx(j-1)))
             d1 = cpml<PML>(I, false, 2, 0, i, i, j, k, hyk - hy_i);
             d2 = cpml<PML>(I, false, 2, 1, j, i, j, k, hxk - hx_j);
-            R ez = e2[kq] + __ldg(I->lutc + v2[kq]) * (d1 - d2);
+            R ez = e2[kq] + coef<R, IT>(slut, I->lutc, v2[kq]) * (d1 - d2);
             // TF/SF: the source plane is total field
             if (sel3(sa, i, j, k) == ss) {
                 const size_t pq = (size_t)sel3(sb, i, j, k) + (size_t)I->na * sel3(sc, i, j, k);
