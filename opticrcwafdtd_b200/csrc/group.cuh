@@ -162,7 +162,8 @@ struct Group2D : Group {
     }
 };
 
-// 3D members share precision, z-chunk depth and index width.
+// 3D members share precision and index width (zc is the z-segment length,
+// the same for every job).
 template <class R>
 struct Group3D : Group {
     std::vector<Job3D<R>*> jobs;
@@ -237,13 +238,10 @@ struct Group3D : Group {
         wire_engine(f64, 1);
         eng.step = [this, f64](int off, int nsub, int par, int we, cudaStream_t s, KernelTimer* tm) -> cudaError_t {
             (void)nsub;
-            (void)par;
             cudaEvent_t a = nullptr;
             if (tm && tm->begin(s, &a) != ORF_OK) return cudaErrorUnknown;
-            cudaError_t e = launch_h3d(f64, zc, false, d_insts, d_tiles, nt, off, s);
-            if (e == cudaSuccess) e = launch_h3d(f64, zc, true, d_insts, d_tiles_pml, ntp, off, s);
-            if (e == cudaSuccess) e = launch_e3d(f64, zc, false, idxw, d_insts, d_tiles, nt, off, we, s);
-            if (e == cudaSuccess) e = launch_e3d(f64, zc, true, idxw, d_insts, d_tiles_pml, ntp, off, we, s);
+            cudaError_t e = launch_step3d(f64, false, idxw, d_insts, d_tiles, nt, par, off, we, s);
+            if (e == cudaSuccess) e = launch_step3d(f64, true, idxw, d_insts, d_tiles_pml, ntp, par, off, we, s);
             if (e != cudaSuccess) return e;
             if (tm && tm->end(s, 0, all_cells, a) != ORF_OK) return cudaErrorUnknown;
             return e;

@@ -196,8 +196,10 @@ int Job3D<R>::create(const orf_sim3d* s) {
         pairs.push_back({4 * m, 4 * m + 3, 4 * m + 1, 4 * m + 2, m, nM, 0.5 * d * d});
     npairs = (int)pairs.size();
 
-    // ---- tiles: kTile3X x kTile3Y columns, zc planes each; a tile is "CPML" if
-    // any cell lies within one cell of an absorbing slab along any axis
+    // ---- tiles: kTile3X x kTile3Y columns, a segment of up to kSeg3 planes
+    // each; a tile takes the CPML instantiation if any cell it updates or
+    // recomputes (one halo cell in x and y, the plane below the segment) lies
+    // within one cell of an absorbing slab along any axis
     tiles.clear();
     tiles_pml.clear();
     auto near_pml = [&](int q, int lo, int hi) {   // cells [lo, hi) along axis q
@@ -205,11 +207,18 @@ int Job3D<R>::create(const orf_sim3d* s) {
         if (np <= 0) return false;
         return lo < np + 1 || hi > n[q] - np - 2;
     };
-    // planes per thread (compiled depths 4 and 2): all loads of the planes are
-    // issued before the updates, which FP32 affords for 4 planes and FP64 for 2
-    const int zc_default = sizeof(R) == 4 ? 4 : 2;
-    zc = ctx->tuning.variant == 2 ? 6 - zc_default : zc_default;
-    for (int k0 = 0; k0 < n[2]; k0 += zc)
+    zc = kSeg3;
+    // z segments of at most kSeg3 planes that never mix planes near a z slab
+    // with planes away from it, so only the planes that need CPML code run it
+    std::vector<std::pair<int, int>> segs;
+    for (int k0 = 0; k0 < n[2];) {
+        const bool pz0 = near_pml(2, k0 - 1, k0 + 2);
+        int k1 = k0 + 1;
+        while (k1 < n[2] && k1 - k0 < kSeg3 && near_pml(2, k1 - 1, k1 + 2) == pz0) ++k1;
+        segs.push_back({k0, k1});
+        k0 = k1;
+    }
+    for (auto [k0, k1] : segs)
         for (int j0 = 0; j0 < n[1]; j0 += kTile3Y)
             for (int i0 = 0; i0 < n[0]; i0 += kTile3X) {
                 Tile3D t;
@@ -219,29 +228,29 @@ int Job3D<R>::create(const orf_sim3d* s) {
                 t.tw = (short)std::min(kTile3X, n[0] - i0);
                 t.th = (short)std::min(kTile3Y, n[1] - j0);
                 t.k0 = k0;
-                t.k1 = std::min(n[2], k0 + zc);
-                const bool pm = near_pml(0, t.i0, t.i0 + t.tw) || near_pml(1, t.j0, t.j0 + t.th) ||
-                                near_pml(2, t.k0, t.k1);
+                t.k1 = k1;
+                const bool pm = near_pml(0, t.i0 - 1, t.i0 + t.tw + 1) || near_pml(1, t.j0 - 1, t.j0 + t.th + 1) ||
+                                near_pml(2, t.k0 - 1, t.k1 + 1);
                 (pm ? tiles_pml : tiles).push_back(t);
             }
 
     // ---- device arena
-    // the H and E half-step kernels update in place: one buffer (index 0)
+    // fields and psi ping-pong: a step reads buffer par and writes par^1
     Arena ar;
-    for (int c = 0; c < 3; ++c) {
-        ar.add(&h.E[0][c], NP());
-        ar.add(&h.H[0][c], NP());
-    }
+    for (int b = 0; b < 2; ++b)
+        for (int c = 0; c < 3; ++c) {
+            ar.add(&h.E[b][c], NP());
+            ar.add(&h.H[b][c], NP());
+        }
     for (int c = 0; c < 3; ++c)
-        for (int q = 0; q < 3; ++q) {
+        for (int q = 0; q < 3; ++q)
             for (int b = 0; b < 2; ++b) {
                 h.psiE[b][c][q] = nullptr;
                 h.psiH[b][c][q] = nullptr;
+                if (q == c) continue;
+                if (nsI[q] > 0) ar.add(&h.psiE[b][c][q], N() / n[q] * nsI[q]);
+                if (nsH[q] > 0) ar.add(&h.psiH[b][c][q], N() / n[q] * nsH[q]);
             }
-            if (q == c) continue;
-            if (nsI[q] > 0) ar.add(&h.psiE[0][c][q], N() / n[q] * nsI[q]);
-            if (nsH[q] > 0) ar.add(&h.psiH[0][c][q], N() / n[q] * nsH[q]);
-        }
     unsigned char* d_ix[3];
     for (int c = 0; c < 3; ++c) ar.add(&d_ix[c], NP() * idxw);
     R *d_lutc, *d_pI[3], *d_pH[3], *d_sHa, *d_sHb, *d_sEa, *d_sEb, *d_samples;
@@ -328,10 +337,6 @@ int Job3D<R>::create(const orf_sim3d* s) {
     for (int l = 0; l < nL; ++l) om[l] = 2.0 * kPi / s->lambdas[l];
     ORF_TRY(up(d_omega, om.data(), nL * sizeof(double)));
 
-    for (int c = 0; c < 3; ++c) {
-        h.E[1][c] = h.E[0][c];
-        h.H[1][c] = h.H[0][c];
-    }
     for (int q = 0; q < 3; ++q) {
         h.n[q] = n[q];
         h.per[q] = per[q] ? 1 : 0;
@@ -398,15 +403,12 @@ int Job3D<R>::create(const orf_sim3d* s) {
     const int64_t ncell = (int64_t)N();
     eng.step = [this, ncell](int off, int nsub, int par, int we, cudaStream_t stream, KernelTimer* tm) -> cudaError_t {
         (void)nsub;
-        (void)par;
         cudaEvent_t a = nullptr;
         if (tm && tm->begin(stream, &a) != ORF_OK) return cudaErrorUnknown;
         const bool f64 = sizeof(R) == 8;
-        cudaError_t e = launch_h3d(f64, zc, false, d_inst, d_tiles, (int)tiles.size(), off, stream);
-        if (e == cudaSuccess) e = launch_h3d(f64, zc, true, d_inst, d_tiles_pml, (int)tiles_pml.size(), off, stream);
-        if (e == cudaSuccess) e = launch_e3d(f64, zc, false, idxw, d_inst, d_tiles, (int)tiles.size(), off, we, stream);
+        cudaError_t e = launch_step3d(f64, false, idxw, d_inst, d_tiles, (int)tiles.size(), par, off, we, stream);
         if (e == cudaSuccess)
-            e = launch_e3d(f64, zc, true, idxw, d_inst, d_tiles_pml, (int)tiles_pml.size(), off, we, stream);
+            e = launch_step3d(f64, true, idxw, d_inst, d_tiles_pml, (int)tiles_pml.size(), par, off, we, stream);
         if (e != cudaSuccess) return e;
         if (tm && tm->end(stream, 0, ncell, a) != ORF_OK) return cudaErrorUnknown;
         return e;
@@ -444,14 +446,17 @@ template <class R>
 int Job3D<R>::reset() {
     cudaStream_t st = ctx->stream;
     ORF_CUDA(cudaStreamSynchronize(st));
-    for (int c = 0; c < 3; ++c) {
-        ORF_CUDA(cudaMemsetAsync(h.E[0][c], 0, NP() * sizeof(R), st));
-        ORF_CUDA(cudaMemsetAsync(h.H[0][c], 0, NP() * sizeof(R), st));
-        for (int q = 0; q < 3; ++q) {
-            if (h.psiE[0][c][q]) ORF_CUDA(cudaMemsetAsync(h.psiE[0][c][q], 0, N() / n[q] * h.nslabI[q] * sizeof(R), st));
-            if (h.psiH[0][c][q]) ORF_CUDA(cudaMemsetAsync(h.psiH[0][c][q], 0, N() / n[q] * h.nslabH[q] * sizeof(R), st));
+    for (int b = 0; b < 2; ++b)
+        for (int c = 0; c < 3; ++c) {
+            ORF_CUDA(cudaMemsetAsync(h.E[b][c], 0, NP() * sizeof(R), st));
+            ORF_CUDA(cudaMemsetAsync(h.H[b][c], 0, NP() * sizeof(R), st));
+            for (int q = 0; q < 3; ++q) {
+                if (h.psiE[b][c][q])
+                    ORF_CUDA(cudaMemsetAsync(h.psiE[b][c][q], 0, N() / n[q] * h.nslabI[q] * sizeof(R), st));
+                if (h.psiH[b][c][q])
+                    ORF_CUDA(cudaMemsetAsync(h.psiH[b][c][q], 0, N() / n[q] * h.nslabH[q] * sizeof(R), st));
+            }
         }
-    }
     size_t acc_elems = 0;
     for (auto& q : host_streams) acc_elems += (size_t)q.len * nL;
     ORF_CUDA(cudaMemsetAsync(d_acc, 0, acc_elems * 16, st));
@@ -523,8 +528,7 @@ int Job3D<R>::get_fields(double* const* f, int nf) {
     ORF_CUDA(cudaStreamSynchronize(ctx->stream));
     JobState js;
     ORF_CUDA(cudaMemcpy(&js, d_st, sizeof js, cudaMemcpyDeviceToHost));
-    const int b = 0;   // in-place update: one buffer
-    (void)js;
+    const int b = js.cur;   // buffer written by the last step
     std::vector<R> tmp(NP());
     for (int q = 0; q < 6; ++q) {
         if (!f[q]) continue;

@@ -206,13 +206,12 @@ int fast2d_blocks_per_sm(bool fp64, bool te, bool idx16, bool pml, int variant);
 int step2d_blocks_per_sm(bool fp64, bool te, bool idx16, bool pml, int variant);
 
 constexpr int kTile3X = 32, kTile3Y = 8;   // 3D CTA tile (x, y)
-// H then E half step of one time step (in place).  zc = planes per thread (a
-// compiled unroll depth: 4 or 2); tiles span <= zc planes.  pml = false only
-// for tiles with no cell near a CPML slab.
-cudaError_t launch_h3d(bool fp64, int zc, bool pml, const void* insts, const Tile3D* tiles, int ntiles,
-                       int launch_off, cudaStream_t s);
-cudaError_t launch_e3d(bool fp64, int zc, bool pml, int idxw, const void* insts, const Tile3D* tiles, int ntiles,
-                       int launch_off, int want_energy, cudaStream_t s);
+constexpr int kSeg3 = 60;                  // z planes marched by one 3D CTA
+// One 3D time step (step3d_fused.cu): reads fields and psi of buffer par,
+// writes buffer par^1.  pml = false only for tiles with no cell (halo and
+// the plane below the segment included) near a CPML slab.
+cudaError_t launch_step3d(bool fp64, bool pml, int idxw, const void* insts, const Tile3D* tiles, int ntiles, int par,
+                          int launch_off, int want_energy, cudaStream_t s);
 
 cudaError_t launch_flush(bool fp64, const DftStream* streams, const FlushItem* items, int nitems,
                          cudaStream_t s);

@@ -1,0 +1,444 @@
+// step3d_fused.cu -- one 3D Yee time step per launch, H and E fused in a z-march
+// (toolbox/+orf/fdtd3D.m:1-29) for sm_100a.
+//
+//   H_c -= C (D+_c1 E_c2 - D+_c2 E_c1),   E_c += C/eps_c (D-_c1 H_c2 - D-_c2 H_c1)
+// with CPML on any axis (cpmlCoefficients.m:4-8), PEC or periodic boundaries,
+// the one-sided TF/SF plane on any axis (fdtd3D.m:15-21) and planar DFT
+// monitors with H averaged onto the E plane (fdtd3D.m:22, 26-28).
+//
+// A CTA owns a 32 x 8 column tile and a segment [k0, k1) of z planes and
+// marches it plane by plane:
+//   - plane p of E (the tile plus one halo cell on every side), H and the
+//     material index arrive in a 4-slot shared-memory ring by cp.async, up to
+//     three planes ahead of the one being updated (the wrapped / zero-filled
+//     x-y addressing of the region is computed once per CTA);
+//   - H at plane k is updated on the tile plus its low x / y halo (the halo
+//     values are recomputed, not read from the neighbour CTA, whose update of
+//     them may not have happened yet) into a shared plane; the tile's own H
+//     goes to global memory;
+//   - E at plane k is then updated from that plane and the H of plane k-1,
+//     which each thread keeps in registers from the previous iteration.
+// Fields, and CPML psi, ping-pong between two buffers (read par, write
+// par^1), so CTAs never see each other's partial results.  Each field is read
+// and written once per step: 12 values plus 3 index bytes per cell, the
+// algorithmic minimum.  The arithmetic of every update is that of the split
+// H-then-E formulation, operation for operation.
+#include "orf_internal.cuh"
+
+namespace orf {
+namespace {
+
+constexpr int TX = kTile3X, TY = kTile3Y, NT = TX * TY;
+constexpr int RX = TX + 2, RY = TY + 2, RC = RX * RY;   // E region [i0-1, i0+TX] x [j0-1, j0+TY]
+constexpr int NS = 4;                                     // planes in the ring
+constexpr int RPT = (RC + NT - 1) / NT;                   // region cells per thread
+
+__device__ __forceinline__ int wrapc(int u, int n, bool per, bool* ok) {
+    if (u >= 0 && u < n) {
+        *ok = true;
+        return u;
+    }
+    if (per) {
+        *ok = true;
+        const int r = u % n;
+        return r < 0 ? r + n : r;
+    }
+    *ok = false;
+    return 0;
+}
+
+__device__ __forceinline__ int sel3(int a, int x, int y, int z) { return a == 0 ? x : (a == 1 ? y : z); }
+
+__device__ __forceinline__ int slab(bool half, int u, int n, int np) {
+    if (np <= 0) return -1;
+    if (u < np) return u;
+    const int hi = half ? n - 1 - np : n - np;
+    return u >= hi ? np + (u - hi) : -1;
+}
+
+// CPML-stretched difference d -> d/kappa + psi, psi <- b psi + a d, reading
+// psi of buffer par and (store) writing buffer par^1
+template <bool PML, class R>
+__device__ __forceinline__ R cpml(const Inst3D<R>* __restrict__ I, int par, bool store, bool half, int c, int q,
+                                  int coord, int i, int j, int k, R d) {
+    if (!PML) return d;
+    const int sl = slab(half, coord, I->n[q], I->np[q]);
+    if (sl < 0) return d;
+    const R* prof = half ? I->pmlH[q] : I->pmlI[q];
+    const R b = prof[3 * coord], a = prof[3 * coord + 1], ki = prof[3 * coord + 2];
+    int v[3] = {i, j, k};
+    int dim[3] = {I->n[0], I->n[1], I->n[2]};
+    v[q] = sl;
+    dim[q] = half ? I->nslabH[q] : I->nslabI[q];
+    const size_t o = (size_t)v[0] + (size_t)dim[0] * ((size_t)v[1] + (size_t)dim[1] * v[2]);
+    const R* pin = half ? I->psiH[par][c][q] : I->psiE[par][c][q];
+    const R p = b * pin[o] + a * d;
+    if (store) (half ? I->psiH[par ^ 1][c][q] : I->psiE[par ^ 1][c][q])[o] = p;
+    return d * ki + p;
+}
+
+__device__ __forceinline__ void cp4(void* sdst, const void* gsrc, bool valid) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gsrc), "r"(valid ? 4u : 0u) : "memory");
+}
+__device__ __forceinline__ void cp8(void* sdst, const void* gsrc, bool valid) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gsrc), "r"(valid ? 8u : 0u) : "memory");
+}
+template <class R>
+__device__ __forceinline__ void cpR(R* sdst, const R* gsrc, bool valid) {
+    if constexpr (sizeof(R) == 4) cp4(sdst, gsrc, valid);
+    else cp8(sdst, gsrc, valid);
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+template <class R, class IT>
+constexpr size_t smem_bytes() {
+    // E and H rings, the new-H plane, the index ring (16-byte rounded)
+    return (size_t)NS * 3 * RC * sizeof(R) * 2 + (size_t)3 * RC * sizeof(R) +
+           (((size_t)NS * 3 * NT * sizeof(IT) + 15) & ~size_t(15));
+}
+
+// H update of one cell (the split formulation's operations, in order)
+template <bool PML, class R>
+__device__ __forceinline__ void h_cell(const Inst3D<R>* __restrict__ I, int par, bool store, int i, int j, int k,
+                                       R ex, R ey, R ez, R ex_k, R ey_k, R ez_i, R ey_i, R ez_j, R ex_j, R& hx, R& hy,
+                                       R& hz, R gE) {
+    const R C = I->C;
+    // Hx -= C ((Ez(j+1) - Ez) - (Ey(k+1) - Ey))
+    R d1 = cpml<PML>(I, par, store, true, 0, 1, j, i, j, k, ez_j - ez);
+    R d2 = cpml<PML>(I, par, store, true, 0, 2, k, i, j, k, ey_k - ey);
+    hx = hx - C * (d1 - d2);
+    // Hy -= C ((Ex(k+1) - Ex) - (Ez(i+1) - Ez))
+    d1 = cpml<PML>(I, par, store, true, 1, 2, k, i, j, k, ex_k - ex);
+    d2 = cpml<PML>(I, par, store, true, 1, 0, i, i, j, k, ez_i - ez);
+    hy = hy - C * (d1 - d2);
+    // Hz -= C ((Ey(i+1) - Ey) - (Ex(j+1) - Ex))
+    d1 = cpml<PML>(I, par, store, true, 2, 0, i, i, j, k, ey_i - ey);
+    d2 = cpml<PML>(I, par, store, true, 2, 1, j, i, j, k, ex_j - ex);
+    hz = hz - C * (d1 - d2);
+    // TF/SF: the H plane just below the source plane is scattered field
+    const int sa = I->sa;
+    if (sel3(sa, i, j, k) == I->ss - 1) {
+        const int sb = (sa + 1) % 3, sc = (sa + 2) % 3;
+        const size_t pq = (size_t)sel3(sb, i, j, k) + (size_t)I->na * sel3(sc, i, j, k);
+        const R ua = __ldg(I->sHa + pq) * gE, ub = __ldg(I->sHb + pq) * gE;
+        if (sa == 0) { hy += ua; hz += ub; }
+        else if (sa == 1) { hz += ua; hx += ub; }
+        else { hx += ua; hy += ub; }
+    }
+}
+
+template <class R, class IT>
+__device__ __forceinline__ R coef(const R* slut, const R* __restrict__ lutc, int v) {
+    if constexpr (sizeof(IT) == 1) return slut[v];
+    else return __ldg(lutc + v);
+}
+
+template <class R, class IT, bool PML>
+__global__ void __launch_bounds__(NT, 3)
+k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, int par, int launch_off,
+         int want_energy) {
+    const Tile3D tile = tiles[blockIdx.x];
+    const Inst3D<R>* __restrict__ I = insts + tile.inst;
+    JobState* st = I->st;
+    if (st->done) return;
+    const long long n = st->step + launch_off;
+    if (n >= st->nmax) return;
+
+    extern __shared__ __align__(16) unsigned char dsm[];
+    R* sE = reinterpret_cast<R*>(dsm);                 // [NS][3][RC]
+    R* sH = sE + NS * 3 * RC;                          // [NS][3][RC] (rows < RY-1, cols < RX-1 used)
+    R* sHn = sH + NS * 3 * RC;                         // [3][RC]
+    IT* sI = reinterpret_cast<IT*>(sHn + 3 * RC);      // [NS][3][NT]
+    __shared__ R slut[sizeof(IT) == 1 ? 256 : 1];
+
+    const int t = threadIdx.x;
+    const int tx = t % TX, ty = t / TX;
+    const int nx = I->n[0], ny = I->n[1], nz = I->n[2], pitch = I->pitch;
+    const bool px = I->per[0] != 0, py = I->per[1] != 0, pz = I->per[2] != 0;
+    const size_t plane = (size_t)ny * pitch;
+    const int i0 = tile.i0, j0 = tile.j0, k0 = tile.k0, k1 = tile.k1;
+    const R* __restrict__ Ein[3] = {I->E[par][0], I->E[par][1], I->E[par][2]};
+    const R* __restrict__ Hin[3] = {I->H[par][0], I->H[par][1], I->H[par][2]};
+
+    if constexpr (sizeof(IT) == 1) slut[t] = I->lutc[t];
+
+    // ---- region addressing, the same for every plane: offset of region cell
+    // e = t + NT r within a plane, and whether it lies inside the grid (or
+    // wraps onto it)
+    size_t roff[RPT];
+    unsigned rmask = 0;
+#pragma unroll
+    for (int r = 0; r < RPT; ++r) {
+        const int e = t + NT * r;
+        roff[r] = 0;
+        if (e < RC) {
+            const int rr = e / RX, c = e % RX;
+            bool iok, jok;
+            const int ii = wrapc(i0 - 1 + c, nx, px, &iok), jj = wrapc(j0 - 1 + rr, ny, py, &jok);
+            roff[r] = (size_t)jj * pitch + ii;
+            if (iok && jok) rmask |= 1u << r;
+        }
+    }
+    // material index of the tile's own cells: 4-byte words of its rows
+    constexpr int WPR = TX * (int)sizeof(IT) / 4;   // words per row
+    constexpr int NWI = 3 * TY * WPR;
+    static_assert(NWI <= 4 * NT, "index words per thread");
+
+    // ---- cp.async of plane p (wrapped or zero outside the grid) into slot s
+    auto load_plane = [&](int p, int s) {
+        bool pok;
+        const int pw = wrapc(p, nz, pz, &pok);
+        const size_t po = (size_t)pw * plane;
+#pragma unroll
+        for (int r = 0; r < RPT; ++r) {
+            const int e = t + NT * r;
+            if (e >= RC) break;
+            const bool v = pok && ((rmask >> r) & 1u);
+            const size_t o = po + roff[r];
+#pragma unroll
+            for (int q = 0; q < 3; ++q) cpR<R>(sE + (s * 3 + q) * RC + e, Ein[q] + o, v);
+            const int rr = e / RX, c = e - rr * RX;
+            if (rr < RY - 1 && c < RX - 1) {
+#pragma unroll
+                for (int q = 0; q < 3; ++q) cpR<R>(sH + (s * 3 + q) * RC + e, Hin[q] + o, v);
+            }
+        }
+        for (int w = t; w < NWI; w += NT) {
+            const int q = w / (TY * WPR), r = (w / WPR) % TY, cw = w % WPR;
+            const int jj = j0 + r;
+            const bool v = pok && jj < ny;
+            const size_t o = (po + (size_t)(v ? jj : 0) * pitch + i0) * sizeof(IT) + 4 * (size_t)cw;
+            cp4(reinterpret_cast<unsigned char*>(sI + (s * 3 + q) * NT) + (size_t)r * TX * sizeof(IT) + 4 * cw,
+                reinterpret_cast<const unsigned char*>(I->idx[q]) + o, v);
+        }
+    };
+
+    load_plane(k0, 0);
+    cp_commit();
+    load_plane(k0 + 1, 1);
+    cp_commit();
+    load_plane(k0 + 2, 2);
+    cp_commit();
+
+    const R gE = (R)(n < I->nsrc ? I->gE[n] : 0.0);
+    const R gH = (R)(n < I->nsrc ? I->gH[n] : 0.0);
+    const bool own = tx < tile.tw && ty < tile.th;
+    const int i = i0 + tx, j = j0 + ty;
+    R* __restrict__ Eout[3] = {I->E[par ^ 1][0], I->E[par ^ 1][1], I->E[par ^ 1][2]};
+    R* __restrict__ Hout[3] = {I->H[par ^ 1][0], I->H[par ^ 1][1], I->H[par ^ 1][2]};
+
+    // ---- H of plane k0-1 at the own column (the E update of plane k0 needs
+    // its x and y components); recomputed here, never stored
+    R hxm = R(0), hym = R(0);
+    if (own) {
+        bool kok;
+        const int km = wrapc(k0 - 1, nz, pz, &kok);
+        if (kok) {
+            bool iok, jok, kpk;
+            const int ip = wrapc(i + 1, nx, px, &iok), jp = wrapc(j + 1, ny, py, &jok);
+            const int kp = wrapc(km + 1, nz, pz, &kpk);
+            const size_t o = (size_t)km * plane + (size_t)j * pitch + i;
+            const size_t oi = (size_t)km * plane + (size_t)j * pitch + ip;
+            const size_t oj = (size_t)km * plane + (size_t)jp * pitch + i;
+            const size_t ok = (size_t)kp * plane + (size_t)j * pitch + i;
+            const R ex = __ldg(Ein[0] + o), ey = __ldg(Ein[1] + o), ez = __ldg(Ein[2] + o);
+            const R ex_k = kpk ? __ldg(Ein[0] + ok) : R(0), ey_k = kpk ? __ldg(Ein[1] + ok) : R(0);
+            const R ez_i = iok ? __ldg(Ein[2] + oi) : R(0), ey_i = iok ? __ldg(Ein[1] + oi) : R(0);
+            const R ez_j = jok ? __ldg(Ein[2] + oj) : R(0), ex_j = jok ? __ldg(Ein[0] + oj) : R(0);
+            R hx = __ldg(Hin[0] + o), hy = __ldg(Hin[1] + o), hz = __ldg(Hin[2] + o);
+            h_cell<PML>(I, par, false, i, j, km, ex, ey, ez, ex_k, ey_k, ez_i, ey_i, ez_j, ex_j, hx, hy, hz, gE);
+            hxm = hx;
+            hym = hy;
+        }
+    }
+
+    // halo H cell of this thread (41 of them: row j0-1, then column i0-1)
+    const bool hasHalo = t < RX - 1 + TY;
+    const int hr = t < RX - 1 ? 0 : t - (RX - 1) + 1;
+    const int hc = t < RX - 1 ? t : 0;
+    bool hiok, hjok;
+    const int hi = wrapc(i0 - 1 + hc, nx, px, &hiok), hj = wrapc(j0 - 1 + hr, ny, py, &hjok);
+    const bool haloValid = hasHalo && hiok && hjok;
+    const int eo = (ty + 1) * RX + (tx + 1);   // own cell in the region
+    const int he = hr * RX + hc;               // halo cell in the region
+
+    // monitors this thread samples: x / y normal planes through its column
+    // (every plane of the march), z normal planes (when k matches)
+    unsigned mcol = 0, mz = 0;
+    for (int m = 0; m < I->nmon; ++m) {
+        const int ax = I->mon_axis[m], ix = I->mon_index[m];
+        if (ax == 2) mz |= 1u << m;
+        else if ((ax == 0 && i == ix) || (ax == 1 && j == ix)) mcol |= 1u << m;
+    }
+    double energy = 0.0;
+    R* smp0 = I->samples + (size_t)launch_off * I->sstride;
+    for (int k = k0; k < k1; ++k) {
+        const int it = k - k0;
+        const int s0 = it % NS, s1 = (it + 1) % NS, s3 = (it + 3) % NS;
+        cp_wait1();              // planes k and k+1 have landed (k+2 may be in flight)
+        __syncthreads();         // ... for every thread; everyone is done with plane k-1
+        load_plane(k + 3, s3);   // into the slot of plane k-1
+        cp_commit();
+        const R* E0 = sE + (s0 * 3) * RC;
+        const R* E1 = sE + (s1 * 3) * RC;
+        const R* H0 = sH + (s0 * 3) * RC;
+        // ---- H of plane k: own cell, then the halo cell
+        {
+            const int e = eo;
+            R hx = H0[e], hy = H0[RC + e], hz = H0[2 * RC + e];
+            if (own) {
+                h_cell<PML>(I, par, true, i, j, k, E0[e], E0[RC + e], E0[2 * RC + e], E1[e], E1[RC + e],
+                            E0[2 * RC + e + 1], E0[RC + e + 1], E0[2 * RC + e + RX], E0[e + RX], hx, hy, hz, gE);
+                const size_t o = (size_t)k * plane + (size_t)j * pitch + i;
+                Hout[0][o] = hx;
+                Hout[1][o] = hy;
+                Hout[2][o] = hz;
+            } else {
+                hx = hy = hz = R(0);
+            }
+            sHn[e] = hx;
+            sHn[RC + e] = hy;
+            sHn[2 * RC + e] = hz;
+        }
+        if (hasHalo) {
+            const int e = he;
+            R hx = R(0), hy = R(0), hz = R(0);
+            if (haloValid) {
+                hx = H0[e];
+                hy = H0[RC + e];
+                hz = H0[2 * RC + e];
+                h_cell<PML>(I, par, false, hi, hj, k, E0[e], E0[RC + e], E0[2 * RC + e], E1[e], E1[RC + e],
+                            E0[2 * RC + e + 1], E0[RC + e + 1], E0[2 * RC + e + RX], E0[e + RX], hx, hy, hz, gE);
+            }
+            sHn[e] = hx;
+            sHn[RC + e] = hy;
+            sHn[2 * RC + e] = hz;
+        }
+        __syncthreads();
+        // ---- E of plane k at the own cell
+        if (own) {
+            const int e = eo;
+            const R hxk = sHn[e], hyk = sHn[RC + e], hzk = sHn[2 * RC + e];
+            const R hy_i = sHn[RC + e - 1], hz_i = sHn[2 * RC + e - 1];
+            const R hx_j = sHn[e - RX], hz_j = sHn[2 * RC + e - RX];
+            const IT* ix = sI + (s0 * 3) * NT + t;
+            const int v0 = (int)ix[0], v1 = (int)ix[NT], v2 = (int)ix[2 * NT];
+            // Ex += cx ((Hz - Hz(j-1)) - (Hy - Hy(k-1)))
+            R d1 = cpml<PML>(I, par, true, false, 0, 1, j, i, j, k, hzk - hz_j);
+            R d2 = cpml<PML>(I, par, true, false, 0, 2, k, i, j, k, hyk - hym);
+            R ex = E0[e] + coef<R, IT>(slut, I->lutc, v0) * (d1 - d2);
+            // Ey += cy ((Hx - Hx(k-1)) - (Hz - Hz(i-1)))
+            d1 = cpml<PML>(I, par, true, false, 1, 2, k, i, j, k, hxk - hxm);
+            d2 = cpml<PML>(I, par, true, false, 1, 0, i, i, j, k, hzk - hz_i);
+            R ey = E0[RC + e] + coef<R, IT>(slut, I->lutc, v1) * (d1 - d2);
+            // Ez += cz ((Hy - Hy(i-1)) - (Hx - Hx(j-1)))
+            d1 = cpml<PML>(I, par, true, false, 2, 0, i, i, j, k, hyk - hy_i);
+            d2 = cpml<PML>(I, par, true, false, 2, 1, j, i, j, k, hxk - hx_j);
+            R ez = E0[2 * RC + e] + coef<R, IT>(slut, I->lutc, v2) * (d1 - d2);
+            // TF/SF: the source plane is total field
+            const int sa = I->sa;
+            if (sel3(sa, i, j, k) == I->ss) {
+                const int sb = (sa + 1) % 3, sc = (sa + 2) % 3;
+                const size_t pq = (size_t)sel3(sb, i, j, k) + (size_t)I->na * sel3(sc, i, j, k);
+                const R ua = __ldg(I->sEa + pq) * gH, ub = __ldg(I->sEb + pq) * gH;
+                if (sa == 0) { ey += ua; ez += ub; }
+                else if (sa == 1) { ez += ua; ex += ub; }
+                else { ex += ua; ey += ub; }
+            }
+            const size_t o = (size_t)k * plane + (size_t)j * pitch + i;
+            Eout[0][o] = ex;
+            Eout[1][o] = ey;
+            Eout[2][o] = ez;
+            // DFT samples: E on the plane, H averaged over the planes m-1, m of its normal
+            unsigned hit = mcol;
+            for (unsigned b = mz; b; b &= b - 1) {
+                const int m = __ffs(b) - 1;
+                if (k == I->mon_index[m]) hit |= 1u << m;
+            }
+            for (; hit; hit &= hit - 1) {
+                const int m = __ffs(hit) - 1;
+                const int ax = I->mon_axis[m];
+                R ea, eb, ha, hb;
+                size_t p, npl;
+                if (ax == 2) {          // a = x, b = y
+                    ea = ex; eb = ey;
+                    ha = R(0.5) * (hxk + hxm); hb = R(0.5) * (hyk + hym);
+                    p = (size_t)i + (size_t)nx * j;
+                    npl = (size_t)nx * ny;
+                } else if (ax == 0) {   // a = y, b = z
+                    ea = ey; eb = ez;
+                    ha = R(0.5) * (hyk + hy_i); hb = R(0.5) * (hzk + hz_i);
+                    p = (size_t)j + (size_t)ny * k;
+                    npl = (size_t)ny * nz;
+                } else {                // a = z, b = x
+                    ea = ez; eb = ex;
+                    ha = R(0.5) * (hzk + hz_j); hb = R(0.5) * (hxk + hx_j);
+                    p = (size_t)k + (size_t)nz * i;
+                    npl = (size_t)nz * nx;
+                }
+                R* smp = smp0 + I->mon_off[m];
+                smp[p] = ea;
+                smp[npl + p] = eb;
+                smp[2 * npl + p] = ha;
+                smp[3 * npl + p] = hb;
+            }
+            if (want_energy) {
+                energy += I->lute[v0] * (double)ex * ex + I->lute[v1] * (double)ey * ey +
+                          I->lute[v2] * (double)ez * ez + (double)hxk * hxk + (double)hyk * hyk +
+                          (double)hzk * hzk;
+            }
+            hxm = hxk;
+            hym = hyk;
+        }
+        // the next iteration's first barrier separates these reads of the
+        // new-H plane and slot s0 from their reuse
+    }
+    asm volatile("cp.async.wait_all;\n" ::: "memory");   // no copy outlives the CTA
+    if (t == 0) st->cur = par ^ 1;   // every CTA of the instance writes the same value
+    if (want_energy) {   // warp reduction, one atomic per warp
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) energy += __shfl_down_sync(0xffffffffu, energy, o);
+        if ((t & 31) == 0 && energy != 0.0) atomicAdd(&st->energy, energy);
+    }
+}
+
+template <class R, class IT, bool PML>
+cudaError_t launch_one(const void* insts, const Tile3D* tiles, int ntiles, int par, int off, int we, cudaStream_t s) {
+    constexpr size_t smem = smem_bytes<R, IT>();
+    static int done[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 64 && !done[dev]) {
+        const cudaError_t e =
+            cudaFuncSetAttribute(k_step3d<R, IT, PML>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        done[dev] = 1;
+    }
+    k_step3d<R, IT, PML><<<ntiles, NT, smem, s>>>(reinterpret_cast<const Inst3D<R>*>(insts), tiles, par, off, we);
+    return cudaGetLastError();
+}
+
+template <class R, bool PML>
+cudaError_t launch_idx(int idxw, const void* insts, const Tile3D* tiles, int ntiles, int par, int off, int we,
+                       cudaStream_t s) {
+    if (idxw == 1) return launch_one<R, uint8_t, PML>(insts, tiles, ntiles, par, off, we, s);
+    if (idxw == 2) return launch_one<R, uint16_t, PML>(insts, tiles, ntiles, par, off, we, s);
+    return launch_one<R, uint32_t, PML>(insts, tiles, ntiles, par, off, we, s);
+}
+
+}  // namespace
+
+cudaError_t launch_step3d(bool fp64, bool pml, int idxw, const void* insts, const Tile3D* tiles, int ntiles, int par,
+                          int launch_off, int want_energy, cudaStream_t s) {
+    if (ntiles <= 0) return cudaSuccess;
+    if (fp64)
+        return pml ? launch_idx<double, true>(idxw, insts, tiles, ntiles, par, launch_off, want_energy, s)
+                   : launch_idx<double, false>(idxw, insts, tiles, ntiles, par, launch_off, want_energy, s);
+    return pml ? launch_idx<float, true>(idxw, insts, tiles, ntiles, par, launch_off, want_energy, s)
+               : launch_idx<float, false>(idxw, insts, tiles, ntiles, par, launch_off, want_energy, s);
+}
+
+}  // namespace orf
