@@ -128,6 +128,7 @@ __global__ void k_check(JobState* const* __restrict__ states, int n) {
     }
     if (step >= st->nmax) done = 1;
     if (st->cancel && *st->cancel) done = 1;
+    if (st->fault) done = 1;   // a step kernel gave up a bounded wait
     if (done) st->done = 1;
     if (conv) st->converged = 1;
     const long long c = st->chunk;

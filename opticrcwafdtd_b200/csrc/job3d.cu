@@ -6,6 +6,8 @@
 // streams of the monitor planes (Ea, Eb, Ha, Hb) and the column tiles, and
 // upload everything into one device arena.  A time step is the in-place H
 // then E half-step kernel (step3d.cu); the shared ChunkEngine runs the loop.
+#include <cuda.h>   // CUtensorMap and the cuTensorMapEncodeTiled signature (entry point fetched at run time)
+
 #include <algorithm>
 #include <unordered_map>
 
@@ -85,6 +87,46 @@ struct Lut3 {
 };
 
 }  // namespace
+
+// cuTensorMapEncodeTiled from the driver, looked up once through the runtime
+// (no link-time dependency on libcuda)
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+int encode_fn(EncodeTiledFn* out) {
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        const cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q);
+        if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !p) {
+            cudaGetLastError();
+            set_error("cuTensorMapEncodeTiled is not available from the driver");
+            return ORF_ECUDA;
+        }
+        fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+    *out = fn;
+    return ORF_OK;
+}
+
+template <class R>
+int Job3D<R>::encode_tmap3(CUtensorMap* m, CUtensorMapDataType t, const void* base, size_t esz, int bx, int by) {
+    EncodeTiledFn fn;
+    ORF_TRY(encode_fn(&fn));
+    const cuuint64_t dims[3] = {(cuuint64_t)n[0], (cuuint64_t)n[1], (cuuint64_t)n[2]};
+    const cuuint64_t strides[2] = {(cuuint64_t)pitch * esz, (cuuint64_t)pitch * n[1] * esz};
+    const cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const CUresult r = fn(m, t, 3, const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_error("cuTensorMapEncodeTiled failed (%d) for a %d x %d x %d grid", (int)r, n[0], n[1], n[2]);
+        return ORF_ECUDA;
+    }
+    return ORF_OK;
+}
 
 template <class R>
 int Job3D<R>::create(const orf_sim3d* s) {
@@ -290,6 +332,8 @@ int Job3D<R>::create(const orf_sim3d* s) {
     ar.add(&d_streams, nstreams + 1);
     ar.add(&d_items, nitems + 1);
     ar.add(&d_pairs, npairs + 1);
+    unsigned char* d_tmap = nullptr;
+    ar.add(&d_tmap, kTmaps3 * sizeof(CUtensorMap));
     ORF_TRY(ar.check_budget(budget, &need));
     ORF_TRY(ar.alloc());
     arena = ar;
@@ -365,6 +409,23 @@ int Job3D<R>::create(const orf_sim3d* s) {
         h.mon_off[m] = m < nM ? moff[m] : 0;
     }
     h.samples = d_samples;
+    {
+        // TMA tensor maps of the plane loads: E[b][c] (box 40 x 10), H[b][c]
+        // (box 40 x 9), index[c] (box 32 x 8); x extent nx, so reads past the
+        // grid (the row padding included) are zero-filled
+        std::vector<CUtensorMap> maps(kTmaps3);
+        const CUtensorMapDataType ft = sizeof(R) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+        const CUtensorMapDataType it = idxw == 1 ? CU_TENSOR_MAP_DATA_TYPE_UINT8
+                                       : idxw == 2 ? CU_TENSOR_MAP_DATA_TYPE_UINT16 : CU_TENSOR_MAP_DATA_TYPE_UINT32;
+        for (int b = 0; b < 2; ++b)
+            for (int c = 0; c < 3; ++c) {
+                ORF_TRY(encode_tmap3(&maps[3 * b + c], ft, h.E[b][c], sizeof(R), kTile3X + 8, kTile3Y + 2));
+                ORF_TRY(encode_tmap3(&maps[6 + 3 * b + c], ft, h.H[b][c], sizeof(R), kTile3X + 8, kTile3Y + 1));
+            }
+        for (int c = 0; c < 3; ++c) ORF_TRY(encode_tmap3(&maps[12 + c], it, d_ix[c], idxw, kTile3X, kTile3Y));
+        ORF_TRY(up(d_tmap, maps.data(), maps.size() * sizeof(CUtensorMap)));
+        h.tmap = d_tmap;
+    }
     h.st = d_st;
     ORF_TRY(up(d_inst, &h, sizeof(h)));
     ORF_TRY(up(d_tiles, tiles.data(), tiles.size() * sizeof(Tile3D)));
@@ -492,6 +553,10 @@ int Job3D<R>::finish3d(orf_out3d* o) {
     ORF_CUDA(cudaStreamSynchronize(st));
     JobState js;
     ORF_CUDA(cudaMemcpy(&js, d_st, sizeof js, cudaMemcpyDeviceToHost));
+    if (js.fault) {
+        set_error("a 3D step kernel gave up waiting for its plane loads at step %lld", js.step);
+        return ORF_ETIMEOUT_DEVICE;
+    }
     const bool f64 = sizeof(R) == 8;
     ORF_CUDA(launch_flux(f64, d_streams, d_pairs, npairs, nL, d_flux, st));
     std::vector<double> fl((size_t)nM * nL);

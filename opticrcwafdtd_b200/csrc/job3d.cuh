@@ -1,5 +1,7 @@
 // job3d.cuh -- device-resident 3D run (orf.fdtd3D).
 #pragma once
+#include <cuda.h>
+
 #include "engine.cuh"
 
 namespace orf {
@@ -52,6 +54,8 @@ struct Job3D : orf_job {
     int64_t step_budget() const override { return nmax; }
 
     int create(const orf_sim3d* s);
+    static constexpr int kTmaps3 = 15;   // E[2][3], H[2][3], index[3]
+    int encode_tmap3(CUtensorMap* m, CUtensorMapDataType t, const void* base, size_t esz, int bx, int by);
     int init_state();
     int advance(int64_t nsteps, orf_progress_fn progress, void* user) override;
     int64_t steps_done() override;

@@ -37,7 +37,7 @@ struct JobState {
     int done;               // no more steps (shutoff, budget or cancel)
     int converged;          // stopped by the energy shutoff
     int cur;                // field buffer (0/1) holding the latest state
-    int pad;
+    int fault;              // a bounded device-side wait ran out (ORF_ETIMEOUT_DEVICE)
     double energy;          // energy accumulator of the current chunk
     double peak;
     double S;               // c0*dt [um]
@@ -178,6 +178,10 @@ struct Inst3D {
     int mon_off[kMaxMon];   // offset of the monitor's Ea, Eb, Ha, Hb planes in one step's samples
     R* samples;
     JobState* st;
+    // TMA tensor maps (CUtensorMap, 128 B each) in device memory, or null:
+    // [0..5] E[b][c] boxes 40 x 10 x 1, [6..11] H[b][c] boxes 40 x 9 x 1,
+    // [12..14] index[c] boxes 32 x 8 x 1 (b = buffer, c = component)
+    const void* tmap;
 };
 
 struct Tile3D {

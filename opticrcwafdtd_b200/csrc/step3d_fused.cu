@@ -9,9 +9,12 @@
 // A CTA owns a 32 x 8 column tile and a segment [k0, k1) of z planes and
 // marches it plane by plane:
 //   - plane p of E (the tile plus one halo cell on every side), H and the
-//     material index arrive in a 4-slot shared-memory ring by cp.async, up to
-//     three planes ahead of the one being updated (the wrapped / zero-filled
-//     x-y addressing of the region is computed once per CTA);
+//     material index arrive in a 4-slot shared-memory ring, up to three planes
+//     ahead of the one being updated: one thread issues TMA tensor copies
+//     (cp.async.bulk.tensor, x window [i0-4, i0+36) so the start stays 16-byte
+//     aligned, zero fill outside the grid) completing on one mbarrier per
+//     slot; tiles whose halo wraps around a periodic x / y edge fill the same
+//     layout with per-element cp.async instead;
 //   - H at plane k is updated on the tile plus its low x / y halo (the halo
 //     values are recomputed, not read from the neighbour CTA, whose update of
 //     them may not have happened yet) into a shared plane; the tile's own H
@@ -30,8 +33,21 @@ namespace {
 
 constexpr int TX = kTile3X, TY = kTile3Y, NT = TX * TY;
 constexpr int RX = TX + 2, RY = TY + 2, RC = RX * RY;   // E region [i0-1, i0+TX] x [j0-1, j0+TY]
+constexpr int SX = TX + 8;                                // smem row: x in [i0-4, i0+TX+4)
+constexpr int CX = 3;                                     // smem column of x = i0-1
 constexpr int NS = 4;                                     // planes in the ring
 constexpr int RPT = (RC + NT - 1) / NT;                   // region cells per thread
+constexpr long long kSpinMax = 1ll << 20;                 // bounded mbarrier wait (try_wait polls)
+
+// per-slot layout (elements of R, each block 128-byte aligned for TMA)
+template <class R>
+constexpr int rnd128(int n) {
+    return (int)((((size_t)n * sizeof(R) + 127) / 128) * 128 / sizeof(R));
+}
+template <class R>
+constexpr int EB = rnd128<R>(SX * RY);        // one E component: [RY][SX]
+template <class R>
+constexpr int HB = rnd128<R>(SX * (RY - 1));  // one H component: [RY-1][SX]
 
 __device__ __forceinline__ int wrapc(int u, int n, bool per, bool* ok) {
     if (u >= 0 && u < n) {
@@ -94,10 +110,37 @@ __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_grou
 __device__ __forceinline__ void cp_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
 template <class R, class IT>
-constexpr size_t smem_bytes() {
-    // E and H rings, the new-H plane, the index ring (16-byte rounded)
-    return (size_t)NS * 3 * RC * sizeof(R) * 2 + (size_t)3 * RC * sizeof(R) +
-           (((size_t)NS * 3 * NT * sizeof(IT) + 15) & ~size_t(15));
+constexpr size_t slot_bytes() {   // 3 E blocks, 3 H blocks, 3 index blocks
+    return 3 * (size_t)EB<R> * sizeof(R) + 3 * (size_t)HB<R> * sizeof(R) + 3 * (size_t)NT * sizeof(IT);
+}
+template <class R, class IT>
+constexpr size_t smem_bytes() {   // the ring, then the new-H plane, + 128 for alignment
+    return NS * slot_bytes<R, IT>() + 3 * (size_t)EB<R> * sizeof(R) + 128;
+}
+
+__device__ __forceinline__ unsigned sm_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long* b, unsigned cnt) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(sm_addr(b)), "r"(cnt) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* b, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(sm_addr(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* b, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(sm_addr(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// 3D tiled TMA load of the box at (x, y, z) into shared memory, completing on b
+__device__ __forceinline__ void tma_load3(void* sdst, const void* tmap, int x, int y, int z, unsigned long long* b) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];\n" ::"r"(sm_addr(sdst)),
+        "l"(tmap), "r"(x), "r"(y), "r"(z), "r"(sm_addr(b))
+        : "memory");
 }
 
 // H update of one cell (the split formulation's operations, in order)
@@ -147,12 +190,22 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
     const long long n = st->step + launch_off;
     if (n >= st->nmax) return;
 
-    extern __shared__ __align__(16) unsigned char dsm[];
-    R* sE = reinterpret_cast<R*>(dsm);                 // [NS][3][RC]
-    R* sH = sE + NS * 3 * RC;                          // [NS][3][RC] (rows < RY-1, cols < RX-1 used)
-    R* sHn = sH + NS * 3 * RC;                         // [3][RC]
-    IT* sI = reinterpret_cast<IT*>(sHn + 3 * RC);      // [NS][3][NT]
+    extern __shared__ __align__(128) unsigned char dsm_raw[];
+    // TMA destinations must be 128-byte aligned: align the base explicitly
+    // (the launch requests 128 spare bytes)
+    unsigned char* dsm = dsm_raw + ((128u - (sm_addr(dsm_raw) & 127u)) & 127u);
+    constexpr int EBr = EB<R>, HBr = HB<R>;
+    constexpr size_t SB = slot_bytes<R, IT>();
+    // slot s: E component q at sEq(s, q), H at sHq(s, q), index at sIq(s, q);
+    // region cell (r, c) (x = i0-1+c, y = j0-1+r) at r * SX + c + CX
+    auto sEq = [&](int s2, int q) { return reinterpret_cast<R*>(dsm + s2 * SB) + q * EBr; };
+    auto sHq = [&](int s2, int q) { return reinterpret_cast<R*>(dsm + s2 * SB) + 3 * EBr + q * HBr; };
+    auto sIq = [&](int s2, int q) {
+        return reinterpret_cast<IT*>(dsm + s2 * SB + 3 * (EBr + HBr) * sizeof(R)) + q * NT;
+    };
+    R* sHn = reinterpret_cast<R*>(dsm + NS * SB);      // [3][EB]
     __shared__ R slut[sizeof(IT) == 1 ? 256 : 1];
+    __shared__ __align__(8) unsigned long long sbar[NS];
 
     const int t = threadIdx.x;
     const int tx = t % TX, ty = t / TX;
@@ -165,9 +218,19 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
 
     if constexpr (sizeof(IT) == 1) slut[t] = I->lutc[t];
 
-    // ---- region addressing, the same for every plane: offset of region cell
-    // e = t + NT r within a plane, and whether it lies inside the grid (or
-    // wraps onto it)
+    // TMA for tiles whose halo does not wrap around a periodic edge
+    const bool wrapx = px && (i0 == 0 || i0 + TX >= nx), wrapy = py && (j0 == 0 || j0 + TY >= ny);
+    const bool use_tma = I->tmap != nullptr && !wrapx && !wrapy;
+    const char* tm = reinterpret_cast<const char*>(I->tmap);
+    constexpr unsigned kTx = (unsigned)(3 * SX * RY * sizeof(R) + 3 * SX * (RY - 1) * sizeof(R) + 3 * NT * sizeof(IT));
+    if (use_tma && t == 0) {
+        for (int q = 0; q < NS; ++q) mbar_init(&sbar[q], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    }
+    __syncthreads();
+
+    // ---- region addressing for the cp.async path, the same for every plane
     size_t roff[RPT];
     unsigned rmask = 0;
 #pragma unroll
@@ -185,12 +248,25 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
     // material index of the tile's own cells: 4-byte words of its rows
     constexpr int WPR = TX * (int)sizeof(IT) / 4;   // words per row
     constexpr int NWI = 3 * TY * WPR;
-    static_assert(NWI <= 4 * NT, "index words per thread");
 
-    // ---- cp.async of plane p (wrapped or zero outside the grid) into slot s
-    auto load_plane = [&](int p, int s) {
+    // ---- plane p (wrapped or zero outside the grid) into slot s
+    auto load_plane = [&](int p, int s2) {
         bool pok;
         const int pw = wrapc(p, nz, pz, &pok);
+        if (use_tma) {
+            if (t == 0) {
+                const int zc = pok ? pw : -1;   // z = -1: the whole box reads as zero
+                // order the block's earlier generic reads of this slot before the async writes
+                asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+                mbar_expect_tx(&sbar[s2], kTx);
+                for (int q = 0; q < 3; ++q) {
+                    tma_load3(sEq(s2, q), tm + 128 * (3 * par + q), i0 - 4, j0 - 1, zc, &sbar[s2]);
+                    tma_load3(sHq(s2, q), tm + 128 * (6 + 3 * par + q), i0 - 4, j0 - 1, zc, &sbar[s2]);
+                    tma_load3(sIq(s2, q), tm + 128 * (12 + q), i0, j0, zc, &sbar[s2]);
+                }
+            }
+            return;
+        }
         const size_t po = (size_t)pw * plane;
 #pragma unroll
         for (int r = 0; r < RPT; ++r) {
@@ -198,12 +274,13 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
             if (e >= RC) break;
             const bool v = pok && ((rmask >> r) & 1u);
             const size_t o = po + roff[r];
-#pragma unroll
-            for (int q = 0; q < 3; ++q) cpR<R>(sE + (s * 3 + q) * RC + e, Ein[q] + o, v);
             const int rr = e / RX, c = e - rr * RX;
+            const int se = rr * SX + c + CX;
+#pragma unroll
+            for (int q = 0; q < 3; ++q) cpR<R>(sEq(s2, q) + se, Ein[q] + o, v);
             if (rr < RY - 1 && c < RX - 1) {
 #pragma unroll
-                for (int q = 0; q < 3; ++q) cpR<R>(sH + (s * 3 + q) * RC + e, Hin[q] + o, v);
+                for (int q = 0; q < 3; ++q) cpR<R>(sHq(s2, q) + se, Hin[q] + o, v);
             }
         }
         for (int w = t; w < NWI; w += NT) {
@@ -211,17 +288,33 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
             const int jj = j0 + r;
             const bool v = pok && jj < ny;
             const size_t o = (po + (size_t)(v ? jj : 0) * pitch + i0) * sizeof(IT) + 4 * (size_t)cw;
-            cp4(reinterpret_cast<unsigned char*>(sI + (s * 3 + q) * NT) + (size_t)r * TX * sizeof(IT) + 4 * cw,
+            cp4(reinterpret_cast<unsigned char*>(sIq(s2, q)) + (size_t)r * TX * sizeof(IT) + 4 * cw,
                 reinterpret_cast<const unsigned char*>(I->idx[q]) + o, v);
         }
     };
+    // wait for plane p in slot s (TMA: its mbarrier; cp.async: this
+    // thread's groups, made visible by the barrier that follows)
+    bool timed_out = false;
+    auto wait_plane = [&](int p, int s2) {
+        if (use_tma) {
+            const unsigned parity = (unsigned)(((p - k0) / NS) & 1);
+            long long spins = 0;
+            while (!mbar_try_wait(&sbar[s2], parity)) {
+                if (++spins > kSpinMax) {
+                    timed_out = true;
+                    break;
+                }
+            }
+        } else {
+            cp_wait1();
+        }
+    };
 
-    load_plane(k0, 0);
-    cp_commit();
-    load_plane(k0 + 1, 1);
-    cp_commit();
-    load_plane(k0 + 2, 2);
-    cp_commit();
+    // planes k0 .. k0+2 (a segment reads planes up to k1)
+    for (int q = 0; q < 3; ++q) {
+        if (k0 + q <= k1) load_plane(k0 + q, q);
+        cp_commit();
+    }
 
     const R gE = (R)(n < I->nsrc ? I->gE[n] : 0.0);
     const R gH = (R)(n < I->nsrc ? I->gH[n] : 0.0);
@@ -262,8 +355,8 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
     bool hiok, hjok;
     const int hi = wrapc(i0 - 1 + hc, nx, px, &hiok), hj = wrapc(j0 - 1 + hr, ny, py, &hjok);
     const bool haloValid = hasHalo && hiok && hjok;
-    const int eo = (ty + 1) * RX + (tx + 1);   // own cell in the region
-    const int he = hr * RX + hc;               // halo cell in the region
+    const int eo = (ty + 1) * SX + (tx + 1) + CX;   // own cell in the region
+    const int he = hr * SX + hc + CX;               // halo cell in the region
 
     // monitors this thread samples: x / y normal planes through its column
     // (every plane of the march), z normal planes (when k matches)
@@ -278,20 +371,26 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
     for (int k = k0; k < k1; ++k) {
         const int it = k - k0;
         const int s0 = it % NS, s1 = (it + 1) % NS, s3 = (it + 3) % NS;
-        cp_wait1();              // planes k and k+1 have landed (k+2 may be in flight)
+        if (it == 0) wait_plane(k, s0);
+        wait_plane(k + 1, s1);   // planes k and k+1 have landed (k+2 may be in flight)
         __syncthreads();         // ... for every thread; everyone is done with plane k-1
-        load_plane(k + 3, s3);   // into the slot of plane k-1
+        if (k + 3 <= k1) load_plane(k + 3, s3);   // into the slot of plane k-1
         cp_commit();
-        const R* E0 = sE + (s0 * 3) * RC;
-        const R* E1 = sE + (s1 * 3) * RC;
-        const R* H0 = sH + (s0 * 3) * RC;
+        const R* E0x = sEq(s0, 0);
+        const R* E0y = sEq(s0, 1);
+        const R* E0z = sEq(s0, 2);
+        const R* E1x = sEq(s1, 0);
+        const R* E1y = sEq(s1, 1);
+        const R* H0x = sHq(s0, 0);
+        const R* H0y = sHq(s0, 1);
+        const R* H0z = sHq(s0, 2);
         // ---- H of plane k: own cell, then the halo cell
         {
             const int e = eo;
-            R hx = H0[e], hy = H0[RC + e], hz = H0[2 * RC + e];
+            R hx = H0x[e], hy = H0y[e], hz = H0z[e];
             if (own) {
-                h_cell<PML>(I, par, true, i, j, k, E0[e], E0[RC + e], E0[2 * RC + e], E1[e], E1[RC + e],
-                            E0[2 * RC + e + 1], E0[RC + e + 1], E0[2 * RC + e + RX], E0[e + RX], hx, hy, hz, gE);
+                h_cell<PML>(I, par, true, i, j, k, E0x[e], E0y[e], E0z[e], E1x[e], E1y[e], E0z[e + 1], E0y[e + 1],
+                            E0z[e + SX], E0x[e + SX], hx, hy, hz, gE);
                 const size_t o = (size_t)k * plane + (size_t)j * pitch + i;
                 Hout[0][o] = hx;
                 Hout[1][o] = hy;
@@ -300,44 +399,43 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
                 hx = hy = hz = R(0);
             }
             sHn[e] = hx;
-            sHn[RC + e] = hy;
-            sHn[2 * RC + e] = hz;
+            sHn[EBr + e] = hy;
+            sHn[2 * EBr + e] = hz;
         }
         if (hasHalo) {
             const int e = he;
             R hx = R(0), hy = R(0), hz = R(0);
             if (haloValid) {
-                hx = H0[e];
-                hy = H0[RC + e];
-                hz = H0[2 * RC + e];
-                h_cell<PML>(I, par, false, hi, hj, k, E0[e], E0[RC + e], E0[2 * RC + e], E1[e], E1[RC + e],
-                            E0[2 * RC + e + 1], E0[RC + e + 1], E0[2 * RC + e + RX], E0[e + RX], hx, hy, hz, gE);
+                hx = H0x[e];
+                hy = H0y[e];
+                hz = H0z[e];
+                h_cell<PML>(I, par, false, hi, hj, k, E0x[e], E0y[e], E0z[e], E1x[e], E1y[e], E0z[e + 1], E0y[e + 1],
+                            E0z[e + SX], E0x[e + SX], hx, hy, hz, gE);
             }
             sHn[e] = hx;
-            sHn[RC + e] = hy;
-            sHn[2 * RC + e] = hz;
+            sHn[EBr + e] = hy;
+            sHn[2 * EBr + e] = hz;
         }
         __syncthreads();
         // ---- E of plane k at the own cell
         if (own) {
             const int e = eo;
-            const R hxk = sHn[e], hyk = sHn[RC + e], hzk = sHn[2 * RC + e];
-            const R hy_i = sHn[RC + e - 1], hz_i = sHn[2 * RC + e - 1];
-            const R hx_j = sHn[e - RX], hz_j = sHn[2 * RC + e - RX];
-            const IT* ix = sI + (s0 * 3) * NT + t;
-            const int v0 = (int)ix[0], v1 = (int)ix[NT], v2 = (int)ix[2 * NT];
+            const R hxk = sHn[e], hyk = sHn[EBr + e], hzk = sHn[2 * EBr + e];
+            const R hy_i = sHn[EBr + e - 1], hz_i = sHn[2 * EBr + e - 1];
+            const R hx_j = sHn[e - SX], hz_j = sHn[2 * EBr + e - SX];
+            const int v0 = (int)sIq(s0, 0)[t], v1 = (int)sIq(s0, 1)[t], v2 = (int)sIq(s0, 2)[t];
             // Ex += cx ((Hz - Hz(j-1)) - (Hy - Hy(k-1)))
             R d1 = cpml<PML>(I, par, true, false, 0, 1, j, i, j, k, hzk - hz_j);
             R d2 = cpml<PML>(I, par, true, false, 0, 2, k, i, j, k, hyk - hym);
-            R ex = E0[e] + coef<R, IT>(slut, I->lutc, v0) * (d1 - d2);
+            R ex = E0x[e] + coef<R, IT>(slut, I->lutc, v0) * (d1 - d2);
             // Ey += cy ((Hx - Hx(k-1)) - (Hz - Hz(i-1)))
             d1 = cpml<PML>(I, par, true, false, 1, 2, k, i, j, k, hxk - hxm);
             d2 = cpml<PML>(I, par, true, false, 1, 0, i, i, j, k, hzk - hz_i);
-            R ey = E0[RC + e] + coef<R, IT>(slut, I->lutc, v1) * (d1 - d2);
+            R ey = E0y[e] + coef<R, IT>(slut, I->lutc, v1) * (d1 - d2);
             // Ez += cz ((Hy - Hy(i-1)) - (Hx - Hx(j-1)))
             d1 = cpml<PML>(I, par, true, false, 2, 0, i, i, j, k, hyk - hy_i);
             d2 = cpml<PML>(I, par, true, false, 2, 1, j, i, j, k, hxk - hx_j);
-            R ez = E0[2 * RC + e] + coef<R, IT>(slut, I->lutc, v2) * (d1 - d2);
+            R ez = E0z[e] + coef<R, IT>(slut, I->lutc, v2) * (d1 - d2);
             // TF/SF: the source plane is total field
             const int sa = I->sa;
             if (sel3(sa, i, j, k) == I->ss) {
@@ -397,6 +495,8 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
         // new-H plane and slot s0 from their reuse
     }
     asm volatile("cp.async.wait_all;\n" ::: "memory");   // no copy outlives the CTA
+    // (every TMA plane issued, k0 .. k1, was waited for inside the loop)
+    if (timed_out) st->fault = 1;
     if (t == 0) st->cur = par ^ 1;   // every CTA of the instance writes the same value
     if (want_energy) {   // warp reduction, one atomic per warp
 #pragma unroll
