@@ -363,7 +363,7 @@ def bench_pillar3d(args, rank, world, local, dist):
     st = ctx.stats()
     ctx.set_timing(False)
     bpc = 51 if args.precision == "single" else 99
-    roof = _roofline(st, bpc, "k_h3d + k_e3d (one time step, interior and CPML tiles)")
+    roof = _roofline(st, bpc, "k_step3d (fused H+E time step, TMA plane ring; interior and CPML tile launches)")
     line = None
     if rank == 0:
         line = {"metric": METRIC, "value": cells * nsteps * args.steps * world / (ms / 1e3) / 1e6, "unit": UNIT,

@@ -292,11 +292,13 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
                 reinterpret_cast<const unsigned char*>(I->idx[q]) + o, v);
         }
     };
-    // wait for plane p in slot s (TMA: its mbarrier; cp.async: this
-    // thread's groups, made visible by the barrier that follows)
+    // wait for plane p in slot s (TMA: thread 0 polls its mbarrier, the
+    // barrier that follows orders the data for everyone; cp.async: each
+    // thread's own groups, made visible by the same barrier)
     bool timed_out = false;
     auto wait_plane = [&](int p, int s2) {
         if (use_tma) {
+            if (t != 0) return;
             const unsigned parity = (unsigned)(((p - k0) / NS) & 1);
             long long spins = 0;
             while (!mbar_try_wait(&sbar[s2], parity)) {
