@@ -180,7 +180,7 @@ __device__ __forceinline__ R coef(const R* slut, const R* __restrict__ lutc, int
 }
 
 template <class R, class IT, bool PML>
-__global__ void __launch_bounds__(NT, 3)
+__global__ void __launch_bounds__(NT, sizeof(R) == 4 ? 4 : 3)
 k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, int par, int launch_off,
          int want_energy) {
     const Tile3D tile = tiles[blockIdx.x];
