@@ -151,7 +151,7 @@ typedef struct orf_ctx orf_ctx;
 /* Tuning knobs of the 2D/3D step kernels; zero fields mean "autotuned". */
 typedef struct orf_tuning {
     int32_t tsteps;            /* time steps fused per launch (temporal block depth) */
-    int32_t variant;           /* kernel tile variant id, 0 = autotune               */
+    int32_t variant;           /* kernel tile variant id, 0 = the precision's default */
     int32_t use_graph;         /* 1: capture the time loop in CUDA graphs            */
     int32_t _pad;
 } orf_tuning;
@@ -192,6 +192,12 @@ ORF_API int32_t orf_ctx_set_tuning(orf_ctx* ctx, const orf_tuning* t);
 ORF_API int32_t orf_ctx_set_timing(orf_ctx* ctx, int32_t on);
 ORF_API int32_t orf_ctx_get_stats(orf_ctx* ctx, orf_kernel_stats* st);
 ORF_API int32_t orf_ctx_reset_stats(orf_ctx* ctx);
+/* No counterpart in the reference.  Times every 2D kernel variant and fused
+ * step depth (4, 6, 8, 10) on `steps` steps (0 = 200) of the n sims (shutoff
+ * off) -- one run for n = 1, one batched orf_batch2d_run for n > 1 -- keeps
+ * the fastest in ctx's tuning and returns it in *best (may be NULL).  Only
+ * speed depends on the choice: every candidate computes the same values. */
+ORF_API int32_t orf_autotune2d(orf_ctx* ctx, int32_t n, const orf_sim2d* sims, int32_t steps, orf_tuning* best);
 
 /* ------------------------------------------------------------ 2D runs --- */
 /* Element counts of the caller-allocated out arrays (complex counts are in

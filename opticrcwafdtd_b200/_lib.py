@@ -47,6 +47,7 @@ _SIGS = {
     "orf_fdtd3d_run_ctx": (C.c_int32, [C.c_void_p, P(_abi.OrfSim3D), P(_abi.OrfOut3D), _abi.PROGRESS_FN, C.c_void_p]),
     "orf_batch2d_run": (C.c_int32, [C.c_void_p, C.c_int32, P(_abi.OrfSim2D), P(_abi.OrfOut2D), _abi.PROGRESS_FN,
                                     C.c_void_p]),
+    "orf_autotune2d": (C.c_int32, [C.c_void_p, C.c_int32, P(_abi.OrfSim2D), C.c_int32, P(_abi.OrfTuning)]),
     "orf_serve_open": (C.c_int32, [C.c_void_p, P(_abi.OrfServeCfg), P(C.c_void_p)]),
     "orf_serve_submit2d": (C.c_int32, [C.c_void_p, P(_abi.OrfSim2D), P(_abi.OrfOut2D), P(C.c_int64)]),
     "orf_serve_submit3d": (C.c_int32, [C.c_void_p, P(_abi.OrfSim3D), P(_abi.OrfOut3D), P(C.c_int64)]),

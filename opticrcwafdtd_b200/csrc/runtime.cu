@@ -54,6 +54,7 @@ void pml_profile(int n, int npts, int npml, double off, double dx, double S, dou
 
 int64_t max_steps(double max_time, double S) {
     const double r = max_time / S;
+    if (!(r < 4e18)) return (int64_t)4e18;   // effectively unbounded, no overflow
     const int64_t n = (int64_t)std::ceil(r - 1e-9);
     return n < 0 ? 0 : n;
 }

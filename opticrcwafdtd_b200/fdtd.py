@@ -32,6 +32,17 @@ class Context:
         t = _abi.OrfTuning(tsteps, variant, 1 if use_graph else 0, 0)
         _lib.check(self._lib.orf_ctx_set_tuning(self.handle, C.byref(t)), "orf_ctx_set_tuning")
 
+    def autotune2d(self, sims, steps: int = 0) -> dict:
+        """Time every 2D kernel variant and fused step depth on one sim (or a
+        batch of sims, run batched) and keep the fastest in this context
+        (orf_autotune2d); returns the choice."""
+        sims = sims if isinstance(sims, (list, tuple)) else [sims]
+        ms = [_abi.marshal_sim2d(s) for s in sims]
+        arr = (_abi.OrfSim2D * len(ms))(*[m.struct for m in ms])
+        t = _abi.OrfTuning()
+        _lib.check(self._lib.orf_autotune2d(self.handle, len(ms), arr, int(steps), C.byref(t)), "autotune2d")
+        return {"tsteps": t.tsteps, "variant": t.variant, "use_graph": bool(t.use_graph)}
+
     def set_timing(self, on: bool) -> None:
         _lib.check(self._lib.orf_ctx_set_timing(self.handle, 1 if on else 0))
 
@@ -107,7 +118,7 @@ def fdtd3D(sim, ctx: Context | None = None) -> dict:
     return out
 
 
-def fdtd2D_batch(sims, ctx: Context | None = None, progress=None) -> list[dict]:
+def fdtd2D_batch(sims, ctx: Context | None = None, progress=None, autotune: bool = False) -> list[dict]:
     """Run many 2D sims (same precision; TE and TM may mix) together: one
     persistent-kernel launch per fused step block advances every instance of
     a kernel configuration (orf_batch2d_run).
@@ -122,6 +133,14 @@ def fdtd2D_batch(sims, ctx: Context | None = None, progress=None) -> list[dict]:
     own = ctx is None
     if own:
         ctx = Context(0)
+    if autotune:
+        # tune on a sample of up to 32 instances, run batched; every instance
+        # then uses that choice
+        step = max(1, len(ms) // 32)
+        sample = ms[::step][:32]
+        sarr = (_abi.OrfSim2D * len(sample))(*[m.struct for m in sample])
+        t = _abi.OrfTuning()
+        _lib.check(lib.orf_autotune2d(ctx.handle, len(sample), sarr, 1000, C.byref(t)), "autotune2d")
     cb, box = _abi.make_progress(progress)
     st = lib.orf_batch2d_run(ctx.handle, len(ms), arr, oarr, cb or _abi.PROGRESS_FN(0), None)
     if own:

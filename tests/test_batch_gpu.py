@@ -39,3 +39,22 @@ def test_batch_shutoff_stops_each_instance():
     assert o[0]["converged"] and not o[1]["converged"]
     ref = oracle.fdtd2DTE(s1)
     assert o[0]["steps"] == ref["steps"]
+
+
+def test_autotune_changes_speed_not_results():
+    """orf_autotune2d picks one of the timed candidates; every candidate
+    computes the same values, so tuned runs equal default runs bitwise."""
+    sim = cases.mixed_te_sim(nx=700, nz=330, steps=300, precision="single", seed=5, pol="TM")
+    ref = orf.fdtd2D(sim)
+    ctx = orf.Context(0)
+    t = ctx.autotune2d(sim, steps=100)
+    assert t["variant"] in (1, 2) and t["tsteps"] in (4, 6, 8, 10) and t["use_graph"]
+    out = orf.fdtd2D(sim, ctx)
+    for k in ("flux", "fluxZ", "P", "B", "PZ", "AZ"):
+        assert np.array_equal(out[k], ref[k]), k
+    sims = [sim, cases.mixed_te_sim(nx=300, nz=160, steps=200, precision="single", seed=6, pol="TM")]
+    outs = orf.fdtd2D_batch(sims, ctx, autotune=True)
+    for s, o in zip(sims, outs):
+        a = orf.fdtd2D(s)
+        assert np.array_equal(o["flux"], a["flux"]) and np.array_equal(o["P"], a["P"])
+    ctx.close()
