@@ -81,9 +81,10 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def ncu_traffic_per_cell_update():
-    """DRAM bytes per cell update of the interior kernel from the committed ncu summary."""
-    p = os.path.join(HERE, "profiles", "interior_kernel_tm_pixel_4000x1500.json")
+def ncu_traffic_per_cell_update(name="interior_kernel_tm_pixel_4000x1500.json"):
+    """DRAM bytes per cell update of a kernel from its committed ncu summary
+    (one capture; scaled here to the cell updates of a launch)."""
+    p = os.path.join(HERE, "profiles", name)
     try:
         with open(p) as f:
             d = json.load(f)
@@ -364,6 +365,10 @@ def bench_pillar3d(args, rank, world, local, dist):
     ctx.set_timing(False)
     bpc = 51 if args.precision == "single" else 99
     roof = _roofline(st, bpc, "k_step3d (fused H+E time step, TMA plane ring; interior and CPML tile launches)")
+    if roof and args.precision == "single":
+        tpc = ncu_traffic_per_cell_update("step3d_kernel_pillar_lattice.json")
+        roof["traffic"] = tpc * roof["cell_updates_per_launch"] if tpc else None
+        roof["traffic_note"] = "interior-launch DRAM bytes per cell update from a 300x300x150 capture, scaled"
     line = None
     if rank == 0:
         line = {"metric": METRIC, "value": cells * nsteps * args.steps * world / (ms / 1e3) / 1e6, "unit": UNIT,

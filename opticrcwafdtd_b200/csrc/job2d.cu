@@ -67,14 +67,23 @@ int validate2d(const orf_sim2d* s) {
 struct Lut {
     std::unordered_map<uint64_t, int> map;
     std::vector<double> vals;
+    uint64_t last_key = ~uint64_t(0);   // neighbouring cells mostly share a material
+    int last_id = -1;
     int get(double v) {
         uint64_t key;
         std::memcpy(&key, &v, 8);
+        if (key == last_key) return last_id;
         auto it = map.find(key);
-        if (it != map.end()) return it->second;
-        const int id = (int)vals.size();
-        map.emplace(key, id);
-        vals.push_back(v);
+        int id;
+        if (it != map.end()) {
+            id = it->second;
+        } else {
+            id = (int)vals.size();
+            map.emplace(key, id);
+            vals.push_back(v);
+        }
+        last_key = key;
+        last_id = id;
         return id;
     }
 };
@@ -105,26 +114,24 @@ int Job2D<R>::create(const orf_sim2d* s) {
     Lut lut;
     std::vector<uint16_t> ix0(cellsP, 0), ix1(te ? 0 : cellsP, 0);
     lut.get(te ? s->eps[0] : s->eps_x[0]);
-    for (int k = 0; k < nz; ++k) {
-        for (int i = 0; i < nx; ++i) {
-            if (te) {
-                ix0[(size_t)k * pitch + i] = 0;
-                const int v = lut.get(s->eps[i + (size_t)nx * k]);
-                if (v > 65535) { set_error("more than 65536 distinct permittivity values"); return ORF_ETOOLARGE; }
-                ix0[(size_t)k * pitch + i] = (uint16_t)v;
-            } else {
-                if (k < nzA) {
-                    const int v = lut.get(s->eps_x[i + (size_t)nx * k]);
-                    if (v > 65535) { set_error("more than 65536 distinct permittivity values"); return ORF_ETOOLARGE; }
-                    ix0[(size_t)k * pitch + i] = (uint16_t)v;
+    // one plane at a time, row by row, so the table's last-value shortcut hits
+    auto index_plane = [&](const double* e, int w, int h, std::vector<uint16_t>& ix) -> int {
+        for (int k = 0; k < h; ++k)
+            for (int i = 0; i < w; ++i) {
+                const int v = lut.get(e[i + (size_t)w * k]);
+                if (v > 65535) {
+                    set_error("more than 65536 distinct permittivity values");
+                    return ORF_ETOOLARGE;
                 }
-                if (i < nxB) {
-                    const int v = lut.get(s->eps_z[i + (size_t)nxB * k]);
-                    if (v > 65535) { set_error("more than 65536 distinct permittivity values"); return ORF_ETOOLARGE; }
-                    ix1[(size_t)k * pitch + i] = (uint16_t)v;
-                }
+                ix[(size_t)k * pitch + i] = (uint16_t)v;
             }
-        }
+        return ORF_OK;
+    };
+    if (te) {
+        ORF_TRY(index_plane(s->eps, nx, nz, ix0));
+    } else {
+        ORF_TRY(index_plane(s->eps_x, nx, nzA, ix0));
+        ORF_TRY(index_plane(s->eps_z, nxB, nz, ix1));
     }
     nlut = (int)lut.vals.size();
     idx16 = nlut > 256;
