@@ -52,7 +52,7 @@ def parse():
     ap.add_argument("--cpu-sample-steps", type=int, default=300)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="pixel2d", choices=["pixel2d", "pillar3d", "coupler_batch", "serve"],
+    ap.add_argument("--workload", default="pixel2d", choices=["pixel2d", "coupler", "pillar3d", "coupler_batch", "serve"],
                     help="pixel2d is the headline; the others measure the 3D, batched and served paths")
     ap.add_argument("--batch", type=int, default=256)
     ap.add_argument("--size3d", default="600,600,300", help="pillar3d grid NX,NY,NZ (smaller for profiling)")
@@ -226,12 +226,29 @@ def _roofline(st, bpc, kernel, kind="interior"):
 
 
 def bench_pixel2d(args, rank, world, local, dist):
-    """Headline: whole 2D TM pixel-region jobs, device-resident inputs."""
+    """Headline: whole 2D TM pixel-region jobs, device-resident inputs
+    (--workload coupler: the 800 x 300 FP64 TE grating coupler instead)."""
     import torch
     from opticrcwafdtd_b200 import Context, Job, fdtd2D, workloads
 
-    sim = workloads.pixel_region_sim(precision=args.precision, steps=args.time_steps)
-    nx, nz = sim["epsX"].shape[0], sim["epsZ"].shape[1]
+    coupler = args.workload == "coupler"
+    if coupler:
+        if args.time_steps == 30000:
+            args.time_steps = 8000
+        args.precision = "double"
+        sim = workloads.coupler_sim(precision="double", steps=args.time_steps)
+        pol, nx, nz = "TE", sim["eps"].shape[0], sim["eps"].shape[1]
+        data = "synthetic (SOI grating coupler: 20 x 630 nm periods, ff 0.5, 70 nm etch)"
+        wl = ("2D TE SOI grating coupler 800x300 dx=20nm 20-cell CPML, TE0 source, 51-lambda DFT, "
+              f"{args.time_steps} time steps per job, FP64")
+        l2 = "working set below L2 (this small case runs from L2)"
+    else:
+        sim = workloads.pixel_region_sim(precision=args.precision, steps=args.time_steps)
+        pol, nx, nz = "TM", sim["epsX"].shape[0], sim["epsZ"].shape[1]
+        data = "synthetic (seeded Bernoulli Si/SiO2 pixel map, 4000x1500)"
+        wl = ("2D TM pixel region 4000x1500 dx=10nm 20-cell CPML, TM0 source, "
+              "101-lambda DFT (3 x-lines, 2 z-lines), 30000 time steps per job")
+        l2 = "inputs larger than L2 (156 MB working set > 126 MB)"
     cells = nx * nz
     stream = torch.cuda.current_stream()
     ctx = Context(local, stream=stream.cuda_stream)
@@ -268,9 +285,9 @@ def bench_pixel2d(args, rank, world, local, dist):
     st = ctx.stats()
     ctx.set_timing(False)
     launches_per_job = st["interior_launches"] + st["frame_launches"] + st["flush_launches"]
-    bpc = BYTES_PER_CELL_UPDATE[("TM", args.precision)]
+    bpc = BYTES_PER_CELL_UPDATE[(pol, args.precision)]
     roof = _roofline(st, bpc, "k_step2d_fast (interior tiles, PML=false)")
-    if roof:
+    if roof and not coupler:
         tpc = ncu_traffic_per_cell_update()
         roof["traffic"] = tpc * roof["cell_updates_per_launch"] if tpc else None
         roof["share_of_step_kernels"] = st["interior_ms"] / max(1e-9, st["interior_ms"] + st["frame_ms"])
@@ -301,7 +318,7 @@ def bench_pixel2d(args, rank, world, local, dist):
         ectx.close()
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and not coupler:
         cpu = cpu_baseline(sim, args.cpu_sample_steps)
     line = None
     if rank == 0:
@@ -309,13 +326,12 @@ def bench_pixel2d(args, rank, world, local, dist):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32" if args.precision == "single" else "f64",
-            "data": "synthetic (seeded Bernoulli Si/SiO2 pixel map, 4000x1500)",
-            "config": {"workload": "2D TM pixel region 4000x1500 dx=10nm 20-cell CPML, TM0 source, "
-                                   "101-lambda DFT (3 x-lines, 2 z-lines), 30000 time steps per job",
+            "data": data,
+            "config": {"workload": wl,
                        "cells": cells, "time_steps_per_job": nsteps,
                        "precision": "FP32 fields, FP32+Kahan DFT, FP64 phases" if args.precision == "single"
                        else "FP64", "parallelism": f"replicas x{world}",
-                       "l2": "inputs larger than L2 (156 MB working set > 126 MB)",
+                       "l2": l2,
                        "timed_path": "CUDA-graph chunk replays, timing events off"},
             "gpu_launches": launches_per_job * args.steps,
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
@@ -496,8 +512,8 @@ def bench_serve(args, rank, world, local, dist):
             "clocks": clk.summary()}
 
 
-WORKLOADS = {"pixel2d": bench_pixel2d, "pillar3d": bench_pillar3d, "coupler_batch": bench_coupler_batch,
-             "serve": bench_serve}
+WORKLOADS = {"pixel2d": bench_pixel2d, "coupler": bench_pixel2d, "pillar3d": bench_pillar3d,
+             "coupler_batch": bench_coupler_batch, "serve": bench_serve}
 
 
 def main():
