@@ -9,8 +9,8 @@
 // A CTA owns a 32 x 8 column tile and a segment [k0, k1) of z planes and
 // marches it plane by plane:
 //   - plane p of E (the tile plus one halo cell on every side), H and the
-//     material index arrive in a 4-slot shared-memory ring, up to three planes
-//     ahead of the one being updated: one thread issues TMA tensor copies
+//     material index arrive in a shared-memory ring (4 slots FP32, 3 FP64),
+//     ahead of the plane being updated: one thread issues TMA tensor copies
 //     (cp.async.bulk.tensor, x window [i0-4, i0+36) so the start stays 16-byte
 //     aligned, zero fill outside the grid) completing on one mbarrier per
 //     slot; tiles whose halo wraps around a periodic x / y edge fill the same
@@ -35,7 +35,8 @@ constexpr int TX = kTile3X, TY = kTile3Y, NT = TX * TY;
 constexpr int RX = TX + 2, RY = TY + 2, RC = RX * RY;   // E region [i0-1, i0+TX] x [j0-1, j0+TY]
 constexpr int SX = TX + 8;                                // smem row: x in [i0-4, i0+TX+4)
 constexpr int CX = 3;                                     // smem column of x = i0-1
-constexpr int NS = 4;                                     // planes in the ring
+template <class R>
+constexpr int NS = sizeof(R) == 4 ? 4 : 3;               // planes in the ring (FP64: 3, for occupancy)
 constexpr int RPT = (RC + NT - 1) / NT;                   // region cells per thread
 constexpr long long kSpinMax = 1ll << 20;                 // bounded mbarrier wait (try_wait polls)
 
@@ -107,7 +108,8 @@ __device__ __forceinline__ void cpR(R* sdst, const R* gsrc, bool valid) {
     else cp8(sdst, gsrc, valid);
 }
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 template <class R, class IT>
 constexpr size_t slot_bytes() {   // 3 E blocks, 3 H blocks, 3 index blocks
@@ -115,7 +117,7 @@ constexpr size_t slot_bytes() {   // 3 E blocks, 3 H blocks, 3 index blocks
 }
 template <class R, class IT>
 constexpr size_t smem_bytes() {   // the ring, then the new-H plane, + 128 for alignment
-    return NS * slot_bytes<R, IT>() + 3 * (size_t)EB<R> * sizeof(R) + 128;
+    return NS<R> * slot_bytes<R, IT>() + 3 * (size_t)EB<R> * sizeof(R) + 128;
 }
 
 __device__ __forceinline__ unsigned sm_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -203,9 +205,10 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
     auto sIq = [&](int s2, int q) {
         return reinterpret_cast<IT*>(dsm + s2 * SB + 3 * (EBr + HBr) * sizeof(R)) + q * NT;
     };
-    R* sHn = reinterpret_cast<R*>(dsm + NS * SB);      // [3][EB]
+    constexpr int ns = NS<R>;
+    R* sHn = reinterpret_cast<R*>(dsm + ns * SB);      // [3][EB]
     __shared__ R slut[sizeof(IT) == 1 ? 256 : 1];
-    __shared__ __align__(8) unsigned long long sbar[NS];
+    __shared__ __align__(8) unsigned long long sbar[ns];
 
     const int t = threadIdx.x;
     const int tx = t % TX, ty = t / TX;
@@ -224,7 +227,7 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
     const char* tm = reinterpret_cast<const char*>(I->tmap);
     constexpr unsigned kTx = (unsigned)(3 * SX * RY * sizeof(R) + 3 * SX * (RY - 1) * sizeof(R) + 3 * NT * sizeof(IT));
     if (use_tma && t == 0) {
-        for (int q = 0; q < NS; ++q) mbar_init(&sbar[q], 1);
+        for (int q = 0; q < ns; ++q) mbar_init(&sbar[q], 1);
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     }
@@ -299,7 +302,7 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
     auto wait_plane = [&](int p, int s2) {
         if (use_tma) {
             if (t != 0) return;
-            const unsigned parity = (unsigned)(((p - k0) / NS) & 1);
+            const unsigned parity = (unsigned)(((p - k0) / ns) & 1);
             long long spins = 0;
             while (!mbar_try_wait(&sbar[s2], parity)) {
                 if (++spins > kSpinMax) {
@@ -308,12 +311,12 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
                 }
             }
         } else {
-            cp_wait1();
+            cp_wait<ns - 3>();   // all but the planes issued after p
         }
     };
 
-    // planes k0 .. k0+2 (a segment reads planes up to k1)
-    for (int q = 0; q < 3; ++q) {
+    // planes k0 .. k0+ns-2 (a segment reads planes up to k1)
+    for (int q = 0; q < ns - 1; ++q) {
         if (k0 + q <= k1) load_plane(k0 + q, q);
         cp_commit();
     }
@@ -372,11 +375,11 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
     R* smp0 = I->samples + (size_t)launch_off * I->sstride;
     for (int k = k0; k < k1; ++k) {
         const int it = k - k0;
-        const int s0 = it % NS, s1 = (it + 1) % NS, s3 = (it + 3) % NS;
+        const int s0 = it % ns, s1 = (it + 1) % ns, sn = (it + ns - 1) % ns;
         if (it == 0) wait_plane(k, s0);
-        wait_plane(k + 1, s1);   // planes k and k+1 have landed (k+2 may be in flight)
+        wait_plane(k + 1, s1);   // planes k and k+1 have landed (later ones may be in flight)
         __syncthreads();         // ... for every thread; everyone is done with plane k-1
-        if (k + 3 <= k1) load_plane(k + 3, s3);   // into the slot of plane k-1
+        if (k + ns - 1 <= k1) load_plane(k + ns - 1, sn);   // into the slot of plane k-1
         cp_commit();
         const R* E0x = sEq(s0, 0);
         const R* E0y = sEq(s0, 1);
