@@ -61,6 +61,43 @@ struct ChunkEngine {
     void collect_timing();
 };
 
+// A second stream for running a job's CPML-frame launch next to its
+// interior launch: both read buffer par and write disjoint cells of par^1,
+// so they may overlap (small grids fill only part of the GPU with either).
+// fork() records the fork on s, returns the side stream waiting on it;
+// join() makes s wait for the side stream.  Captured as parallel graph
+// branches when s is being captured.
+struct SideStream {
+    cudaStream_t s2 = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    bool ok() const { return s2 != nullptr; }
+    int init() {
+        if (s2) return ORF_OK;
+        ORF_CUDA(cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking));
+        ORF_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+        ORF_CUDA(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+        return ORF_OK;
+    }
+    cudaError_t fork(cudaStream_t s) {
+        cudaError_t e = cudaEventRecord(ev_fork, s);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(s2, ev_fork, 0);
+        return e;
+    }
+    cudaError_t join(cudaStream_t s) {
+        cudaError_t e = cudaEventRecord(ev_join, s2);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(s, ev_join, 0);
+        return e;
+    }
+    ~SideStream() {
+        if (s2) {
+            cudaStreamSynchronize(s2);
+            cudaStreamDestroy(s2);
+        }
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_join) cudaEventDestroy(ev_join);
+    }
+};
+
 // Host-side progress loop over one job's status ring.
 struct ProgressLoop {
     const ChunkStatus* ring = nullptr;   // mapped host ring of the job

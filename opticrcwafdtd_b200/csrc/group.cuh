@@ -76,6 +76,7 @@ struct Group2D : Group {
     int T = 1, fv = 1;
     FastTile2D *d_inner = nullptr, *d_frame = nullptr;
     int ni = 0, nf = 0, grid_f = 0, grid_p = 0;
+    SideStream side;   // CPML frame launches next to the interior ones
     int64_t interior_cells = 0, all_cells = 0;
 
     static bool compatible(const Job2D<R>* a, const Job2D<R>* b) {
@@ -140,9 +141,17 @@ struct Group2D : Group {
         grid_f = (int)std::min<int64_t>(ni, (int64_t)ctx->sm_count * std::max(1, bps_f));
         grid_p = (int)std::min<int64_t>(nf, (int64_t)ctx->sm_count * std::max(1, bps_p));
         wire_engine(f64, T);
+        if (ni && nf) ORF_TRY(side.init());
         eng.step = [this, f64](int off, int nsub, int par, int we, cudaStream_t s, KernelTimer* tm) -> cudaError_t {
             cudaError_t e = cudaSuccess;
             cudaEvent_t a = nullptr;
+            const bool overlap = !tm && side.ok() && ni && nf;
+            cudaStream_t fs = s;
+            if (overlap) {
+                e = side.fork(s);
+                if (e != cudaSuccess) return e;
+                fs = side.s2;
+            }
             if (ni) {
                 if (tm && tm->begin(s, &a) != ORF_OK) return cudaErrorUnknown;
                 e = launch_fast2d(f64, te, idx16, false, fv, d_inner, ni, off, nsub, par, we, grid_f, s);
@@ -150,11 +159,12 @@ struct Group2D : Group {
                 if (tm && tm->end(s, 0, interior_cells * nsub, a) != ORF_OK) return cudaErrorUnknown;
             }
             if (nf) {
-                if (tm && tm->begin(s, &a) != ORF_OK) return cudaErrorUnknown;
-                e = launch_fast2d(f64, te, idx16, true, 0, d_frame, nf, off, nsub, par, we, grid_p, s);
+                if (tm && tm->begin(fs, &a) != ORF_OK) return cudaErrorUnknown;
+                e = launch_fast2d(f64, te, idx16, true, 0, d_frame, nf, off, nsub, par, we, grid_p, fs);
                 if (e != cudaSuccess) return e;
-                if (tm && tm->end(s, 1, (all_cells - interior_cells) * nsub, a) != ORF_OK) return cudaErrorUnknown;
+                if (tm && tm->end(fs, 1, (all_cells - interior_cells) * nsub, a) != ORF_OK) return cudaErrorUnknown;
             }
+            if (overlap) e = side.join(s);
             return e;
         };
         dirty = false;

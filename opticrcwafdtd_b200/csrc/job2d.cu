@@ -366,11 +366,22 @@ int Job2D<R>::create(const orf_sim2d* s) {
     eng.nstates = 1;
     int64_t interior_cells = 0;
     for (int q = 0; q < nfast; ++q) interior_cells += (int64_t)ftiles_host[q].ow * ftiles_host[q].oh;
+    if (!ext_base && nfast && nframe) ORF_TRY(side.init());   // no extra stream in no-allocation mode
     eng.step = [this, interior_cells](int off, int nsub, int par, int we, cudaStream_t stream,
                                       KernelTimer* tm) -> cudaError_t {
         const bool f64 = sizeof(R) == 8;
         cudaError_t e = cudaSuccess;
         cudaEvent_t a = nullptr;
+        // frame next to the interior on the side stream (not while timing
+        // individual launches); the interior is submitted first, the side
+        // stream waits only for the fork recorded before it
+        const bool overlap = !tm && side.ok();
+        cudaStream_t fs = stream;
+        if (overlap) {
+            e = side.fork(stream);
+            if (e != cudaSuccess) return e;
+            fs = side.s2;
+        }
         if (nfast) {
             if (tm && tm->begin(stream, &a) != ORF_OK) return cudaErrorUnknown;
             e = launch_fast2d(f64, te, idx16, false, fvariant, d_ftiles, nfast, off, nsub, par, we, grid_fast, stream);
@@ -378,13 +389,13 @@ int Job2D<R>::create(const orf_sim2d* s) {
             if (tm && tm->end(stream, 0, interior_cells * nsub, a) != ORF_OK) return cudaErrorUnknown;
         }
         if (nframe) {
-            if (tm && tm->begin(stream, &a) != ORF_OK) return cudaErrorUnknown;
-            e = launch_fast2d(f64, te, idx16, true, 0, d_ftiles + nfast, nframe, off, nsub, par, we, grid_frame,
-                              stream);
+            if (tm && tm->begin(fs, &a) != ORF_OK) return cudaErrorUnknown;
+            e = launch_fast2d(f64, te, idx16, true, 0, d_ftiles + nfast, nframe, off, nsub, par, we, grid_frame, fs);
             if (e != cudaSuccess) return e;
-            if (tm && tm->end(stream, 1, ((int64_t)nx * nz - interior_cells) * nsub, a) != ORF_OK)
+            if (tm && tm->end(fs, 1, ((int64_t)nx * nz - interior_cells) * nsub, a) != ORF_OK)
                 return cudaErrorUnknown;
         }
+        if (overlap) e = side.join(stream);
         return e;
     };
     ORF_CUDA(cudaStreamSynchronize(st));

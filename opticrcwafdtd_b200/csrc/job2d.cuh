@@ -41,6 +41,7 @@ struct Job2D : orf_job {
     int* cancel_d = nullptr;
     ChunkEngine eng;
     ProgressLoop pl;
+    SideStream side;   // CPML frame launches next to the interior ones
     // no-allocation mode: device state carved from ext_base (see noalloc.cu),
     // no mapped status ring, no graphs, no events
     void* ext_base = nullptr;
