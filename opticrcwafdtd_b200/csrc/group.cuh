@@ -181,6 +181,7 @@ struct Group3D : Group {
     Inst3D<R>* d_insts = nullptr;
     Tile3D *d_tiles = nullptr, *d_tiles_pml = nullptr;
     int nt = 0, ntp = 0;
+    SideStream side;   // CPML tiles next to the interior tiles
     int64_t all_cells = 0;
 
     static bool compatible(const Job3D<R>* a, const Job3D<R>* b) { return a->zc == b->zc && a->idxw == b->idxw; }
@@ -246,12 +247,17 @@ struct Group3D : Group {
         ntp = (int)tp.size();
         const bool f64 = sizeof(R) == 8;
         wire_engine(f64, 1);
+        if (nt && ntp) ORF_TRY(side.init());
         eng.step = [this, f64](int off, int nsub, int par, int we, cudaStream_t s, KernelTimer* tm) -> cudaError_t {
             (void)nsub;
             cudaEvent_t a = nullptr;
             if (tm && tm->begin(s, &a) != ORF_OK) return cudaErrorUnknown;
-            cudaError_t e = launch_step3d(f64, false, idxw, d_insts, d_tiles, nt, par, off, we, s);
-            if (e == cudaSuccess) e = launch_step3d(f64, true, idxw, d_insts, d_tiles_pml, ntp, par, off, we, s);
+            const bool overlap = !tm && side.ok() && nt && ntp;
+            cudaError_t e = overlap ? side.fork(s) : cudaSuccess;
+            if (e == cudaSuccess) e = launch_step3d(f64, false, idxw, d_insts, d_tiles, nt, par, off, we, s);
+            if (e == cudaSuccess)
+                e = launch_step3d(f64, true, idxw, d_insts, d_tiles_pml, ntp, par, off, we, overlap ? side.s2 : s);
+            if (e == cudaSuccess && overlap) e = side.join(s);
             if (e != cudaSuccess) return e;
             if (tm && tm->end(s, 0, all_cells, a) != ORF_OK) return cudaErrorUnknown;
             return e;

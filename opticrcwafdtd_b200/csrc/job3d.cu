@@ -462,14 +462,22 @@ int Job3D<R>::create(const orf_sim3d* s) {
     eng.d_states = d_states;
     eng.nstates = 1;
     const int64_t ncell = (int64_t)N();
+    if (!tiles.empty() && !tiles_pml.empty()) ORF_TRY(side.init());
     eng.step = [this, ncell](int off, int nsub, int par, int we, cudaStream_t stream, KernelTimer* tm) -> cudaError_t {
         (void)nsub;
         cudaEvent_t a = nullptr;
         if (tm && tm->begin(stream, &a) != ORF_OK) return cudaErrorUnknown;
         const bool f64 = sizeof(R) == 8;
-        cudaError_t e = launch_step3d(f64, false, idxw, d_inst, d_tiles, (int)tiles.size(), par, off, we, stream);
+        // the CPML tiles run next to the interior tiles (disjoint cells, both
+        // read buffer par) unless launches are being timed
+        const bool overlap = !tm && side.ok();
+        cudaError_t e = overlap ? side.fork(stream) : cudaSuccess;
         if (e == cudaSuccess)
-            e = launch_step3d(f64, true, idxw, d_inst, d_tiles_pml, (int)tiles_pml.size(), par, off, we, stream);
+            e = launch_step3d(f64, false, idxw, d_inst, d_tiles, (int)tiles.size(), par, off, we, stream);
+        if (e == cudaSuccess)
+            e = launch_step3d(f64, true, idxw, d_inst, d_tiles_pml, (int)tiles_pml.size(), par, off, we,
+                              overlap ? side.s2 : stream);
+        if (e == cudaSuccess && overlap) e = side.join(stream);
         if (e != cudaSuccess) return e;
         if (tm && tm->end(stream, 0, ncell, a) != ORF_OK) return cudaErrorUnknown;
         return e;

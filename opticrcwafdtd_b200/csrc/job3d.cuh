@@ -38,6 +38,7 @@ struct Job3D : orf_job {
     int* cancel_d = nullptr;
     ChunkEngine eng;
     ProgressLoop pl;
+    SideStream side;   // CPML tiles next to the interior tiles
 
     Job3D() { dims = 3; }
     ~Job3D() override {
