@@ -11,7 +11,8 @@ a GPU is missing.
 from ._abi import NotConvergedWarning, OrfError  # noqa: F401
 from .geometry import epsCellMean, epsComponents2D, epsComponents3D, epsFromBoxes  # noqa: F401
 from .modes import slabModes  # noqa: F401
-from .coupler import fiberCoupling, gratingCouplerTE, gratingCouplerTE_batch  # noqa: F401
+from .coupler import (apodizedGrating, bestFiberCoupling, fiberCoupling, gratingCouplerTE,  # noqa: F401
+                      gratingCouplerTE_batch)
 
 __version__ = "0.1.0"
 from .fdtd import Context, Job, Server, device_count, fdtd2D, fdtd2D_batch, fdtd2DTE, fdtd3D  # noqa: F401,E402

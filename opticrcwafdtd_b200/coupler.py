@@ -1,4 +1,5 @@
-"""orf.gratingCouplerTE and orf.fiberCoupling on the B200 engine.
+"""orf.gratingCouplerTE, orf.fiberCoupling, orf.bestFiberCoupling and
+orf.apodizedGrating on the B200 engine.
 
 gratingCouplerTE (toolbox/+orf/gratingCouplerTE.m:1-27, documented interface;
 the implementation is closed) builds the SOI grating cross-section, launches
@@ -138,7 +139,7 @@ def gratingCouplerTE_sim(p: Any = None) -> tuple[dict, dict]:
     if q["courant"] is not None:
         sim["courant"] = float(q["courant"])
     sim["source"] = dict(ix=ix_src + 1, profile=prof, neff=neff, lambda0=float(q["lambda0"]), bw=float(q["bw"]))
-    boxdesc = dict(q=q, dx=dx, x=x, z=z, eps=eps, neff=neff, mons=mons, monz=monz,
+    boxdesc = dict(q=q, dx=dx, x=x, z=z, eps=eps, neff=neff, mons=mons, monz=monz, grating=(X_GRATING, x_end),
                    k_lo=monz[1], k_hi=monz[0], i_lo=mons[1], i_hi=mons[2])
     return sim, boxdesc
 
@@ -173,6 +174,7 @@ def coupler_budget(out: dict, bd: dict) -> dict:
     res["converged"] = out["converged"]
     res["geometry"] = dict(x=bd["x"], z=bd["z"], eps=bd["eps"])
     res["params"] = q
+    res["grating"] = bd["grating"]
     return res
 
 
@@ -233,3 +235,57 @@ def fiberCoupling(res: dict, theta, x0, w0: float):
                 overlap[i, j, l] = abs(np.vdot(Ef, E)) ** 2 / (EE * np.real(np.vdot(Ef, Ef)))
         eta[:, :, l] = overlap[:, :, l] * pup[l]
     return eta, overlap
+
+
+def bestFiberCoupling(res: dict, thetaDeg=None, w0: float = 5.2) -> dict:
+    """b = bestFiberCoupling(res, thetaDeg, w0) (bestFiberCoupling.m:1-8,
+    documented interface): scans the fiber tilt over thetaDeg (default
+    5:0.5:15) and its centre over the grating in 0.1 um steps, maximising the
+    coupling at the design wavelength res.params.lambda0.
+      b.eta, b.dB : coupling at lambda0;  b.theta [deg], b.x0 [um]
+      b.spectrum  : coupling vs res.lambdas at that fiber position
+      b.band1dB   : [min max] sampled wavelengths within 1 dB of the peak
+      b.Pup       : upward power fraction at lambda0"""
+    theta = np.arange(5.0, 15.0 + 1e-9, 0.5) if thetaDeg is None else np.atleast_1d(np.asarray(thetaDeg, float))
+    lam = np.atleast_1d(np.asarray(res["lambdas"], dtype=float))
+    lam0 = float(res.get("params", {}).get("lambda0", 1.55)) if isinstance(res.get("params"), dict) else 1.55
+    g0, g1 = res.get("grating", (float(np.min(res["xUp"])), float(np.max(res["xUp"]))))
+    x0 = np.arange(g0, g1 + 1e-9, 0.1)
+    eta, _ = fiberCoupling(res, np.deg2rad(theta), x0, w0)
+    il = int(np.argmin(np.abs(lam - lam0)))
+    i, j = np.unravel_index(int(np.argmax(eta[:, :, il])), eta[:, :, il].shape)
+    best = float(eta[i, j, il])
+    spec = eta[i, j, :].copy()
+    inband = lam[spec >= best / 10 ** 0.1]
+    pup = np.atleast_1d(np.asarray(res["Pup"], dtype=float))
+    return dict(eta=best, dB=10 * np.log10(best) if best > 0 else -np.inf, theta=float(theta[i]), x0=float(x0[j]),
+                spectrum=spec, band1dB=np.array([inband.min(), inband.max()]) if inband.size else np.array([]),
+                Pup=float(pup[il] if pup.size > 1 else pup[0]), lambdas=lam.copy())
+
+
+def _slab_te0(n_core_top: float, q: dict) -> float:
+    """TE0 effective index of the SOI slab whose Si is n_core_top thick (BOX
+    below, cladding above), on a 5 nm grid."""
+    dz = 0.005
+    z = np.arange(-2.0, n_core_top + 2.0, dz) + dz / 2
+    n = np.where(z < 0, float(q["nBox"]), np.where(z < n_core_top, float(q["nSi"]), float(q["nClad"])))
+    m = slabModes(z, n, float(q["lambda0"]), "TE", 1)
+    return float(np.real(m["neff"][0]))
+
+
+def apodizedGrating(ffStart: float, ffEnd: float, thetaDeg: float, nPer: int, scale: float = 1.0, p: Any = None):
+    """[period, ff] = apodizedGrating(ffStart, ffEnd, thetaDeg, nPer, scale, p)
+    (apodizedGrating.m:1-9, documented interface): the unetched fraction
+    ramps linearly from ffStart to ffEnd over nPer periods, and each period
+    meets the local Bragg condition
+        period_k = scale * lambda0 / (neff_k - nClad sin(theta)),
+        neff_k = ff_k n_full + (1 - ff_k) n_etched,
+    with n_full, n_etched the TE0 slab indices of the unetched (tSi) and
+    etched (tSi - etch) cross-sections of the gratingCouplerTE stack p."""
+    q = _params(p)
+    ff = np.linspace(float(ffStart), float(ffEnd), int(nPer))
+    n_full = _slab_te0(float(q["tSi"]), q)
+    n_etch = _slab_te0(float(q["tSi"]) - float(q["etch"]), q)
+    neff = ff * n_full + (1.0 - ff) * n_etch
+    period = float(scale) * float(q["lambda0"]) / (neff - float(q["nClad"]) * np.sin(np.deg2rad(float(thetaDeg))))
+    return period, ff

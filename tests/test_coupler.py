@@ -59,3 +59,31 @@ def test_apodized_and_sidewall_geometry():
     sw, _ = coupler._grating_boxes(coupler._params(dict(nPer=2, sidewall=80)))
     widths = [b[1] - b[0] for b in sw[: len(sw) // 2]]
     assert all(w2 < w1 for w1, w2 in zip(widths, widths[1:]))   # narrowing with depth
+
+
+def test_best_fiber_coupling_finds_the_matching_fiber():
+    """A field that is a tilted Gaussian at 9 deg centred at 10.3 um: the scan
+    (bestFiberCoupling.m:1-8 interface) finds that fiber, eta = Pup there."""
+    x = np.arange(0, 20.0 + 1e-9, 0.02)
+    lam = np.array([1.53, 1.55, 1.57])
+    th, w0, xc = np.deg2rad(9.0), 5.2, 10.3
+    E = np.stack([np.exp(-((x - xc) * np.cos(th) / w0) ** 2) * np.exp(1j * 2 * np.pi / l * np.sin(th) * (x - xc))
+                  for l in lam], axis=1)
+    res = dict(xUp=x, EyUp=E, lambdas=lam, nClad=1.0, Pup=np.array([0.5, 0.6, 0.55]), grating=(4.0, 16.0),
+               params=dict(lambda0=1.55))
+    b = coupler.bestFiberCoupling(res, np.arange(5, 15.01, 0.5), w0)
+    assert b["theta"] == 9.0 and abs(b["x0"] - 10.3) < 1e-9
+    assert abs(b["eta"] - 0.6) < 1e-9 and abs(b["Pup"] - 0.6) < 1e-12
+    assert b["spectrum"].shape == (3,) and b["band1dB"][0] <= 1.55 <= b["band1dB"][1]
+
+
+def test_apodized_grating_meets_the_bragg_condition():
+    per, ff = coupler.apodizedGrating(0.875, 0.435, 15, 25, 1.014)
+    assert per.shape == (25,) and np.allclose(ff, np.linspace(0.875, 0.435, 25))
+    q = coupler._params(None)
+    nf = coupler._slab_te0(0.22, q)
+    ne = coupler._slab_te0(0.22 - 0.07, q)
+    assert 2.7 < nf < 2.95 and ne < nf                  # TE0 of 220 nm / 150 nm Si in air-clad SOI
+    neff = ff * nf + (1 - ff) * ne
+    np.testing.assert_allclose(per * (neff - np.sin(np.deg2rad(15))), 1.014 * 1.55, rtol=1e-12)
+    assert np.all(np.diff(per) > 0)                     # weaker grating toward the end: longer periods

@@ -59,3 +59,19 @@ def test_default_design_point():
     i, j = np.unravel_index(np.argmax(eta[:, :, iL]), eta[:, :, iL].shape)
     assert abs(np.rad2deg(th[i]) - 10.5) <= 1.0
     assert abs(eta[i, j, iL] - 0.481) < 0.03
+
+
+def test_apodized_box_sweep_as_one_batch():
+    """The BOX-thickness sweep of examples/cpo_box_scan.m:16-31 (apodized
+    design, best fiber per BOX) as one batched submission; the batched
+    budgets equal single runs, and the best fiber lies in the scanned range."""
+    base = dict(lambdas=[1.53, 1.55, 1.57], precision="single")
+    per, ff = coupler.apodizedGrating(0.875, 0.435, 15, 10, 1.014, base)
+    ps = [dict(base, period=per, ff=ff, nPer=10, box=b) for b in (1.8, 2.0, 2.2)]
+    rs = coupler.gratingCouplerTE_batch(ps)
+    for p, r in zip(ps, rs):
+        assert np.max(np.abs(r["balance"])) < 1e-3
+        b = coupler.bestFiberCoupling(r, np.arange(5, 15.01, 1.0))
+        assert 0 < b["eta"] <= b["Pup"] + 1e-12 and 5 <= b["theta"] <= 15
+    a = coupler.gratingCouplerTE(ps[1])
+    assert np.array_equal(a["Pup"], rs[1]["Pup"])
