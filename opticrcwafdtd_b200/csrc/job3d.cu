@@ -3,9 +3,11 @@
 // Host work at creation: validate the sim struct, turn the three eps arrays
 // into material indices (uint8/16/32) plus a table of C/eps (exact), build the
 // CPML profiles and slab maps of every axis, the TF/SF plane tables, the DFT
-// streams of the monitor planes (Ea, Eb, Ha, Hb) and the column tiles, and
-// upload everything into one device arena.  A time step is the in-place H
-// then E half-step kernel (step3d.cu); the shared ChunkEngine runs the loop.
+// streams of the monitor planes (Ea, Eb, Ha, Hb), the column tiles and z
+// segments, and the TMA tensor maps, and upload everything into one device
+// arena.  A time step is one launch of the fused H+E kernel over the interior
+// tiles and one over the CPML tiles (step3d_fused.cu), reading one field
+// buffer and writing the other; the shared ChunkEngine runs the loop.
 #include <cuda.h>   // CUtensorMap and the cuTensorMapEncodeTiled signature (entry point fetched at run time)
 
 #include <algorithm>

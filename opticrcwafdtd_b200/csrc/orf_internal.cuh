@@ -207,7 +207,6 @@ bool fast2d_info(int id, bool fp64, bool pml, Variant2D* v);
 cudaError_t launch_fast2d(bool fp64, bool te, bool idx16, bool pml, int variant, const FastTile2D* tiles, int ntiles,
                           int launch_off, int nsub, int par, int want_energy, int grid, cudaStream_t s);
 int fast2d_blocks_per_sm(bool fp64, bool te, bool idx16, bool pml, int variant);
-int step2d_blocks_per_sm(bool fp64, bool te, bool idx16, bool pml, int variant);
 
 constexpr int kTile3X = 32, kTile3Y = 8;   // 3D CTA tile (x, y)
 constexpr int kSeg3 = 60;                  // z planes marched by one 3D CTA
