@@ -426,6 +426,21 @@ int Job2D<R>::pick_tiling(int npx, int npz) {
     // below the upper slabs (A starts at nz-1-npz, B at nx-1-npx) and exist.
     int ax = npx + T, bx = nx - npx - T;
     int az = per ? 0 : npz + T, bz = per ? nz : nz - npz - T;
+    // A frame tile outputs a fixed extent whatever the strip needs, so widen
+    // the strips to whole frame tiles: the frame costs the same number of
+    // tiles and the interior shrinks by the cells the frame covers anyway.
+    {
+        const int ohp = pv.lz() - 2 * T;                       // frame tile output rows
+        const int l0 = -T - (((-T) % 4) + 4) % 4;               // loaded origin of a tile at x = 0
+        const int owl = l0 + pv.lx() - T;                       // its output columns
+        const int owr = pv.lx() - 2 * T - 3;                    // output columns, worst x alignment
+        if (ohp > 0 && !per) {
+            az = ((az + ohp - 1) / ohp) * ohp;
+            bz = nz - ((nz - bz + ohp - 1) / ohp) * ohp;
+        }
+        if (owl > 0 && ax < owl) ax = owl;
+        if (owr > 0 && nx - bx < owr) bx = nx - owr;
+    }
     if (bx - ax < 8 || bz - az < 4) { ax = bx = 0; az = bz = 0; }   // everything is frame
     std::vector<FastTile2D> inner, frame;
     // tile the rectangle [x0,x1) x [z0,z1) with a geometry of LX x LZ cells;
