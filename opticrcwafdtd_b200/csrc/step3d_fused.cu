@@ -73,25 +73,51 @@ __device__ __forceinline__ int slab(bool half, int u, int n, int np) {
     return u >= hi ? np + (u - hi) : -1;
 }
 
-// CPML-stretched difference d -> d/kappa + psi, psi <- b psi + a d, reading
-// psi of buffer par and (store) writing buffer par^1
-template <bool PML, class R>
-__device__ __forceinline__ R cpml(const Inst3D<R>* __restrict__ I, int par, bool store, bool half, int c, int q,
-                                  int coord, int i, int j, int k, R d) {
-    if (!PML) return d;
-    const int sl = slab(half, coord, I->n[q], I->np[q]);
-    if (sl < 0) return d;
-    const R* prof = half ? I->pmlH[q] : I->pmlI[q];
-    const R b = prof[3 * coord], a = prof[3 * coord + 1], ki = prof[3 * coord + 2];
-    int v[3] = {i, j, k};
-    int dim[3] = {I->n[0], I->n[1], I->n[2]};
-    v[q] = sl;
-    dim[q] = half ? I->nslabH[q] : I->nslabI[q];
-    const size_t o = (size_t)v[0] + (size_t)dim[0] * ((size_t)v[1] + (size_t)dim[1] * v[2]);
-    const R* pin = half ? I->psiH[par][c][q] : I->psiE[par][c][q];
-    const R p = b * pin[o] + a * d;
-    if (store) (half ? I->psiH[par ^ 1][c][q] : I->psiE[par ^ 1][c][q])[o] = p;
-    return d * ki + p;
+// CPML context of one instance, staged in shared memory by the CPML launches
+// so that a stretched difference costs one psi load, not a chain of
+// dependent descriptor loads.  kind 0: E update (integer positions, psiE),
+// kind 1: H update (half positions, psiH).
+template <class R>
+struct Cpml3 {
+    const R* prof[2][3];        // (b, a, 1/kappa) per coordinate, per axis
+    const R* pin[2][3][3];      // psi of (component, axis), buffer par (read)
+    R* pout[2][3][3];           // the same, buffer par^1 (written)
+    int n[3], np[3], nsl[2][3];
+};
+
+// The six differences of one cell's H or E update, in the order
+// (c, q) = (0,1) (0,2) (1,2) (1,0) (2,0) (2,1): component c, derivative axis q.
+// CPML stretch d -> d/kappa + psi, psi <- b psi + a d (reading buffer par,
+// writing par^1 when store) of those on an absorbing slab of their axis,
+// axis by axis: the two psi loads of an axis are issued together, and a cell
+// on the slab of a single axis (all but the slab corners) has all its psi
+// loads in flight at once.  psi of buffer par is read-only during the launch.
+template <class R>
+__device__ __forceinline__ void cpml6(const Cpml3<R>& X, int kind, bool store, int i, int j, int k, R (&d)[6]) {
+    const bool half = kind == 1;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        const int coord = q == 0 ? i : (q == 1 ? j : k);
+        const int sl = slab(half, coord, X.n[q], X.np[q]);
+        if (sl < 0) continue;
+        // the entries on axis q: (component c1, entry e1), (c2, e2)
+        constexpr int E1[3] = {3, 0, 1}, E2[3] = {4, 5, 2};
+        constexpr int C1[3] = {1, 0, 0}, C2[3] = {2, 2, 1};
+        const int v0 = q == 0 ? sl : i, v1 = q == 1 ? sl : j, v2 = q == 2 ? sl : k;
+        const int d0 = q == 0 ? X.nsl[kind][0] : X.n[0], d1 = q == 1 ? X.nsl[kind][1] : X.n[1];
+        const size_t o = (size_t)v0 + (size_t)d0 * ((size_t)v1 + (size_t)d1 * v2);
+        const R* pr = X.prof[kind][q] + 3 * coord;
+        const R ps1 = __ldg(X.pin[kind][C1[q]][q] + o), ps2 = __ldg(X.pin[kind][C2[q]][q] + o);
+        const R b = __ldg(pr), a = __ldg(pr + 1), ki = __ldg(pr + 2);
+        const R p1 = b * ps1 + a * d[E1[q]];
+        const R p2 = b * ps2 + a * d[E2[q]];
+        if (store) {
+            X.pout[kind][C1[q]][q][o] = p1;
+            X.pout[kind][C2[q]][q][o] = p2;
+        }
+        d[E1[q]] = d[E1[q]] * ki + p1;
+        d[E2[q]] = d[E2[q]] * ki + p2;
+    }
 }
 
 __device__ __forceinline__ void cp4(void* sdst, const void* gsrc, bool valid) {
@@ -147,22 +173,18 @@ __device__ __forceinline__ void tma_load3(void* sdst, const void* tmap, int x, i
 
 // H update of one cell (the split formulation's operations, in order)
 template <bool PML, class R>
-__device__ __forceinline__ void h_cell(const Inst3D<R>* __restrict__ I, int par, bool store, int i, int j, int k,
-                                       R ex, R ey, R ez, R ex_k, R ey_k, R ez_i, R ey_i, R ez_j, R ex_j, R& hx, R& hy,
-                                       R& hz, R gE) {
+__device__ __forceinline__ void h_cell(const Inst3D<R>* __restrict__ I, const Cpml3<R>& X, bool store, int i, int j,
+                                       int k, R ex, R ey, R ez, R ex_k, R ey_k, R ez_i, R ey_i, R ez_j, R ex_j, R& hx,
+                                       R& hy, R& hz, R gE) {
     const R C = I->C;
     // Hx -= C ((Ez(j+1) - Ez) - (Ey(k+1) - Ey))
-    R d1 = cpml<PML>(I, par, store, true, 0, 1, j, i, j, k, ez_j - ez);
-    R d2 = cpml<PML>(I, par, store, true, 0, 2, k, i, j, k, ey_k - ey);
-    hx = hx - C * (d1 - d2);
     // Hy -= C ((Ex(k+1) - Ex) - (Ez(i+1) - Ez))
-    d1 = cpml<PML>(I, par, store, true, 1, 2, k, i, j, k, ex_k - ex);
-    d2 = cpml<PML>(I, par, store, true, 1, 0, i, i, j, k, ez_i - ez);
-    hy = hy - C * (d1 - d2);
     // Hz -= C ((Ey(i+1) - Ey) - (Ex(j+1) - Ex))
-    d1 = cpml<PML>(I, par, store, true, 2, 0, i, i, j, k, ey_i - ey);
-    d2 = cpml<PML>(I, par, store, true, 2, 1, j, i, j, k, ex_j - ex);
-    hz = hz - C * (d1 - d2);
+    R dd[6] = {ez_j - ez, ey_k - ey, ex_k - ex, ez_i - ez, ey_i - ey, ex_j - ex};
+    if (PML) cpml6(X, 1, store, i, j, k, dd);
+    hx = hx - C * (dd[0] - dd[1]);
+    hy = hy - C * (dd[2] - dd[3]);
+    hz = hz - C * (dd[4] - dd[5]);
     // TF/SF: the H plane just below the source plane is scattered field
     const int sa = I->sa;
     if (sel3(sa, i, j, k) == I->ss - 1) {
@@ -209,8 +231,22 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
     R* sHn = reinterpret_cast<R*>(dsm + ns * SB);      // [3][EB]
     __shared__ R slut[sizeof(IT) == 1 ? 256 : 1];
     __shared__ __align__(8) unsigned long long sbar[ns];
+    __shared__ Cpml3<R> sx;
 
     const int t = threadIdx.x;
+    if (PML && t < 18) {   // CPML context: thread (kind, c, q) copies one psi pair
+        const int kind = t / 9, c = (t / 3) % 3, q = t % 3;
+        sx.pin[kind][c][q] = kind ? I->psiH[par][c][q] : I->psiE[par][c][q];
+        sx.pout[kind][c][q] = kind ? I->psiH[par ^ 1][c][q] : I->psiE[par ^ 1][c][q];
+        if (c == 0) {
+            sx.prof[kind][q] = kind ? I->pmlH[q] : I->pmlI[q];
+            sx.nsl[kind][q] = kind ? I->nslabH[q] : I->nslabI[q];
+            if (kind == 0) {
+                sx.n[q] = I->n[q];
+                sx.np[q] = I->np[q];
+            }
+        }
+    }
     const int tx = t % TX, ty = t / TX;
     const int nx = I->n[0], ny = I->n[1], nz = I->n[2], pitch = I->pitch;
     const bool px = I->per[0] != 0, py = I->per[1] != 0, pz = I->per[2] != 0;
@@ -347,7 +383,7 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
             const R ez_i = iok ? __ldg(Ein[2] + oi) : R(0), ey_i = iok ? __ldg(Ein[1] + oi) : R(0);
             const R ez_j = jok ? __ldg(Ein[2] + oj) : R(0), ex_j = jok ? __ldg(Ein[0] + oj) : R(0);
             R hx = __ldg(Hin[0] + o), hy = __ldg(Hin[1] + o), hz = __ldg(Hin[2] + o);
-            h_cell<PML>(I, par, false, i, j, km, ex, ey, ez, ex_k, ey_k, ez_i, ey_i, ez_j, ex_j, hx, hy, hz, gE);
+            h_cell<PML>(I, sx, false, i, j, km, ex, ey, ez, ex_k, ey_k, ez_i, ey_i, ez_j, ex_j, hx, hy, hz, gE);
             hxm = hx;
             hym = hy;
         }
@@ -389,24 +425,8 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
         const R* H0x = sHq(s0, 0);
         const R* H0y = sHq(s0, 1);
         const R* H0z = sHq(s0, 2);
-        // ---- H of plane k: own cell, then the halo cell
-        {
-            const int e = eo;
-            R hx = H0x[e], hy = H0y[e], hz = H0z[e];
-            if (own) {
-                h_cell<PML>(I, par, true, i, j, k, E0x[e], E0y[e], E0z[e], E1x[e], E1y[e], E0z[e + 1], E0y[e + 1],
-                            E0z[e + SX], E0x[e + SX], hx, hy, hz, gE);
-                const size_t o = (size_t)k * plane + (size_t)j * pitch + i;
-                Hout[0][o] = hx;
-                Hout[1][o] = hy;
-                Hout[2][o] = hz;
-            } else {
-                hx = hy = hz = R(0);
-            }
-            sHn[e] = hx;
-            sHn[EBr + e] = hy;
-            sHn[2 * EBr + e] = hz;
-        }
+        // ---- H of plane k: the halo cell (its psi reads issued ahead of the
+        // own cell's psi writes), then the own cell
         if (hasHalo) {
             const int e = he;
             R hx = R(0), hy = R(0), hz = R(0);
@@ -414,8 +434,25 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
                 hx = H0x[e];
                 hy = H0y[e];
                 hz = H0z[e];
-                h_cell<PML>(I, par, false, hi, hj, k, E0x[e], E0y[e], E0z[e], E1x[e], E1y[e], E0z[e + 1], E0y[e + 1],
+                h_cell<PML>(I, sx, false, hi, hj, k, E0x[e], E0y[e], E0z[e], E1x[e], E1y[e], E0z[e + 1], E0y[e + 1],
                             E0z[e + SX], E0x[e + SX], hx, hy, hz, gE);
+            }
+            sHn[e] = hx;
+            sHn[EBr + e] = hy;
+            sHn[2 * EBr + e] = hz;
+        }
+        {
+            const int e = eo;
+            R hx = H0x[e], hy = H0y[e], hz = H0z[e];
+            if (own) {
+                h_cell<PML>(I, sx, true, i, j, k, E0x[e], E0y[e], E0z[e], E1x[e], E1y[e], E0z[e + 1], E0y[e + 1],
+                            E0z[e + SX], E0x[e + SX], hx, hy, hz, gE);
+                const size_t o = (size_t)k * plane + (size_t)j * pitch + i;
+                Hout[0][o] = hx;
+                Hout[1][o] = hy;
+                Hout[2][o] = hz;
+            } else {
+                hx = hy = hz = R(0);
             }
             sHn[e] = hx;
             sHn[EBr + e] = hy;
@@ -430,17 +467,13 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
             const R hx_j = sHn[e - SX], hz_j = sHn[2 * EBr + e - SX];
             const int v0 = (int)sIq(s0, 0)[t], v1 = (int)sIq(s0, 1)[t], v2 = (int)sIq(s0, 2)[t];
             // Ex += cx ((Hz - Hz(j-1)) - (Hy - Hy(k-1)))
-            R d1 = cpml<PML>(I, par, true, false, 0, 1, j, i, j, k, hzk - hz_j);
-            R d2 = cpml<PML>(I, par, true, false, 0, 2, k, i, j, k, hyk - hym);
-            R ex = E0x[e] + coef<R, IT>(slut, I->lutc, v0) * (d1 - d2);
             // Ey += cy ((Hx - Hx(k-1)) - (Hz - Hz(i-1)))
-            d1 = cpml<PML>(I, par, true, false, 1, 2, k, i, j, k, hxk - hxm);
-            d2 = cpml<PML>(I, par, true, false, 1, 0, i, i, j, k, hzk - hz_i);
-            R ey = E0y[e] + coef<R, IT>(slut, I->lutc, v1) * (d1 - d2);
             // Ez += cz ((Hy - Hy(i-1)) - (Hx - Hx(j-1)))
-            d1 = cpml<PML>(I, par, true, false, 2, 0, i, i, j, k, hyk - hy_i);
-            d2 = cpml<PML>(I, par, true, false, 2, 1, j, i, j, k, hxk - hx_j);
-            R ez = E0z[e] + coef<R, IT>(slut, I->lutc, v2) * (d1 - d2);
+            R dd[6] = {hzk - hz_j, hyk - hym, hxk - hxm, hzk - hz_i, hyk - hy_i, hxk - hx_j};
+            if (PML) cpml6(sx, 0, true, i, j, k, dd);
+            R ex = E0x[e] + coef<R, IT>(slut, I->lutc, v0) * (dd[0] - dd[1]);
+            R ey = E0y[e] + coef<R, IT>(slut, I->lutc, v1) * (dd[2] - dd[3]);
+            R ez = E0z[e] + coef<R, IT>(slut, I->lutc, v2) * (dd[4] - dd[5]);
             // TF/SF: the source plane is total field
             const int sa = I->sa;
             if (sel3(sa, i, j, k) == I->ss) {
