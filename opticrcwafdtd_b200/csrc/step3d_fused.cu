@@ -175,7 +175,7 @@ __device__ __forceinline__ void tma_load3(void* sdst, const void* tmap, int x, i
 template <bool PML, class R>
 __device__ __forceinline__ void h_cell(const Inst3D<R>* __restrict__ I, const Cpml3<R>& X, bool store, int i, int j,
                                        int k, R ex, R ey, R ez, R ex_k, R ey_k, R ez_i, R ey_i, R ez_j, R ex_j, R& hx,
-                                       R& hy, R& hz, R gE) {
+                                       R& hy, R& hz, R gE, bool src) {
     const R C = I->C;
     // Hx -= C ((Ez(j+1) - Ez) - (Ey(k+1) - Ey))
     // Hy -= C ((Ex(k+1) - Ex) - (Ez(i+1) - Ez))
@@ -186,8 +186,9 @@ __device__ __forceinline__ void h_cell(const Inst3D<R>* __restrict__ I, const Cp
     hy = hy - C * (dd[2] - dd[3]);
     hz = hz - C * (dd[4] - dd[5]);
     // TF/SF: the H plane just below the source plane is scattered field
-    const int sa = I->sa;
-    if (sel3(sa, i, j, k) == I->ss - 1) {
+    // (src: sel3(sa, i, j, k) == ss - 1)
+    if (src) {
+        const int sa = I->sa;
         const int sb = (sa + 1) % 3, sc = (sa + 2) % 3;
         const size_t pq = (size_t)sel3(sb, i, j, k) + (size_t)I->na * sel3(sc, i, j, k);
         const R ua = __ldg(I->sHa + pq) * gE, ub = __ldg(I->sHb + pq) * gE;
@@ -383,7 +384,8 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
             const R ez_i = iok ? __ldg(Ein[2] + oi) : R(0), ey_i = iok ? __ldg(Ein[1] + oi) : R(0);
             const R ez_j = jok ? __ldg(Ein[2] + oj) : R(0), ex_j = jok ? __ldg(Ein[0] + oj) : R(0);
             R hx = __ldg(Hin[0] + o), hy = __ldg(Hin[1] + o), hz = __ldg(Hin[2] + o);
-            h_cell<PML>(I, sx, false, i, j, km, ex, ey, ez, ex_k, ey_k, ez_i, ey_i, ez_j, ex_j, hx, hy, hz, gE);
+            h_cell<PML>(I, sx, false, i, j, km, ex, ey, ez, ex_k, ey_k, ez_i, ey_i, ez_j, ex_j, hx, hy, hz, gE,
+                        sel3(I->sa, i, j, km) == I->ss - 1);
             hxm = hx;
             hym = hy;
         }
@@ -407,6 +409,20 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
         if (ax == 2) mz |= 1u << m;
         else if ((ax == 0 && i == ix) || (ax == 1 && j == ix)) mcol |= 1u << m;
     }
+    // planes of the segment (k - k0 < kSeg3 <= 64) that carry a z normal monitor
+    static_assert(kSeg3 <= 64, "one bit per plane of a segment");
+    unsigned long long zpl = 0;
+    for (unsigned b = mz; b; b &= b - 1) {
+        const int dk = I->mon_index[__ffs(b) - 1] - k0;
+        if (dk >= 0 && dk < k1 - k0) zpl |= 1ull << dk;
+    }
+    // the TF/SF plane: on an x / y plane a fixed set of columns, on a z plane
+    // one plane of the march (sel3(sa, i, j, k) == ss - 1 for H, == ss for E)
+    const int sa = I->sa, ss = I->ss;
+    const int kSrcH = sa == 2 ? ss - 1 : -2, kSrcE = sa == 2 ? ss : -2;
+    const bool ownSrcH = sa != 2 && sel3(sa, i, j, 0) == ss - 1;
+    const bool ownSrcE = sa != 2 && sel3(sa, i, j, 0) == ss;
+    const bool haloSrcH = sa != 2 && sel3(sa, hi, hj, 0) == ss - 1;
     double energy = 0.0;
     R* smp0 = I->samples + (size_t)launch_off * I->sstride;
     for (int k = k0; k < k1; ++k) {
@@ -435,7 +451,7 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
                 hy = H0y[e];
                 hz = H0z[e];
                 h_cell<PML>(I, sx, false, hi, hj, k, E0x[e], E0y[e], E0z[e], E1x[e], E1y[e], E0z[e + 1], E0y[e + 1],
-                            E0z[e + SX], E0x[e + SX], hx, hy, hz, gE);
+                            E0z[e + SX], E0x[e + SX], hx, hy, hz, gE, haloSrcH || k == kSrcH);
             }
             sHn[e] = hx;
             sHn[EBr + e] = hy;
@@ -446,7 +462,7 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
             R hx = H0x[e], hy = H0y[e], hz = H0z[e];
             if (own) {
                 h_cell<PML>(I, sx, true, i, j, k, E0x[e], E0y[e], E0z[e], E1x[e], E1y[e], E0z[e + 1], E0y[e + 1],
-                            E0z[e + SX], E0x[e + SX], hx, hy, hz, gE);
+                            E0z[e + SX], E0x[e + SX], hx, hy, hz, gE, ownSrcH || k == kSrcH);
                 const size_t o = (size_t)k * plane + (size_t)j * pitch + i;
                 Hout[0][o] = hx;
                 Hout[1][o] = hy;
@@ -475,8 +491,7 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
             R ey = E0y[e] + coef<R, IT>(slut, I->lutc, v1) * (dd[2] - dd[3]);
             R ez = E0z[e] + coef<R, IT>(slut, I->lutc, v2) * (dd[4] - dd[5]);
             // TF/SF: the source plane is total field
-            const int sa = I->sa;
-            if (sel3(sa, i, j, k) == I->ss) {
+            if (ownSrcE || k == kSrcE) {
                 const int sb = (sa + 1) % 3, sc = (sa + 2) % 3;
                 const size_t pq = (size_t)sel3(sb, i, j, k) + (size_t)I->na * sel3(sc, i, j, k);
                 const R ua = __ldg(I->sEa + pq) * gH, ub = __ldg(I->sEb + pq) * gH;
@@ -490,9 +505,11 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
             Eout[2][o] = ez;
             // DFT samples: E on the plane, H averaged over the planes m-1, m of its normal
             unsigned hit = mcol;
-            for (unsigned b = mz; b; b &= b - 1) {
-                const int m = __ffs(b) - 1;
-                if (k == I->mon_index[m]) hit |= 1u << m;
+            if ((zpl >> it) & 1ull) {
+                for (unsigned b = mz; b; b &= b - 1) {
+                    const int m = __ffs(b) - 1;
+                    if (k == I->mon_index[m]) hit |= 1u << m;
+                }
             }
             for (; hit; hit &= hit - 1) {
                 const int m = __ffs(hit) - 1;
