@@ -457,28 +457,32 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
             sHn[EBr + e] = hy;
             sHn[2 * EBr + e] = hz;
         }
+        // the own cell's E and new H stay in registers for the E update
+        R exo = R(0), eyo = R(0), ezo = R(0), hxk = R(0), hyk = R(0), hzk = R(0);
         {
             const int e = eo;
-            R hx = H0x[e], hy = H0y[e], hz = H0z[e];
             if (own) {
-                h_cell<PML>(I, sx, true, i, j, k, E0x[e], E0y[e], E0z[e], E1x[e], E1y[e], E0z[e + 1], E0y[e + 1],
-                            E0z[e + SX], E0x[e + SX], hx, hy, hz, gE, ownSrcH || k == kSrcH);
+                exo = E0x[e];
+                eyo = E0y[e];
+                ezo = E0z[e];
+                hxk = H0x[e];
+                hyk = H0y[e];
+                hzk = H0z[e];
+                h_cell<PML>(I, sx, true, i, j, k, exo, eyo, ezo, E1x[e], E1y[e], E0z[e + 1], E0y[e + 1], E0z[e + SX],
+                            E0x[e + SX], hxk, hyk, hzk, gE, ownSrcH || k == kSrcH);
                 const size_t o = (size_t)k * plane + (size_t)j * pitch + i;
-                Hout[0][o] = hx;
-                Hout[1][o] = hy;
-                Hout[2][o] = hz;
-            } else {
-                hx = hy = hz = R(0);
+                Hout[0][o] = hxk;
+                Hout[1][o] = hyk;
+                Hout[2][o] = hzk;
             }
-            sHn[e] = hx;
-            sHn[EBr + e] = hy;
-            sHn[2 * EBr + e] = hz;
+            sHn[e] = hxk;
+            sHn[EBr + e] = hyk;
+            sHn[2 * EBr + e] = hzk;
         }
         __syncthreads();
         // ---- E of plane k at the own cell
         if (own) {
             const int e = eo;
-            const R hxk = sHn[e], hyk = sHn[EBr + e], hzk = sHn[2 * EBr + e];
             const R hy_i = sHn[EBr + e - 1], hz_i = sHn[2 * EBr + e - 1];
             const R hx_j = sHn[e - SX], hz_j = sHn[2 * EBr + e - SX];
             const int v0 = (int)sIq(s0, 0)[t], v1 = (int)sIq(s0, 1)[t], v2 = (int)sIq(s0, 2)[t];
@@ -487,9 +491,9 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
             // Ez += cz ((Hy - Hy(i-1)) - (Hx - Hx(j-1)))
             R dd[6] = {hzk - hz_j, hyk - hym, hxk - hxm, hzk - hz_i, hyk - hy_i, hxk - hx_j};
             if (PML) cpml6(sx, 0, true, i, j, k, dd);
-            R ex = E0x[e] + coef<R, IT>(slut, I->lutc, v0) * (dd[0] - dd[1]);
-            R ey = E0y[e] + coef<R, IT>(slut, I->lutc, v1) * (dd[2] - dd[3]);
-            R ez = E0z[e] + coef<R, IT>(slut, I->lutc, v2) * (dd[4] - dd[5]);
+            R ex = exo + coef<R, IT>(slut, I->lutc, v0) * (dd[0] - dd[1]);
+            R ey = eyo + coef<R, IT>(slut, I->lutc, v1) * (dd[2] - dd[3]);
+            R ez = ezo + coef<R, IT>(slut, I->lutc, v2) * (dd[4] - dd[5]);
             // TF/SF: the source plane is total field
             if (ownSrcE || k == kSrcE) {
                 const int sb = (sa + 1) % 3, sc = (sa + 2) % 3;
