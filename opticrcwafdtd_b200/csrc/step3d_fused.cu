@@ -39,6 +39,8 @@ template <class R>
 constexpr int NS = sizeof(R) == 4 ? 4 : 3;               // planes in the ring (FP64: 3, for occupancy)
 constexpr int RPT = (RC + NT - 1) / NT;                   // region cells per thread
 constexpr long long kSpinMax = 1ll << 20;                 // bounded mbarrier wait (try_wait polls)
+constexpr int kIssuer = NT - 32;   // issues the TMA copies and polls their mbarriers: lane 0 of the
+                                   // last warp, which has no halo H cell to recompute
 
 // per-slot layout (elements of R, each block 128-byte aligned for TMA)
 template <class R>
@@ -294,7 +296,7 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
         bool pok;
         const int pw = wrapc(p, nz, pz, &pok);
         if (use_tma) {
-            if (t == 0) {
+            if (t == kIssuer) {
                 const int zc = pok ? pw : -1;   // z = -1: the whole box reads as zero
                 // order the block's earlier generic reads of this slot before the async writes
                 asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
@@ -332,13 +334,13 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
                 reinterpret_cast<const unsigned char*>(I->idx[q]) + o, v);
         }
     };
-    // wait for plane p in slot s (TMA: thread 0 polls its mbarrier, the
+    // wait for plane p in slot s (TMA: the issuer polls its mbarrier, the
     // barrier that follows orders the data for everyone; cp.async: each
     // thread's own groups, made visible by the same barrier)
     bool timed_out = false;
     auto wait_plane = [&](int p, int s2) {
         if (use_tma) {
-            if (t != 0) return;
+            if (t != kIssuer) return;
             const unsigned parity = (unsigned)(((p - k0) / ns) & 1);
             long long spins = 0;
             while (!mbar_try_wait(&sbar[s2], parity)) {
@@ -392,6 +394,7 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
     }
 
     // halo H cell of this thread (41 of them: row j0-1, then column i0-1)
+    static_assert(kIssuer >= RX - 1 + TY, "the issuer warp has no halo cell");
     const bool hasHalo = t < RX - 1 + TY;
     const int hr = t < RX - 1 ? 0 : t - (RX - 1) + 1;
     const int hc = t < RX - 1 ? t : 0;
