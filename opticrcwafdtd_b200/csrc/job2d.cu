@@ -172,11 +172,14 @@ int Job2D<R>::create(const orf_sim2d* s) {
 
     // ---- tiles
     ORF_TRY(pick_tiling(npx, npz));
-    int lx_int = 32, lx_pml = 32;
+    int lx_int = 32, lx_pml = 32, lz_pml = 0;
     {
         Variant2D fv;
         if (fast2d_info(fvariant, sizeof(R) == 8, false, &fv)) lx_int = fv.lx();
-        if (fast2d_info(0, sizeof(R) == 8, true, &fv)) lx_pml = fv.lx();
+        if (fast2d_info(0, sizeof(R) == 8, true, &fv)) {
+            lx_pml = fv.lx();
+            lz_pml = fv.lz();
+        }
     }
 
     // ---- DFT streams: x monitors (P, B lines), z monitors (P, A lines)
@@ -327,6 +330,15 @@ int Job2D<R>::create(const orf_sim2d* s) {
         t.inst = d_inst;
         t.flags = 0;
         if ((sx - 1 >= t.li0 && sx - 1 < t.li0 + lxt) || (sx >= t.li0 && sx < t.li0 + lxt)) t.flags |= 1;
+        if ((int)q >= nfast) {
+            // frame tile: CPML slabs of x (columns < npx, >= nx-1-npx) and of
+            // z (rows < npz, >= nz-1-npz) that its loaded cells reach, with a
+            // cell of margin; the kernel skips the psi updates of an axis
+            // whose slabs the tile does not reach (they would leave every
+            // value unchanged: psi 0, profile (1, 0, 1))
+            if (npx > 0 && (t.li0 < npx + 1 || t.li0 + lxt > nx - npx - 2)) t.flags |= 8;
+            if (npz > 0 && (t.lk0 < npz + 1 || t.lk0 + lz_pml > nz - npz - 2)) t.flags |= 16;
+        }
         for (int m = 0; m < nM; ++m)
             if (s->monitors[m] >= t.oi0 && s->monitors[m] < t.oi0 + t.ow) t.flags |= 2;
         for (int m = 0; m < nMZ; ++m)

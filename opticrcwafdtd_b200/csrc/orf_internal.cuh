@@ -128,7 +128,8 @@ struct alignas(16) FastTile2D {
     int pitch, nz, periodic;
     int li0, lk0;           // loaded origin; li0 is a multiple of 4 cells (may be negative)
     int oi0, ok0, ow, oh;   // output rectangle
-    int flags;              // 1: TF/SF plane in the loaded columns, 2: x monitor, 4: z monitor
+    int flags;              // 1: TF/SF plane in the loaded columns, 2: x monitor, 4: z monitor,
+                            // 8 / 16: (frame tiles) the loaded cells reach an x / z CPML slab
     int nx;
     int pad;
 };

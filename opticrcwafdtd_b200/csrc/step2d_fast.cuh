@@ -26,13 +26,20 @@
 // Two instantiations per geometry: interior tiles (PML = false: every cell of
 // the tile's dependency cone is a plain cell, no masks and no CPML code) and
 // frame tiles (PML = true: CPML psi in a shared working plane, boundary
-// masks, zero fill outside the grid).  Both perform, cell by cell, the same
-// floating-point operations, so results do not depend on the tiling.
+// masks, zero fill outside the grid), the latter specialised on the CPML axes
+// a tile reaches.  Every update is written with explicit fma, so each
+// instantiation performs, cell by cell, the same roundings (no contraction
+// choice left to the compiler) and results do not depend on the tiling.
 #pragma once
 #include "orf_internal.cuh"
 
 namespace orf {
 namespace fast {
+
+template <bool B>
+struct Flag {
+    static constexpr bool value = B;
+};
 
 __device__ __forceinline__ int pmod(int a, int n) {
     int r = a % n;
@@ -381,124 +388,144 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
                 pxb = prx[cx * 6 + 0]; pxa = prx[cx * 6 + 1]; pxk = prx[cx * 6 + 2];
                 phb = prx[cx * 6 + 3]; pha = prx[cx * 6 + 4]; phk = prx[cx * 6 + 5];
             }
-            for (int s = 0; s < nsub; ++s) {
-                // ----- H half step: A (d/dz P), B (d/dx P)
-                if (lane == 0) store_row<R, KS>(&xPc[warp][0], P);
-                xPr[warp][lane] = P[0];
-                __syncthreads();
-                R Pdn = xPr[wDn][lane];
-                if (!hasDn) Pdn = PML ? R(0) : P[KS - 1];
-                constexpr int VEC = 16 / sizeof(R);
-                static_assert(KS % VEC == 0, "KS must be a multiple of 16 bytes of R");
-                R pe[VEC];
-#pragma unroll
-                for (int j = 0; j < KS; ++j) {
-                    const int c = (ck0 + j) * LX + cx;
-                    if (j % VEC == 0) load16<R>(pe, &xPc[wR][j]);
-                    R pr = __shfl_down_sync(FULL, P[j], 1);
-                    const R pej = (PML && !hasR) ? R(0) : pe[j % VEC];
-                    pr = (lane == 31) ? pej : pr;
-                    const R pk = (j + 1 < KS) ? P[j + 1] : Pdn;
-                    R dz = pk - P[j];
-                    R dx = pr - P[j];
-                    if (PML) {
-                        const R* pz = prz + (ck0 + j) * 6;
-                        const R ps = pz[3] * psA[c] + pz[4] * dz;
-                        psA[c] = ps;
-                        dz = dz * pz[5] + ps;
-                        const R qs = phb * psB[c] + pha * dx;
-                        psB[c] = qs;
-                        dx = dx * phk + qs;
-                    }
-                    const R ca = TE ? C : K0[j];
-                    const R cb = TE ? C : K1[j];
-                    if (PML) {
-                        if ((mA >> j) & 1u) A[j] += ca * dz;
-                        if ((mB >> j) & 1u) B[j] -= cb * dx;
-                    } else {
-                        A[j] += ca * dz;
-                        B[j] -= cb * dx;
-                    }
-                }
-                if (hs && i == six - 1) {   // TF/SF: the B column left of the plane is scattered field
-                    const R ge = (R)sg[0][s];
-#pragma unroll
+            // the fused steps, specialised on the CPML axes the tile reaches
+            // (frame tiles: flags 16 = z slab, 8 = x slab); skipping an axis
+            // the tile does not reach leaves every value unchanged
+            auto steps = [&](auto zc, auto xc) {
+                constexpr bool ZC = PML && decltype(zc)::value;
+                constexpr bool XC = PML && decltype(xc)::value;
+                for (int s = 0; s < nsub; ++s) {
+                    // ----- H half step: A (d/dz P), B (d/dx P)
+                    if (lane == 0) store_row<R, KS>(&xPc[warp][0], P);
+                    xPr[warp][lane] = P[0];
+                    __syncthreads();
+                    R Pdn = xPr[wDn][lane];
+                    if (!hasDn) Pdn = PML ? R(0) : P[KS - 1];
+                    constexpr int VEC = 16 / sizeof(R);
+                    static_assert(KS % VEC == 0, "KS must be a multiple of 16 bytes of R");
+                    R pe[VEC];
+    #pragma unroll
                     for (int j = 0; j < KS; ++j) {
-                        if ((mB >> j) & 1u) {
-                            const int kk = d.periodic ? pmod(kb + j, nz) : kb + j;
-                            B[j] += __ldg(I->srcB + kk) * ge;
+                        const int c = (ck0 + j) * LX + cx;
+                        if (j % VEC == 0) load16<R>(pe, &xPc[wR][j]);
+                        R pr = __shfl_down_sync(FULL, P[j], 1);
+                        const R pej = (PML && !hasR) ? R(0) : pe[j % VEC];
+                        pr = (lane == 31) ? pej : pr;
+                        const R pk = (j + 1 < KS) ? P[j + 1] : Pdn;
+                        R dz = pk - P[j];
+                        R dx = pr - P[j];
+                        if (ZC) {
+                            const R* pz = prz + (ck0 + j) * 6;
+                            const R ps = fma(pz[3], psA[c], pz[4] * dz);
+                            psA[c] = ps;
+                            dz = fma(dz, pz[5], ps);
+                        }
+                        if (XC) {
+                            const R qs = fma(phb, psB[c], pha * dx);
+                            psB[c] = qs;
+                            dx = fma(dx, phk, qs);
+                        }
+                        const R ca = TE ? C : K0[j];
+                        const R cb = TE ? C : K1[j];
+                        if (PML) {
+                            if ((mA >> j) & 1u) A[j] = fma(ca, dz, A[j]);
+                            if ((mB >> j) & 1u) B[j] = fma(-cb, dx, B[j]);
+                        } else {
+                            A[j] = fma(ca, dz, A[j]);
+                            B[j] = fma(-cb, dx, B[j]);
                         }
                     }
-                }
-                // ----- E half step: P (branch-free stencil loop)
-                if (lane == 31) store_row<R, KS>(&xBc[warp][0], B);
-                xAr[warp][lane] = A[KS - 1];
-                __syncthreads();
-                R Aup = xAr[wUp][lane];
-                if (!hasUp) Aup = PML ? R(0) : A[0];
-                R be[VEC];
-#pragma unroll
-                for (int j = 0; j < KS; ++j) {
-                    const int c = (ck0 + j) * LX + cx;
-                    if (j % VEC == 0) load16<R>(be, &xBc[wL][j]);
-                    R bl = __shfl_up_sync(FULL, B[j], 1);
-                    const R bej = (PML && !hasL) ? R(0) : be[j % VEC];
-                    bl = (lane == 0) ? bej : bl;
-                    const R am = (j > 0) ? A[j - 1] : Aup;
-                    R da = A[j] - am;
-                    R db = B[j] - bl;
-                    if (PML) {
-                        const R* pz = prz + (ck0 + j) * 6;
-                        const R ps = pz[0] * psPz[c] + pz[1] * da;
-                        psPz[c] = ps;
-                        da = da * pz[2] + ps;
-                        const R qs = pxb * psPx[c] + pxa * db;
-                        psPx[c] = qs;
-                        db = db * pxk + qs;
-                    }
-                    const R cp = TE ? K0[j] : C;
-                    if (PML) {
-                        if ((mP >> j) & 1u) P[j] += cp * (da - db);
-                    } else {
-                        P[j] += cp * (da - db);
-                    }
-                }
-                // rare paths, each behind a tile-uniform flag
-                if (hs && i == six) {   // TF/SF: the plane is total field
-                    const R gh = (R)sg[1][s];
-#pragma unroll
-                    for (int j = 0; j < KS; ++j) {
-                        if ((mP >> j) & 1u) {
-                            const int kk = d.periodic ? pmod(kb + j, nz) : kb + j;
-                            P[j] += __ldg(I->srcP + kk) * gh;
+                    if (hs && i == six - 1) {   // TF/SF: the B column left of the plane is scattered field
+                        const R ge = (R)sg[0][s];
+    #pragma unroll
+                        for (int j = 0; j < KS; ++j) {
+                            if ((mB >> j) & 1u) {
+                                const int kk = d.periodic ? pmod(kb + j, nz) : kb + j;
+                                B[j] = fma(__ldg(I->srcB + kk), ge, B[j]);
+                            }
                         }
                     }
-                }
-                if (d.flags & 6) {      // DFT monitor samples of this step
-                    const int sslot = launch_off + s;
-                    R* smp0 = I->samples + (size_t)sslot * I->sstride;
-#pragma unroll
+                    // ----- E half step: P (branch-free stencil loop)
+                    if (lane == 31) store_row<R, KS>(&xBc[warp][0], B);
+                    xAr[warp][lane] = A[KS - 1];
+                    __syncthreads();
+                    R Aup = xAr[wUp][lane];
+                    if (!hasUp) Aup = PML ? R(0) : A[0];
+                    R be[VEC];
+    #pragma unroll
                     for (int j = 0; j < KS; ++j) {
+                        const int c = (ck0 + j) * LX + cx;
                         if (j % VEC == 0) load16<R>(be, &xBc[wL][j]);
                         R bl = __shfl_up_sync(FULL, B[j], 1);
                         const R bej = (PML && !hasL) ? R(0) : be[j % VEC];
                         bl = (lane == 0) ? bej : bl;
-                        if (xm >= 0 && ((own >> j) & 1u)) {
-                            R* smp = smp0 + (size_t)xm * 2 * nz;
-                            smp[kb + j] = P[j];
-                            smp[nz + kb + j] = R(0.5) * (bl + B[j]);
+                        const R am = (j > 0) ? A[j - 1] : Aup;
+                        R da = A[j] - am;
+                        R db = B[j] - bl;
+                        if (ZC) {
+                            const R* pz = prz + (ck0 + j) * 6;
+                            const R ps = fma(pz[0], psPz[c], pz[1] * da);
+                            psPz[c] = ps;
+                            da = fma(da, pz[2], ps);
                         }
-                        if ((zmask >> j) & 1u) {
-                            const R am = (j > 0) ? A[j - 1] : Aup;
-                            for (int m = 0; m < I->nmonz; ++m) {
-                                if (I->monz[m] != kb + j) continue;
-                                R* smp = smp0 + (size_t)I->nmon * 2 * nz + (size_t)m * 2 * d.nx;
-                                smp[i] = P[j];
-                                smp[d.nx + i] = R(0.5) * (am + A[j]);
+                        if (XC) {
+                            const R qs = fma(pxb, psPx[c], pxa * db);
+                            psPx[c] = qs;
+                            db = fma(db, pxk, qs);
+                        }
+                        const R cp = TE ? K0[j] : C;
+                        if (PML) {
+                            if ((mP >> j) & 1u) P[j] = fma(cp, da - db, P[j]);
+                        } else {
+                            P[j] = fma(cp, da - db, P[j]);
+                        }
+                    }
+                    // rare paths, each behind a tile-uniform flag
+                    if (hs && i == six) {   // TF/SF: the plane is total field
+                        const R gh = (R)sg[1][s];
+    #pragma unroll
+                        for (int j = 0; j < KS; ++j) {
+                            if ((mP >> j) & 1u) {
+                                const int kk = d.periodic ? pmod(kb + j, nz) : kb + j;
+                                P[j] = fma(__ldg(I->srcP + kk), gh, P[j]);
+                            }
+                        }
+                    }
+                    if (d.flags & 6) {      // DFT monitor samples of this step
+                        const int sslot = launch_off + s;
+                        R* smp0 = I->samples + (size_t)sslot * I->sstride;
+    #pragma unroll
+                        for (int j = 0; j < KS; ++j) {
+                            if (j % VEC == 0) load16<R>(be, &xBc[wL][j]);
+                            R bl = __shfl_up_sync(FULL, B[j], 1);
+                            const R bej = (PML && !hasL) ? R(0) : be[j % VEC];
+                            bl = (lane == 0) ? bej : bl;
+                            if (xm >= 0 && ((own >> j) & 1u)) {
+                                R* smp = smp0 + (size_t)xm * 2 * nz;
+                                smp[kb + j] = P[j];
+                                smp[nz + kb + j] = R(0.5) * (bl + B[j]);
+                            }
+                            if ((zmask >> j) & 1u) {
+                                const R am = (j > 0) ? A[j - 1] : Aup;
+                                for (int m = 0; m < I->nmonz; ++m) {
+                                    if (I->monz[m] != kb + j) continue;
+                                    R* smp = smp0 + (size_t)I->nmon * 2 * nz + (size_t)m * 2 * d.nx;
+                                    smp[i] = P[j];
+                                    smp[d.nx + i] = R(0.5) * (am + A[j]);
+                                }
                             }
                         }
                     }
                 }
+            };
+            if constexpr (!PML) {
+                steps(Flag<false>{}, Flag<false>{});
+            } else {
+                const bool zc = (d.flags & 16) != 0, xc = (d.flags & 8) != 0;
+                if (zc && xc) steps(Flag<true>{}, Flag<true>{});
+                else if (zc) steps(Flag<true>{}, Flag<false>{});
+                else if (xc) steps(Flag<false>{}, Flag<true>{});
+                else steps(Flag<false>{}, Flag<false>{});
             }
             // ----- energy on the chunk's last launch
             if (want_energy) {
