@@ -172,6 +172,12 @@ typedef struct orf_kernel_stats {
     int64_t cell_updates;            /* all cells x time steps advanced           */
     int64_t h2d_bytes;               /* host->device bytes copied by run/create   */
     int64_t d2h_bytes;               /* device->host bytes copied by finish       */
+    /* host wall time of orf_batch2d_run calls, by phase: instance setup (host
+     * tables, device allocation, uploads, groups), the time loop, and the
+     * copy-out of results (with the release of the instances' memory) */
+    double setup_ms;
+    double loop_ms;
+    double finish_ms;
 } orf_kernel_stats;
 
 ORF_API int32_t     orf_abi_version(void);

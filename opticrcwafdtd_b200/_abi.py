@@ -100,7 +100,8 @@ class OrfKernelStats(C.Structure):
                 ("interior_cell_updates", C.c_int64),
                 ("frame_ms", C.c_double), ("frame_launches", C.c_int64), ("frame_cell_updates", C.c_int64),
                 ("flush_ms", C.c_double), ("flush_launches", C.c_int64),
-                ("cell_updates", C.c_int64), ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64)]
+                ("cell_updates", C.c_int64), ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64),
+                ("setup_ms", C.c_double), ("loop_ms", C.c_double), ("finish_ms", C.c_double)]
 
 
 class OrfServeCfg(C.Structure):

@@ -20,6 +20,7 @@ namespace {
 
 template <class R>
 int run_batch(orf_ctx* ctx, int n, const orf_sim2d* sims, orf_out2d* outs, orf_progress_fn progress, void* user) {
+    double t0 = now_s();
     std::vector<std::unique_ptr<Job2D<R>>> jobs;
     jobs.reserve(n);
     for (int q = 0; q < n; ++q) {
@@ -53,6 +54,8 @@ int run_batch(orf_ctx* ctx, int n, const orf_sim2d* sims, orf_out2d* outs, orf_p
     }
     cudaStream_t st = ctx->stream;
     for (auto& g : groups) ORF_TRY(g->build(st));
+    double t1 = now_s();
+    ctx->stats.setup_ms += 1e3 * (t1 - t0);
 
     // time loop: graph replays in batches; every instance's status ring is
     // read after each batch (progress = mean fraction, stop when all are done)
@@ -110,10 +113,15 @@ int run_batch(orf_ctx* ctx, int n, const orf_sim2d* sims, orf_out2d* outs, orf_p
     ORF_CUDA(se);
     for (auto& g : groups) g->eng.collect_timing();
     if (rc != ORF_OK) return rc;
+    t0 = now_s();
+    ctx->stats.loop_ms += 1e3 * (t0 - t1);
     for (int q = 0; q < n; ++q) {
         ctx->stats.cell_updates += jobs[q]->pl.last_step * jobs[q]->cells();
         ORF_TRY(jobs[q]->finish2d(&outs[q]));
     }
+    groups.clear();
+    jobs.clear();
+    ctx->stats.finish_ms += 1e3 * (now_s() - t0);
     return ORF_OK;
 }
 

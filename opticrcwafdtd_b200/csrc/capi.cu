@@ -32,6 +32,7 @@ void ctx_release(orf_ctx* c) {
     if (c->refs.fetch_sub(1) != 1) return;
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    dev_trim(c->device);   // the device blocks cached for reuse go back to the driver
     delete c;
 }
 

@@ -1,6 +1,9 @@
 // runtime.cu -- errors, shared physics definitions, context, chunk engine.
 #include <atomic>
+#include <map>
+#include <mutex>
 #include <thread>
+#include <unordered_map>
 
 #include "engine.cuh"
 
@@ -8,6 +11,115 @@ namespace orf {
 
 namespace {
 thread_local std::string g_err;
+}
+
+namespace {
+struct DevPool {
+    std::mutex mu;
+    std::multimap<size_t, void*> idle;                           // cached blocks by size
+    std::unordered_map<void*, std::pair<size_t, int>> blocks;    // every pool block: size, device
+    size_t idle_bytes = 0;
+};
+DevPool& dev_pool() {
+    static DevPool* p = new DevPool;   // never destroyed: blocks may be released during exit
+    return *p;
+}
+}  // namespace
+
+int dev_alloc(size_t bytes, void** out) {
+    *out = nullptr;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const size_t want = (bytes + kPoolGrain - 1) / kPoolGrain * kPoolGrain;
+    DevPool& P = dev_pool();
+    {
+        std::lock_guard<std::mutex> g(P.mu);
+        // the smallest cached block of this device that fits, wasting at most a quarter
+        for (auto it = P.idle.lower_bound(want); it != P.idle.end() && it->first <= want + want / 4 + kPoolGrain;
+             ++it) {
+            if (P.blocks[it->second].second != dev) continue;
+            *out = it->second;
+            P.idle_bytes -= it->first;
+            P.idle.erase(it);
+            return ORF_OK;
+        }
+    }
+    cudaError_t e = cudaMalloc(out, want);
+    if (e == cudaErrorMemoryAllocation) {   // give the cached blocks back and retry once
+        cudaGetLastError();
+        dev_trim(dev);
+        e = cudaMalloc(out, want);
+    }
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *out = nullptr;
+        set_error("device allocation of %.3f GB failed: %s", want / 1e9, cudaGetErrorString(e));
+        return ORF_ENOMEM_DEVICE;
+    }
+    std::lock_guard<std::mutex> g(P.mu);
+    P.blocks[*out] = {want, dev};
+    return ORF_OK;
+}
+
+void dev_free(void* p) {
+    if (!p) return;
+    DevPool& P = dev_pool();
+    size_t size = 0;
+    int bdev = 0;
+    {
+        std::lock_guard<std::mutex> g(P.mu);
+        auto it = P.blocks.find(p);
+        if (it == P.blocks.end()) return;
+        size = it->second.first;
+        bdev = it->second.second;
+    }
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != bdev) cudaSetDevice(bdev);
+    const cudaError_t e = cudaDeviceSynchronize();
+    std::vector<void*> evict;
+    {
+        std::lock_guard<std::mutex> g(P.mu);
+        if (e != cudaSuccess) {   // a failed context: do not keep its memory
+            P.blocks.erase(p);
+            evict.push_back(p);
+        } else {
+            P.idle.insert({size, p});
+            P.idle_bytes += size;
+            while (P.idle_bytes > kPoolKeep) {   // drop the largest cached blocks
+                auto last = std::prev(P.idle.end());
+                P.idle_bytes -= last->first;
+                evict.push_back(last->second);
+                P.blocks.erase(last->second);
+                P.idle.erase(last);
+            }
+        }
+    }
+    for (void* q : evict) cudaFree(q);
+    if (cur != bdev) cudaSetDevice(cur);
+}
+
+void dev_trim(int device) {
+    DevPool& P = dev_pool();
+    std::vector<void*> evict;
+    {
+        std::lock_guard<std::mutex> g(P.mu);
+        for (auto it = P.idle.begin(); it != P.idle.end();) {
+            if (P.blocks[it->second].second == device) {
+                P.idle_bytes -= it->first;
+                evict.push_back(it->second);
+                P.blocks.erase(it->second);
+                it = P.idle.erase(it);
+            } else {
+                ++it;
+            }
+        }
+    }
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (!evict.empty() && cur != device) cudaSetDevice(device);
+    for (void* q : evict) cudaFree(q);
+    if (!evict.empty() && cur != device) cudaSetDevice(cur);
 }
 
 void set_error(const char* fmt, ...) {

@@ -82,7 +82,18 @@ double progress_fraction(double t, double src_end, double ratio, double shutoff)
 // ---------------------------------------------------------------- context --
 struct orf_ctx_impl;
 
-// Bump allocator over one cudaMalloc: a job's buffers come from one block.
+// Device blocks for job and group arenas, with a per-process cache: a
+// released block is kept (up to kPoolKeep bytes in all) and handed to a later
+// request of about its size, so repeated runs map no new device memory.
+// Release waits for the device to be idle, as cudaFree does, so no kernel
+// still reads a block that is handed out again.
+constexpr size_t kPoolGrain = size_t(2) << 20;   // block sizes: multiples of 2 MiB
+constexpr size_t kPoolKeep = size_t(8) << 30;    // cached bytes kept for reuse
+int dev_alloc(size_t bytes, void** out);
+void dev_free(void* p);
+void dev_trim(int device);                        // cudaFree the cached blocks of a device
+
+// Bump allocator over one device block: a job's buffers come from one block.
 struct Arena {
     std::vector<std::pair<void**, size_t>> req;
     void* base = nullptr;
@@ -99,12 +110,8 @@ struct Arena {
     int alloc() {
         total = bytes();
         if (total == 0) return ORF_OK;
-        cudaError_t e = cudaMalloc(&base, total);
-        if (e != cudaSuccess) {
-            cudaGetLastError();
-            set_error("device allocation of %.3f GB failed: %s", total / 1e9, cudaGetErrorString(e));
-            return ORF_ENOMEM_DEVICE;
-        }
+        const int rc = dev_alloc(total, &base);
+        if (rc != ORF_OK) return rc;
         char* p = static_cast<char*>(base);
         for (auto& r : req) {
             *r.first = p;
@@ -141,7 +148,7 @@ struct Arena {
     }
     bool owned = true;
     void release() {
-        if (base && owned) cudaFree(base);
+        if (base && owned) dev_free(base);
         base = nullptr;
     }
 };

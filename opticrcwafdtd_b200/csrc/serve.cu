@@ -331,6 +331,7 @@ int32_t orf_serve_open(orf_ctx* ctx, const orf_serve_cfg* cfg, orf_server** srv)
         s->budget = (size_t)c.max_device_bytes;
     } else {
         size_t fr = 0, tot = 0;
+        dev_trim(ctx->device);   // cached blocks count as free memory here
         ORF_CUDA(cudaMemGetInfo(&fr, &tot));
         s->budget = (size_t)(0.9 * (double)fr);
     }
