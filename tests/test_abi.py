@@ -69,3 +69,30 @@ def test_no_device_fails_loudly_without_fallback():
     with pytest.raises(_abi.OrfError) as e:
         orf.fdtd2DTE(_sim())
     assert e.value.identifier == "orf:noDevice"
+
+
+def _header_struct_fields(name):
+    """Field names of `typedef struct name { ... } name;` in the header, in order."""
+    src = open(os.path.join(ROOT, "include", "orf_fdtd.h")).read()
+    body = re.search(r"typedef struct %s \{(.*?)\} %s;" % (name, name), src, re.S).group(1)
+    body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
+    names = []
+    for decl in body.split(";"):
+        decl = decl.strip()
+        if not decl:
+            continue
+        # "type a, b[3], *c" -> a, b, c
+        for part in re.split(r",", decl):
+            m = re.search(r"\**\s*(\w+)\s*(\[[^\]]*\])*\s*$", part.strip())
+            names.append(m.group(1))
+    return names
+
+
+@pytest.mark.parametrize("cname,pyname", [
+    ("orf_sim2d", "OrfSim2D"), ("orf_out2d", "OrfOut2D"), ("orf_sim3d", "OrfSim3D"), ("orf_out3d", "OrfOut3D"),
+    ("orf_tuning", "OrfTuning"), ("orf_kernel_stats", "OrfKernelStats"), ("orf_serve_cfg", "OrfServeCfg"),
+    ("orf_serve_job_info", "OrfServeJobInfo"),
+])
+def test_ctypes_mirrors_match_header_structs(cname, pyname):
+    fields = [f[0] for f in getattr(_abi, pyname)._fields_]
+    assert fields == _header_struct_fields(cname)
