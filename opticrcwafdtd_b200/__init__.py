@@ -10,7 +10,7 @@ a GPU is missing.
 """
 from ._abi import NotConvergedWarning, OrfError  # noqa: F401
 from .geometry import epsCellMean, epsComponents2D, epsComponents3D, epsFromBoxes  # noqa: F401
-from .modes import slabModes  # noqa: F401
+from .modes import slabModes, wgModes2D  # noqa: F401
 from .coupler import (apodizedGrating, bestFiberCoupling, fiberCoupling, gratingCouplerTE,  # noqa: F401
                       gratingCouplerTE_batch)
 

@@ -65,3 +65,129 @@ def slabModes(z, n, lambda0: float, pol: str = "TE", nModes: int = 1, EpsHalf=No
     if np.all(np.abs(neff.imag) == 0):
         neff = neff.real
     return {"neff": neff, "field": V}
+
+
+# ------------------------------------------------------------ full vector --
+def _fwd(n: int, h: float, periodic: bool):
+    """Forward difference (f[i+1] - f[i]) / h on n points: zero past the last
+    point, or wrapping when periodic."""
+    from scipy import sparse
+    U = sparse.diags([-np.ones(n), np.ones(n - 1)], [0, 1], shape=(n, n), format="lil")
+    if periodic:
+        U[n - 1, 0] = 1.0
+    return (U.tocsr() / h)
+
+
+def _wrap_eps(xc, yc, dx, dy, boxes, nBg, hdir, NSub, Lx, x0):
+    """epsCellMean with the x samples folded into [x0, x0+Lx): the boxes
+    repeat with period Lx along x (geometry.epsCellMean folds its second
+    coordinate, so x and y swap roles)."""
+    from .geometry import _as_boxes, epsCellMean
+    b = _as_boxes(boxes)
+    bs = b[:, [2, 3, 0, 1, 4]]
+    sdir = {"x": "y", "y": "x"}.get(hdir, hdir)
+    return epsCellMean(yc, xc, dy, dx, bs, nBg, sdir, NSub, WrapY=(x0, Lx)).T
+
+
+def wgModes2D(x, y, nBg: float, boxes, lambda0: float, nModes: int = 1, NGuess=None,
+              PeriodicX: bool = False, NSub: int = 4, Eps=None) -> dict:
+    """modes = wgModes2D(x, y, nBg, boxes, lambda0, nModes, ...): full-vector
+    modes of a waveguide cross-section on the Yee grid, propagating as
+    exp(i(beta z - w t)) (the documented method of toolbox/+orf/wgModes2D.m,
+    whose implementation is closed).
+
+    x, y: uniform cell centres [um] = the E_z points; E_x, h_y at (i+1/2, j);
+    E_y, h_x at (i, j+1/2); h_z at (i+1/2, j+1/2); h = eta0 H.  Eliminating
+    E_z and h_z from the curl equations leaves, with U the forward
+    differences (zero past the last point; wrapping in x when PeriodicX) and
+    V = -U^T,
+        beta E_t = P h_t,   beta h_t = Q E_t,   beta^2 E_t = P Q E_t,
+        P = (1/k0)[-Ux ez^-1 Vy,  Ux ez^-1 Vx; -Uy ez^-1 Vy,  Uy ez^-1 Vx] + k0[0 I; -I 0]
+        Q = (1/k0)[ Vx Uy, -Vx Ux; Vy Uy, -Vy Ux] + k0[0 -ey; ex 0],
+    and E_z = i/(k0 ez) (Vx h_y - Vy h_x), h_z = -i/k0 (Ux E_y - Uy E_x).
+    eps_x / eps_y are harmonic means along x / y, eps_z the arithmetic mean
+    of NSub x NSub samples of the boxes [x1 x2 y1 y2 n] (epsCellMean), unless
+    Eps = {"x", "y", "z"} (numel(x) x numel(y) each, e.g. a plane of an FDTD
+    grid) gives them.  The nModes eigenvalues of P Q nearest (k0 NGuess)^2
+    (default: the largest index present) come from a sparse shift-invert
+    solve.
+
+    Returns {"neff" (descending), "Ex", "Ey", "Ez", "Hx", "Hy", "Hz"
+    (numel(x) x numel(y) x nModes, complex, scaled so max |E_t| = 1 with that
+    entry real and positive), "teFraction" (sum |Ex|^2 / sum |E_t|^2),
+    "grid" (coordinates of each component), "eps"}.
+    """
+    from scipy import sparse
+    from scipy.sparse.linalg import eigs
+
+    x = np.asarray(x, dtype=float).ravel()
+    y = np.asarray(y, dtype=float).ravel()
+    nx, ny = x.size, y.size
+    if nx < 2 or ny < 2:
+        raise ValueError("wgModes2D:grid: x and y need at least two points.")
+    dx, dy = x[1] - x[0], y[1] - y[0]
+    k0 = 2 * np.pi / lambda0
+    if Eps is not None:
+        get = (lambda k: Eps[k]) if isinstance(Eps, dict) else (lambda k: getattr(Eps, k))
+        ex, ey, ez = (np.asarray(get(k), dtype=float) for k in ("x", "y", "z"))
+        for e in (ex, ey, ez):
+            if e.shape != (nx, ny):
+                raise ValueError("wgModes2D:eps: Eps.x, .y, .z must be numel(x) x numel(y).")
+    elif PeriodicX:
+        x0, Lx = x[0] - dx / 2, nx * dx
+        ex = _wrap_eps(x + dx / 2, y, dx, dy, boxes, nBg, "x", NSub, Lx, x0)
+        ey = _wrap_eps(x, y + dy / 2, dx, dy, boxes, nBg, "y", NSub, Lx, x0)
+        ez = _wrap_eps(x, y, dx, dy, boxes, nBg, "none", NSub, Lx, x0)
+    else:
+        from .geometry import epsCellMean
+        ex = epsCellMean(x + dx / 2, y, dx, dy, boxes, nBg, "x", NSub)
+        ey = epsCellMean(x, y + dy / 2, dx, dy, boxes, nBg, "y", NSub)
+        ez = epsCellMean(x, y, dx, dy, boxes, nBg, "none", NSub)
+    N = nx * ny
+    nModes = int(nModes)
+    if not 1 <= nModes < 2 * N - 1:
+        raise ValueError("wgModes2D:nModes: 1 <= nModes < 2 numel(x) numel(y) - 1.")
+
+    # unknowns ordered like a column-major numel(x) x numel(y) array: x fastest
+    vec = lambda a: np.asarray(a).ravel(order="F")
+    Ix, Iy = sparse.identity(nx, format="csr"), sparse.identity(ny, format="csr")
+    Ux = sparse.kron(Iy, _fwd(nx, dx, PeriodicX), format="csr")
+    Uy = sparse.kron(_fwd(ny, dy, False), Ix, format="csr")
+    Vx, Vy = (-Ux.T).tocsr(), (-Uy.T).tocsr()
+    iez = sparse.diags(1.0 / vec(ez))
+    I = sparse.identity(N, format="csr")
+    P = sparse.bmat([[-Ux @ iez @ Vy, Ux @ iez @ Vx], [-Uy @ iez @ Vy, Uy @ iez @ Vx]]) / k0 \
+        + k0 * sparse.bmat([[None, I], [-I, None]])
+    Q = sparse.bmat([[Vx @ Uy, -Vx @ Ux], [Vy @ Uy, -Vy @ Ux]]) / k0 \
+        + k0 * sparse.bmat([[None, -sparse.diags(vec(ey))], [sparse.diags(vec(ex)), None]])
+    P, Q = P.tocsr(), Q.tocsr()
+    A = (P @ Q).tocsc()
+    ng = float(NGuess) if NGuess is not None else float(np.sqrt(max(ex.max(), ey.max(), ez.max())))
+    vals, vecs = eigs(A, k=nModes, sigma=(k0 * ng) ** 2, which="LM")
+    beta = np.sqrt(vals.astype(complex))
+    neff = beta / k0
+    order = np.argsort(-neff.real, kind="stable")
+    neff, beta, vecs = neff[order], beta[order], vecs[:, order]
+
+    shp = (nx, ny, nModes)
+    F = {k: np.zeros(shp, dtype=complex) for k in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")}
+    te = np.zeros(nModes)
+    for m in range(nModes):
+        Et = vecs[:, m]
+        s = Et[int(np.argmax(np.abs(Et)))]
+        Et = Et / s
+        ht = (Q @ Et) / beta[m]
+        Exv, Eyv, hxv, hyv = Et[:N], Et[N:], ht[:N], ht[N:]
+        Ezv = 1j / (k0 * vec(ez)) * (Vx @ hyv - Vy @ hxv)
+        hzv = -1j / k0 * (Ux @ Eyv - Uy @ Exv)
+        for k, v in (("Ex", Exv), ("Ey", Eyv), ("Ez", Ezv), ("Hx", hxv), ("Hy", hyv), ("Hz", hzv)):
+            F[k][:, :, m] = v.reshape((nx, ny), order="F")
+        px, py = np.sum(np.abs(Exv) ** 2), np.sum(np.abs(Eyv) ** 2)
+        te[m] = px / (px + py)
+    if np.all(np.abs(neff.imag) <= 1e-12 * np.abs(neff.real)):
+        neff = neff.real
+    xh, yh = x + dx / 2, y + dy / 2
+    grid = {"Ex": (xh, y), "Ey": (x, yh), "Ez": (x, y), "Hx": (x, yh), "Hy": (xh, y), "Hz": (xh, yh)}
+    out = {"neff": neff, "teFraction": te, "grid": grid, "eps": {"x": ex, "y": ey, "z": ez}}
+    out.update(F)
+    return out
