@@ -138,3 +138,50 @@ def plane_wave_3d(x, y, z, d, lam, lambda0, bw, zSrc, zR, zT):
                Hb=np.ones((Na, Nb)), neff=1, lambda0=lambda0, bw=bw)
     return dict(x=x, y=y, z=z, npml=[0, 0, round(0.3 / d)], periodic=[True, True, False], source=src,
                 lambdas=lam, monitors=[dict(axis=3, index=izOf(zR)), dict(axis=3, index=izOf(zT))])
+
+
+def strip3d_sim(precision="double"):
+    """tests/TestFDTD3D.m:36-58 (stripRun): a 500 x 220 nm SOI strip along x
+    (d = 40 nm) fed by its TE0 mode, solved by wgModes2D on the 3D grid's own
+    (y, z) permittivity plane.  Returns (sim, prof, ms_eps)."""
+    from opticrcwafdtd_b200 import epsComponents3D, wgModes2D
+    d = 0.04
+    x = np.arange(0, 2.6 + 1e-9, d)
+    y = (np.arange(-30, 30) + 0.5) * d
+    z = (np.arange(-25, 25) + 0.5) * d
+    e = epsComponents3D(x, y, z, 1.444, [["box", [-np.inf, np.inf, -0.25, 0.25, -0.11, 0.11, 3.476]]])
+    # mode-solver plane (a, b) = (y, z): its E_x, E_y, E_z are the 3D E_y, E_z, E_x
+    ms_eps = {"x": e["y"][0], "y": e["z"][0], "z": e["x"][0]}
+    m = wgModes2D(y, z, 1.444, np.zeros((0, 5)), 1.55, 2, Eps=ms_eps)
+    ite = int(np.argmax(m["teFraction"]))
+    prof = {k: np.real(m[f][:, :, ite]) for k, f in (("Ea", "Ex"), ("Eb", "Ey"), ("Ha", "Hx"), ("Hb", "Hy"))}
+    ix = lambda xx: int(round(xx / d)) + 1
+    src = dict(axis=1, index=ix(0.6), neff=float(m["neff"][ite]), lambda0=1.55, bw=0.1, **prof)
+    sim = dict(x=x, y=y, z=z, eps=e, npml=[8, 8, 8], source=src, lambdas=[1.55],
+               monitors=[dict(axis=1, index=ix(0.4)), dict(axis=1, index=ix(0.9)), dict(axis=1, index=ix(2.0))],
+               precision=precision)
+    return sim, prof, ms_eps
+
+
+def check_strip3d(o, sim, prof, ms_eps):
+    """tests/TestFDTD3D.m:100-117: unidirectional (< 1e-4 back), lossless
+    guide (1e-3), and the phase advance between monitors 2 and 3 matching
+    the mode index at the numerical wavenumber through the exact Yee
+    dispersion along x (1e-4)."""
+    from opticrcwafdtd_b200 import wgModes2D
+    flux = o["flux"][:, 0]
+    assert -flux[0] / flux[1] < 1e-4
+    assert abs(flux[2] / flux[1] - 1.0) <= 1e-3
+    d = sim["x"][1] - sim["x"][0]
+    S = 0.99 / np.sqrt(3) * d
+    k0 = 2 * np.pi / 1.55
+    k0n = 2 / S * np.sin(k0 * S / 2)
+    mt = wgModes2D(sim["y"], sim["z"], 1.444, np.zeros((0, 5)), 2 * np.pi / k0n, 2, Eps=ms_eps)
+    it = int(np.argmax(mt["teFraction"]))
+    n_pred = 2 / d * np.arcsin(mt["neff"][it] * k0n * d / 2) / k0
+    ov = lambda q: (np.sum(prof["Ea"] * o["mon"][q]["Ea"][:, :, 0]) +
+                    np.sum(prof["Eb"] * o["mon"][q]["Eb"][:, :, 0]))
+    L = (sim["monitors"][2]["index"] - sim["monitors"][1]["index"]) * d
+    ph = np.angle(ov(2)) - np.angle(ov(1))
+    q = round((n_pred * k0 * L - ph) / (2 * np.pi))
+    assert abs((ph + 2 * np.pi * q) / (k0 * L) - n_pred) <= 1e-4

@@ -158,3 +158,11 @@ def test_3d_slab_matches_tmm_oracle():
     assert np.max(np.abs(R - tm["R"].ravel())) < 2e-3
     assert np.max(np.abs(R + T - 1)) < 2e-5
     assert np.max(np.abs(o0["flux"][0] / o0["flux"][1])) < 1e-8
+
+
+def test_3d_strip_mode_source_and_dispersion():
+    """The oracle fed by wgModes2D's TE0 mode of an SOI strip: unidirectional,
+    lossless, and the exact-Yee dispersion of the solved index
+    (tests/TestFDTD3D.m:100-117)."""
+    sim, prof, ms_eps = cases.strip3d_sim()
+    cases.check_strip3d(oracle.fdtd3D(sim), sim, prof, ms_eps)
