@@ -237,6 +237,20 @@ ORF_API int32_t orf_job3d_finish(orf_job* job, orf_out3d* out);
 ORF_API int32_t orf_job_get_fields(orf_job* job, double* const* fields, int32_t nfields);
 ORF_API int32_t orf_job_destroy(orf_job* job);
 
+/* Checkpoint / resume (no counterpart in the reference).  The state of a job
+ * between chunks -- current fields, CPML psi, DFT sums, step and chunk
+ * counters, energy peak -- as one self-describing host buffer of
+ * orf_job_checkpoint_size bytes.  orf_job_restore loads it into a job created
+ * from the same sim (maxTime may differ): advancing that job continues the
+ * run exactly, bitwise, whatever the tuning of its context.  A run stopped
+ * by cancellation or by its step budget resumes; one stopped by the energy
+ * shutoff stays finished.  Both calls synchronise the job's stream; restore
+ * fails with ORF_EINVAL on a buffer of another size, dimension, precision or
+ * grid. */
+ORF_API int32_t orf_job_checkpoint_size(orf_job* job, size_t* bytes);
+ORF_API int32_t orf_job_checkpoint(orf_job* job, void* buf, size_t bytes);
+ORF_API int32_t orf_job_restore(orf_job* job, const void* buf, size_t bytes);
+
 /* No counterpart in the reference.  orf.fdtd2D(sim) for callers that cannot
  * allocate device memory at call time (a host with its own device memory
  * pool, such as a MATLAB gpuArray session, a serving process with a fixed

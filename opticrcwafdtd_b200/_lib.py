@@ -42,6 +42,9 @@ _SIGS = {
     "orf_job3d_finish": (C.c_int32, [C.c_void_p, P(_abi.OrfOut3D)]),
     "orf_job_get_fields": (C.c_int32, [C.c_void_p, P(C.POINTER(C.c_double)), C.c_int32]),
     "orf_job_destroy": (C.c_int32, [C.c_void_p]),
+    "orf_job_checkpoint_size": (C.c_int32, [C.c_void_p, P(C.c_size_t)]),
+    "orf_job_checkpoint": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_size_t]),
+    "orf_job_restore": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_size_t]),
     "orf_out3d_sizes": (C.c_int32, [P(_abi.OrfSim3D), P(C.c_int32), P(C.c_int32)]),
     "orf_fdtd3d_run": (C.c_int32, [P(_abi.OrfSim3D), P(_abi.OrfOut3D), _abi.PROGRESS_FN, C.c_void_p]),
     "orf_fdtd3d_run_ctx": (C.c_int32, [C.c_void_p, P(_abi.OrfSim3D), P(_abi.OrfOut3D), _abi.PROGRESS_FN, C.c_void_p]),

@@ -568,6 +568,50 @@ int Job2D<R>::reset() {
 }
 
 template <class R>
+void Job2D<R>::state_regions(int b, std::vector<std::pair<void*, size_t>>& out) {
+    const size_t f = sizeof(R) * pitch * nz;
+    const size_t px = sizeof(R) * ((size_t)nz * 2 * h.npx + 1), pz = sizeof(R) * ((size_t)2 * h.npz * nx + 1);
+    out = {{h.P[b], f}, {h.A[b], f}, {h.B[b], f}, {h.psiB[b], px}, {h.psiPx[b], px}, {h.psiA[b], pz}, {h.psiPz[b], pz}};
+    size_t acc_elems = 0;
+    for (auto& q : host_streams) acc_elems += (size_t)q.len * nL;
+    out.push_back({d_acc, acc_elems * 16});
+}
+
+template <class R>
+uint64_t Job2D<R>::state_key() const {
+    uint64_t k = 1469598103934665603ull;   // FNV-1a over the grid and run options
+    auto mix = [&k](const void* p, size_t n) {
+        const unsigned char* c = static_cast<const unsigned char*>(p);
+        for (size_t q = 0; q < n; ++q) k = (k ^ c[q]) * 1099511628211ull;
+    };
+    const int v[] = {2, (int)sizeof(R), te, per, nx, nz, pitch, h.npx, h.npz, h.src_ix, nM, nMZ, nL};
+    mix(v, sizeof v);
+    mix(h.mon, sizeof h.mon);
+    mix(h.monz, sizeof h.monz);
+    mix(&S, sizeof S);
+    mix(&dx, sizeof dx);
+    return k;
+}
+
+template <class R>
+void Job2D<R>::resume_host(const JobState& js) {
+    enq_steps = js.chunk * kChunk;
+    pl = ProgressLoop{};
+    pl.ring = ring_h;
+    pl.cancel = cancel_h;
+    pl.S = S;
+    pl.src_end = src_end;
+    pl.shutoff = shutoff;
+    pl.seen = js.chunk;
+    pl.last_step = js.step;
+    pl.done = js.done != 0;
+    if (ring_h) std::memset(ring_h, 0, sizeof(ChunkStatus) * kStatusRing);
+    if (cancel_h) *cancel_h = 0;
+    eng.par = js.cur;
+    eng.drop_graph();   // a graph captured before encodes the old buffer parity
+}
+
+template <class R>
 int Job2D<R>::advance(int64_t nsteps, orf_progress_fn progress, void* user) {
     int dev = 0;
     cudaGetDevice(&dev);

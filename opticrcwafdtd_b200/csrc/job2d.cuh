@@ -61,6 +61,11 @@ struct Job2D : orf_job {
     int finish2d(orf_out2d* o) override;
     // enqueue every remaining chunk with direct launches, then synchronize
     int advance_all_direct();
+    void state_regions(int b, std::vector<std::pair<void*, size_t>>& out) override;
+    uint64_t state_key() const override;
+    JobState* state_dev() const override { return d_st; }
+    int64_t nmax_steps() const override { return nmax; }
+    void resume_host(const JobState& js) override;
 };
 
 }  // namespace orf

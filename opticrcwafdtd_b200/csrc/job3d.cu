@@ -535,6 +535,56 @@ int Job3D<R>::reset() {
 }
 
 template <class R>
+void Job3D<R>::state_regions(int b, std::vector<std::pair<void*, size_t>>& out) {
+    out.clear();
+    for (int c = 0; c < 3; ++c) out.push_back({h.E[b][c], NP() * sizeof(R)});
+    for (int c = 0; c < 3; ++c) out.push_back({h.H[b][c], NP() * sizeof(R)});
+    for (int c = 0; c < 3; ++c)
+        for (int q = 0; q < 3; ++q) {
+            if (h.psiE[b][c][q]) out.push_back({h.psiE[b][c][q], N() / n[q] * h.nslabI[q] * sizeof(R)});
+            if (h.psiH[b][c][q]) out.push_back({h.psiH[b][c][q], N() / n[q] * h.nslabH[q] * sizeof(R)});
+        }
+    size_t acc_elems = 0;
+    for (auto& q : host_streams) acc_elems += (size_t)q.len * nL;
+    out.push_back({d_acc, acc_elems * 16});
+}
+
+template <class R>
+uint64_t Job3D<R>::state_key() const {
+    uint64_t k = 1469598103934665603ull;   // FNV-1a over the grid and run options
+    auto mix = [&k](const void* p, size_t m) {
+        const unsigned char* c = static_cast<const unsigned char*>(p);
+        for (size_t q = 0; q < m; ++q) k = (k ^ c[q]) * 1099511628211ull;
+    };
+    const int v[] = {3, (int)sizeof(R), n[0], n[1], n[2], pitch, per[0], per[1], per[2],
+                     h.np[0], h.np[1], h.np[2], h.sa, h.ss, nM, nL};
+    mix(v, sizeof v);
+    mix(h.mon_axis, sizeof h.mon_axis);
+    mix(h.mon_index, sizeof h.mon_index);
+    mix(&S, sizeof S);
+    mix(&d, sizeof d);
+    return k;
+}
+
+template <class R>
+void Job3D<R>::resume_host(const JobState& js) {
+    enq_steps = js.chunk * kChunk;
+    pl = ProgressLoop{};
+    pl.ring = ring_h;
+    pl.cancel = cancel_h;
+    pl.S = S;
+    pl.src_end = src_end;
+    pl.shutoff = shutoff;
+    pl.seen = js.chunk;
+    pl.last_step = js.step;
+    pl.done = js.done != 0;
+    if (ring_h) std::memset(ring_h, 0, sizeof(ChunkStatus) * kStatusRing);
+    if (cancel_h) *cancel_h = 0;
+    eng.par = js.cur;
+    eng.drop_graph();   // a graph captured before encodes the old buffer parity
+}
+
+template <class R>
 int Job3D<R>::advance(int64_t nsteps, orf_progress_fn progress, void* user) {
     int dev = 0;
     cudaGetDevice(&dev);

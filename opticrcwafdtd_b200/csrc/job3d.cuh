@@ -63,6 +63,11 @@ struct Job3D : orf_job {
     int reset() override;
     int get_fields(double* const* f, int nf) override;
     int finish3d(orf_out3d* o) override;
+    void state_regions(int b, std::vector<std::pair<void*, size_t>>& out) override;
+    uint64_t state_key() const override;
+    JobState* state_dev() const override { return d_st; }
+    int64_t nmax_steps() const override { return nmax; }
+    void resume_host(const JobState& js) override;
 };
 
 

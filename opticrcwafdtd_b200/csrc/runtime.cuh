@@ -191,6 +191,15 @@ struct orf_job {
     virtual int get_fields(double* const* f, int nf) = 0;
     virtual int finish2d(orf_out2d*) { return ORF_EINVAL; }
     virtual int finish3d(orf_out3d*) { return ORF_EINVAL; }
+    // checkpoint / resume (checkpoint.cu): the device regions of field
+    // buffer b holding the run's state (fields, CPML psi, then the DFT sums,
+    // which have one copy), a key of the grid and run options, the device
+    // state block, and the host bookkeeping after a restore
+    virtual void state_regions(int b, std::vector<std::pair<void*, size_t>>& out) = 0;
+    virtual uint64_t state_key() const = 0;
+    virtual orf::JobState* state_dev() const = 0;
+    virtual int64_t nmax_steps() const = 0;
+    virtual void resume_host(const orf::JobState& js) = 0;
 };
 
 namespace orf {

@@ -199,6 +199,21 @@ class Job:
         _lib.check(self.lib.orf_job_get_fields(self.handle, ptrs, len(arrs)), "get_fields")
         return arrs
 
+    def checkpoint(self) -> bytes:
+        """The run's state between chunks (fields, CPML psi, DFT sums, step
+        counters) as bytes (orf_job_checkpoint)."""
+        n = C.c_size_t(0)
+        _lib.check(self.lib.orf_job_checkpoint_size(self.handle, C.byref(n)), "checkpoint")
+        buf = C.create_string_buffer(n.value)
+        _lib.check(self.lib.orf_job_checkpoint(self.handle, buf, n.value), "checkpoint")
+        return buf.raw
+
+    def restore(self, state: bytes) -> None:
+        """Load a checkpoint of a run of the same sim (maxTime may differ);
+        advancing then continues that run exactly (orf_job_restore)."""
+        buf = C.create_string_buffer(bytes(state), len(state))
+        _lib.check(self.lib.orf_job_restore(self.handle, buf, len(state)), "restore")
+
     def finish(self) -> dict:
         if self.dims == 2:
             o, bufs = _abi.alloc_out2d(self.m)
