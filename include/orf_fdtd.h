@@ -300,6 +300,8 @@ typedef struct orf_serve_job_info {
     int32_t status;            /* the job's orf_status                        */
     int32_t dims;              /* 2 or 3                                       */
     int64_t device_bytes;      /* device memory the job held while resident    */
+    int32_t preemptions;       /* times orf_serve_preempt moved it off the GPU */
+    int32_t reserved;
 } orf_serve_job_info;
 
 ORF_API int32_t orf_serve_open(orf_ctx* ctx, const orf_serve_cfg* cfg, orf_server** srv);
@@ -317,6 +319,12 @@ ORF_API int32_t orf_serve_step(orf_server* srv);
 /* ORF_OK when the ticket is done (info filled), ORF_EBUSY otherwise. */
 ORF_API int32_t orf_serve_poll(orf_server* srv, int64_t ticket, orf_serve_job_info* info);
 ORF_API int32_t orf_serve_pending(orf_server* srv, int32_t* queued, int32_t* resident);
+/* Preemption: a resident job's state (as orf_job_checkpoint) moves to host
+ * memory, its device memory returns to the budget, and it joins the end of
+ * the queue; re-admitted, it continues where it stopped, and its result is
+ * bitwise that of the job run alone.  A queued or finished ticket is left
+ * as it is.  Call from the thread that calls orf_serve_step. */
+ORF_API int32_t orf_serve_preempt(orf_server* srv, int64_t ticket);
 ORF_API double  orf_serve_clock(orf_server* srv);
 ORF_API int32_t orf_serve_close(orf_server* srv);
 

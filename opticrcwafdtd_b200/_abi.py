@@ -112,7 +112,8 @@ class OrfServeCfg(C.Structure):
 class OrfServeJobInfo(C.Structure):
     _fields_ = [("t_submit", C.c_double), ("t_admit", C.c_double), ("t_done", C.c_double),
                 ("steps", C.c_int64), ("cells", C.c_int64), ("status", C.c_int32),
-                ("dims", C.c_int32), ("device_bytes", C.c_int64)]
+                ("dims", C.c_int32), ("device_bytes", C.c_int64), ("preemptions", C.c_int32),
+                ("reserved", C.c_int32)]
 
 
 class OrfError(RuntimeError):

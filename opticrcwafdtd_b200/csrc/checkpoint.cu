@@ -7,9 +7,10 @@
 // checkpoint is a header, those scalars, and the state regions of buffer
 // `cur` in the order the job lists them (Job2D / Job3D::state_regions).  A
 // restore writes the regions into buffer 0 of a job created from the same
-// sim, sets cur = 0 and the counters, and re-arms the host's progress loop at
-// the restored chunk: the kernels' arithmetic does not depend on the buffer
-// parity or the tiling, so the continued run is bitwise the uninterrupted one.
+// sim (the server: the buffer its group launches from next), sets cur and the
+// counters, and re-arms the host's progress loop at the restored chunk: the
+// kernels' arithmetic does not depend on the buffer parity or the tiling, so
+// the continued run is bitwise the uninterrupted one.
 #include "engine.cuh"
 
 namespace orf {
@@ -91,7 +92,7 @@ int job_checkpoint(orf_job* job, void* buf, size_t bytes) {
     return ORF_OK;
 }
 
-int job_restore(orf_job* job, const void* buf, size_t bytes) {
+int job_restore(orf_job* job, const void* buf, size_t bytes, int into) {
     CkptHeader hd{};
     if (bytes < sizeof hd) {
         set_error("not a checkpoint: %zu bytes", bytes);
@@ -99,7 +100,7 @@ int job_restore(orf_job* job, const void* buf, size_t bytes) {
     }
     std::memcpy(&hd, buf, sizeof hd);
     std::vector<std::pair<void*, size_t>> regs;
-    job->state_regions(0, regs);
+    job->state_regions(into, regs);
     if (std::memcmp(hd.magic, kMagic, sizeof kMagic) != 0) {
         set_error("not a checkpoint of this library");
         return ORF_EINVAL;
@@ -132,7 +133,7 @@ int job_restore(orf_job* job, const void* buf, size_t bytes) {
     // the energy shutoff ends a run for good; a cancelled run, or one that
     // used up a smaller step budget, continues
     js.done = (hd.converged || hd.step >= job->nmax_steps()) ? 1 : 0;
-    js.cur = 0;
+    js.cur = into;
     js.fault = 0;
     js.energy = hd.energy;
     js.peak = hd.peak;
@@ -158,7 +159,7 @@ int32_t orf_job_checkpoint(orf_job* job, void* buf, size_t bytes) {
 
 int32_t orf_job_restore(orf_job* job, const void* buf, size_t bytes) {
     if (!job || !buf) return ORF_EINVAL;
-    return orf::job_restore(job, buf, bytes);
+    return orf::job_restore(job, buf, bytes, 0);
 }
 
 }  // extern "C"

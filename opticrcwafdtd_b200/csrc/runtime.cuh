@@ -203,6 +203,10 @@ struct orf_job {
 };
 
 namespace orf {
+// checkpoint / resume (checkpoint.cu); restore writes into field buffer `into`
+int job_checkpoint_size(orf_job* job, size_t* bytes);
+int job_checkpoint(orf_job* job, void* buf, size_t bytes);
+int job_restore(orf_job* job, const void* buf, size_t bytes, int into);
 int make_job2d(orf_ctx* ctx, const orf_sim2d* sim, orf_job** out);
 int make_job3d(orf_ctx* ctx, const orf_sim3d* sim, orf_job** out);
 int batch2d_run(orf_ctx* ctx, int n, const orf_sim2d* sims, orf_out2d* outs, orf_progress_fn progress,

@@ -52,6 +52,7 @@ struct SrvJob {
     ProgressLoop* pl = nullptr;   // the job's status-ring reader
     Group* group = nullptr;
     size_t need = 0;    // device arena bytes, known after the first admission attempt
+    std::vector<unsigned char> snapshot;   // checkpoint of a preempted job, restored at re-admission
     orf_serve_job_info info{};
 
     void copy2d(const orf_sim2d* s, orf_out2d* o) {
@@ -173,6 +174,7 @@ struct orf_server {
             g = groups.back().g.get();
         }
         static_cast<Group2D<R>*>(g)->add(j.get());
+        ORF_TRY(resume(J, j.get(), g));
         J->group = g;
         J->pl = &j->pl;
         J->job = std::move(j);
@@ -196,10 +198,59 @@ struct orf_server {
             g = groups.back().g.get();
         }
         static_cast<Group3D<R>*>(g)->add(j.get());
+        ORF_TRY(resume(J, j.get(), g));
         J->group = g;
         J->pl = &j->pl;
         J->job = std::move(j);
         return ORF_OK;
+    }
+
+    // a preempted job continues from its checkpoint, restored into the field
+    // buffer its group launches from next (the group's members share one
+    // buffer parity)
+    int resume(SrvJob* J, orf_job* j, Group* g) {
+        if (J->snapshot.empty()) return ORF_OK;
+        const int st = job_restore(j, J->snapshot.data(), J->snapshot.size(), g->eng.par);
+        if (st != ORF_OK) {
+            g->remove(j);
+            return st;
+        }
+        std::vector<unsigned char>().swap(J->snapshot);
+        return ORF_OK;
+    }
+
+    // move a resident job's state to host memory and queue it again (at the
+    // end); called between scheduling rounds, when no group work is in flight
+    int preempt(int64_t ticket) {
+        for (size_t q = 0; q < resident.size(); ++q) {
+            if (resident[q]->ticket != ticket) continue;
+            SrvJob* J = resident[q].get();
+            orf_job* j = J->job.get();
+            J->pl->poll(nullptr, nullptr);
+            if (J->pl->done) return ORF_OK;   // finished: it retires at the next round
+            size_t n = 0;
+            ORF_TRY(job_checkpoint_size(j, &n));
+            std::vector<unsigned char> snap(n);
+            ORF_TRY(job_checkpoint(j, snap.data(), n));
+            J->group->remove(j);
+            J->group = nullptr;
+            J->pl = nullptr;
+            J->job.reset();
+            used -= std::min(used, J->need);
+            J->snapshot = std::move(snap);
+            J->info.preemptions += 1;
+            std::unique_ptr<SrvJob> P = std::move(resident[q]);
+            resident.erase(resident.begin() + q);
+            std::lock_guard<std::mutex> lk(mu);
+            queue.push_back(std::move(P));
+            return ORF_OK;
+        }
+        std::lock_guard<std::mutex> lk(mu);
+        if (ticket < 1 || ticket >= next) {
+            set_error("unknown ticket %lld", (long long)ticket);
+            return ORF_EINVAL;
+        }
+        return ORF_OK;   // queued or finished: nothing to move
     }
 
     void fail(std::unique_ptr<SrvJob> J, int status) {
@@ -232,7 +283,7 @@ struct orf_server {
                 st = J->precision() == ORF_SINGLE ? admit3d<float>(J.get(), left, &fits)
                                                   : admit3d<double>(J.get(), left, &fits);
             if (st == ORF_OK) {
-                J->info.t_admit = clock();
+                if (J->info.preemptions == 0) J->info.t_admit = clock();   // the first admission
                 J->info.device_bytes = (int64_t)J->need;
                 used += J->need;
                 resident.push_back(std::move(J));
@@ -405,6 +456,17 @@ int32_t orf_serve_poll(orf_server* srv, int64_t ticket, orf_serve_job_info* info
         return ORF_EINVAL;
     }
     return ORF_EBUSY;
+}
+
+int32_t orf_serve_preempt(orf_server* srv, int64_t ticket) {
+    if (!srv) {
+        set_error("srv is NULL");
+        return ORF_EINVAL;
+    }
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev != srv->ctx->device) ORF_CUDA(cudaSetDevice(srv->ctx->device));
+    return srv->preempt(ticket);
 }
 
 int32_t orf_serve_pending(orf_server* srv, int32_t* queued, int32_t* resident) {

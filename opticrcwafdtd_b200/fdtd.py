@@ -282,6 +282,11 @@ class Server:
     def clock(self) -> float:
         return float(self.lib.orf_serve_clock(self.handle))
 
+    def preempt(self, ticket: int) -> None:
+        """Move a resident job's state to host memory and queue it again at
+        the end; it continues where it stopped (orf_serve_preempt)."""
+        _lib.check(self.lib.orf_serve_preempt(self.handle, int(ticket)), "serve preempt")
+
     def info(self, ticket: int) -> dict | None:
         """Timing record of a finished ticket, None while it is queued or resident."""
         i = _abi.OrfServeJobInfo()

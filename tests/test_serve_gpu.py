@@ -117,3 +117,62 @@ def test_poll_unknown_ticket_and_busy():
     srv.drain()
     assert srv.info(t)["status"] == 0
     srv.close()
+
+
+@pytest.mark.parametrize("precision", ["single", "double"])
+def test_preempted_jobs_equal_alone_runs(precision):
+    """Jobs preempted mid-run (their state parked in host memory, their
+    device memory freed) and re-admitted later -- into groups at either
+    buffer parity -- finish bitwise as when run alone."""
+    sims2, sims3 = _mix(precision)
+    alone2 = [orf.fdtd2D(s) for s in sims2]
+    alone3 = [orf.fdtd3D(s) for s in sims3]
+    srv = orf.Server(macro_steps=100)
+    t2 = [srv.submit(s) for s in sims2]
+    t3 = [srv.submit(s, dims=3) for s in sims3]
+    srv.step()
+    srv.preempt(t2[0])
+    srv.preempt(t3[1])
+    srv.step()
+    srv.preempt(t2[3])
+    srv.preempt(t2[0])          # re-admitted above, preempted again
+    srv.step()
+    srv.drain()
+    for t, a in zip(t2, alone2):
+        _bitwise2d(srv.result(t), a)
+    for t, a in zip(t3, alone3):
+        _bitwise3d(srv.result(t), a)
+    pre = {t: srv.info(t)["preemptions"] for t in t2 + t3}
+    assert pre[t2[0]] == 2 and pre[t2[3]] == 1 and pre[t3[1]] == 1
+    assert sum(pre.values()) == 4
+    srv.close()
+
+
+def test_preemption_frees_memory_for_the_queue():
+    """With room for one job, preempting the resident one lets the queued
+    job run first; the preempted one resumes afterwards, both exact."""
+    sims2, _ = _mix("single")
+    a, b = sims2[0], sims2[3]
+    alone_a, alone_b = orf.fdtd2D(a), orf.fdtd2D(b)
+    probe = orf.Server()
+    pa, pb = probe.submit(a), probe.submit(b)
+    probe.drain()
+    na, nb = probe.info(pa)["device_bytes"], probe.info(pb)["device_bytes"]
+    probe.close()
+    srv = orf.Server(max_device_bytes=max(na, nb) + min(na, nb) // 2, max_jobs=8, macro_steps=50)
+    ta, tb = srv.submit(a), srv.submit(b)
+    srv.step()
+    assert srv.pending() == (1, 1)          # a resident, b waiting for memory
+    srv.preempt(ta)
+    assert srv.pending() == (2, 0)
+    srv.step()
+    assert srv.pending() == (1, 1)          # b resident now, a waits
+    srv.drain()
+    ia, ib = srv.info(ta), srv.info(tb)
+    assert ia["preemptions"] == 1 and ib["preemptions"] == 0
+    assert ia["t_done"] >= ib["t_admit"]
+    _bitwise2d(srv.result(ta), alone_a)
+    _bitwise2d(srv.result(tb), alone_b)
+    with pytest.raises(orf.OrfError):
+        srv.preempt(10 ** 6)
+    srv.close()
