@@ -328,6 +328,35 @@ ORF_API int32_t orf_serve_preempt(orf_server* srv, int64_t ticket);
 ORF_API double  orf_serve_clock(orf_server* srv);
 ORF_API int32_t orf_serve_close(orf_server* srv);
 
+/* Subpixel-averaged permittivity of a 3D grid on the GPU (the device form
+ * of epsComponents3D, toolbox/+orf/epsComponents3D.m:1-27, Method
+ * "directional"): for each Yee E component, cells whose centre an interface
+ * passes near are sampled at nsub^3 points and take the harmonic mean along
+ * the component's axis, then the arithmetic mean over the other two; shapes
+ * paint in order over the background nbg.  x, y, z are the cell centres
+ * (uniform, one spacing); period = {Lx, Ly} folds x and y into [-L/2, L/2)
+ * (NULL: no folding).  ex, ey, ez receive nx*ny*nz doubles each, column-major
+ * (x fastest), at (x+d/2, y, z), (x, y+d/2, z), (x, y, z+d/2).  The values
+ * are bitwise those of the package's host generator. */
+enum {
+    ORF_SHAPE_BOX = 0,      /* lo / hi: the box                                        */
+    ORF_SHAPE_CONE = 1,     /* p: cx cy r1 r2 z1 z2 (a cylinder when r1 = r2)          */
+    ORF_SHAPE_POLYGON = 2,  /* p: z1 z2; data: n0 vertices x0 y0 x1 y1 ...             */
+    ORF_SHAPE_LATTICE = 3   /* p: x0 y0 period z1 z2 dRdz; data: radii R[n0][n1], row-major */
+};
+typedef struct orf_eps_shape {
+    int32_t kind;
+    int32_t n0, n1;
+    int32_t reserved;
+    double n;               /* refractive index                                        */
+    double lo[3], hi[3];    /* bounding box (the band test's "near" region, minus h)   */
+    double p[8];
+    const double* data;
+} orf_eps_shape;
+ORF_API int32_t orf_eps3d(orf_ctx* ctx, const double* x, const double* y, const double* z, int32_t nx,
+                          int32_t ny, int32_t nz, double nbg, int32_t nsub, const double* period,
+                          int32_t nshape, const orf_eps_shape* shapes, double* ex, double* ey, double* ez);
+
 #ifdef __cplusplus
 }
 #endif

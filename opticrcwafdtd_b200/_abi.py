@@ -104,6 +104,12 @@ class OrfKernelStats(C.Structure):
                 ("setup_ms", C.c_double), ("loop_ms", C.c_double), ("finish_ms", C.c_double)]
 
 
+class OrfEpsShape(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("n0", C.c_int32), ("n1", C.c_int32), ("reserved", C.c_int32),
+                ("n", C.c_double), ("lo", C.c_double * 3), ("hi", C.c_double * 3), ("p", C.c_double * 8),
+                ("data", c_double_p)]
+
+
 class OrfServeCfg(C.Structure):
     _fields_ = [("max_device_bytes", C.c_int64), ("max_jobs", C.c_int32),
                 ("macro_steps", C.c_int32)]

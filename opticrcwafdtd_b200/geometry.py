@@ -285,7 +285,8 @@ class _Shape:
                 ex, ey = xs[b] - xs[a], ys[b] - ys[a]
                 L2 = max(ex * ex + ey * ey, 1e-300)
                 t = np.clip(((X - xs[a]) * ex + (Y - ys[a]) * ey) / L2, 0, 1)
-                dmin = np.minimum(dmin, np.hypot(X - xs[a] - t * ex, Y - ys[a] - t * ey))
+                u, v = X - xs[a] - t * ex, Y - ys[a] - t * ey
+                dmin = np.minimum(dmin, np.sqrt(u * u + v * v))
             return near & (zface | (dmin <= hd))
         raise AssertionError
 
@@ -297,16 +298,21 @@ def _fold(v, L):
 
 
 def epsComponents3D(x, y, z, nBg: float, shapes, NSub: int = 4, Period=None,
-                    Method: str = "directional") -> dict:
+                    Method: str = "directional", device=None) -> dict:
     """eps at the 3D Yee E locations (epsComponents3D.m:1-27).
 
     e["x"] at (x+d/2, y, z), e["y"] at (x, y+d/2, z), e["z"] at (x, y, z+d/2),
-    each numel(x) x numel(y) x numel(z).  Shapes paint in order (box, cyl,
+    each numel(x) x numel(y) x numel(z), column-major (MATLAB's layout, which
+    the engine takes without a copy).  Shapes paint in order (box, cyl,
     cone, polygon, lattice).  "directional": harmonic mean along the
     component's own axis, arithmetic over the other two; "kottke":
     1/eps_cc = n_c^2 <1/eps> + (1 - n_c^2)/<eps> with n from the first moment
     of eps.  Only cells an interface crosses are sub-sampled; Period = [Lx Ly]
     folds x, y into [-L/2, L/2).
+
+    device: a Context (or True for the current device's default context)
+    computes the "directional" form on the GPU (orf_eps3d), bitwise the same
+    values, in milliseconds per component instead of seconds.
     """
     x = np.asarray(x, dtype=float).ravel()
     y = np.asarray(y, dtype=float).ravel()
@@ -317,6 +323,10 @@ def epsComponents3D(x, y, z, nBg: float, shapes, NSub: int = 4, Period=None,
     Lx = Ly = None
     if Period is not None:
         Lx, Ly = (float(Period[0]), float(Period[1]))
+    if device is not None and device is not False:
+        if Method != "directional":
+            raise ValueError('the GPU generator computes Method "directional" only')
+        return _eps3d_device(x, y, z, nBg, sh, NSub, Period, device)
     off = _offsets(NSub)
     out = {}
     for c, name in enumerate(("x", "y", "z")):
@@ -330,7 +340,55 @@ def epsComponents3D(x, y, z, nBg: float, shapes, NSub: int = 4, Period=None,
         # one representative of each such class, and every other plane alone
         rep, inv = _z_classes(Zall, sh, h)
         e = _component(c, X, Y, Zall[rep][None, None, :], sh, nBg, h, d, off, NSub, Lx, Ly, Method)
-        out[name] = np.ascontiguousarray(e[:, :, inv]) if rep.size < Zall.size else e
+        if rep.size < Zall.size:
+            # column-major (the layout the engine takes without a copy): each
+            # plane is one contiguous block, copied from its representative
+            full = np.empty(e.shape[:2] + (Zall.size,), order="F")
+            for k in range(Zall.size):
+                full[:, :, k] = e[:, :, inv[k]]
+            e = full
+        out[name] = e
+    return out
+
+
+def _eps3d_device(x, y, z, nBg, sh, NSub, Period, device) -> dict:
+    """epsComponents3D on the GPU through orf_eps3d (csrc/eps3d.cu)."""
+    import ctypes as C
+    from . import _abi, _lib
+    lib = _lib.load()
+    kinds = {"box": 0, "cyl": 1, "cone": 1, "polygon": 2, "lattice": 3}
+    arr = (_abi.OrfEpsShape * max(1, len(sh)))()
+    keep = []
+    for q, s in enumerate(sh):
+        o = arr[q]
+        o.kind = kinds[s.kind]
+        o.n = float(s.n)
+        for t in range(3):
+            o.lo[t], o.hi[t] = float(s.lo[t]), float(s.hi[t])
+        p = []
+        if s.kind in ("cyl", "cone"):
+            p = [s.c[0], s.c[1], s.r1, s.r2, s.z1, s.z2]
+        elif s.kind == "polygon":
+            p = [s.z1, s.z2]
+            tab = np.ascontiguousarray(s.xy, dtype=float)
+            o.n0 = tab.shape[0]
+        elif s.kind == "lattice":
+            p = [s.x0, s.y0, s.P, s.z1, s.z2, s.dRdz]
+            tab = np.ascontiguousarray(s.R, dtype=float)
+            o.n0, o.n1 = tab.shape
+        for t, v in enumerate(p):
+            o.p[t] = float(v)
+        if s.kind in ("polygon", "lattice"):
+            keep.append(tab)
+            o.data = _abi._ptr(tab)
+    shape = (x.size, y.size, z.size)
+    out = {k: np.empty(shape, order="F") for k in ("x", "y", "z")}
+    per = None if Period is None else np.array([float(Period[0]), float(Period[1])])
+    ctx = getattr(device, "handle", None)
+    st = lib.orf_eps3d(ctx, _abi._ptr(x), _abi._ptr(y), _abi._ptr(z), x.size, y.size, z.size, float(nBg),
+                       int(NSub), _abi._ptr(per), len(sh), C.cast(arr, C.c_void_p),
+                       _abi._ptr(out["x"]), _abi._ptr(out["y"]), _abi._ptr(out["z"]))
+    _lib.check(st, "epsComponents3D")
     return out
 
 
@@ -350,7 +408,11 @@ def _z_classes(Z: np.ndarray, sh: list, h: float):
         face = np.zeros(n, dtype=bool)
         keys = np.zeros((n, 0), dtype=bool)
     else:
-        face = (np.abs(Z[:, None] - zb[None, :]) <= h).any(axis=1)
+        # planes within 2h of a z boundary are computed one by one: farther
+        # out, every band, inside and sub-sample test of a plane depends only
+        # on which side of each boundary it lies (its key), with no rounding
+        # at a threshold, so the planes of one class carry the same map
+        face = (np.abs(Z[:, None] - zb[None, :]) <= 2 * h).any(axis=1)
         keys = Z[:, None] >= zb[None, :]
     rep, inv, seen = [], np.empty(n, dtype=np.int64), {}
     for k in range(n):
@@ -369,9 +431,9 @@ def _component(c, X, Y, Z, sh, nBg, h, d, off, NSub, Lx, Ly, Method):
     """One eps component at cell centres X (nx,1,1), Y (1,ny,1), Z (1,1,nz)."""
     Xf, Yf = _fold(X, Lx), _fold(Y, Ly)
     shape3 = (X.shape[0], Y.shape[1], Z.shape[2])
-    # material at the cell centres
-    e = np.full(shape3, float(nBg) ** 2)
-    band = np.zeros(shape3, dtype=bool)
+    # material at the cell centres (column-major, as the engine takes it)
+    e = np.full(shape3, float(nBg) ** 2, order="F")
+    band = np.zeros(shape3, dtype=bool, order="F")
     for s in sh:
         e[np.broadcast_to(s.inside(Xf, Yf, Z), shape3)] = s.n ** 2
         band |= np.broadcast_to(s.band(Xf, Yf, Z, h), shape3)
@@ -397,8 +459,18 @@ def _component(c, X, Y, Z, sh, nBg, h, d, off, NSub, Lx, Ly, Method):
                 es[np.broadcast_to(s.inside(SXb, SYb, SZb), es.shape)] = s.n ** 2
             mq = q1 - q0
             if Method == "directional":
-                inv_along = (1.0 / es).mean(axis=1 + c)                 # harmonic along c
-                val[q0:q1] = (1.0 / inv_along).reshape(mq, -1).mean(axis=1)
+                # harmonic mean along c, then arithmetic over the other two
+                # axes, each sum sequential in index order (the GPU generator,
+                # csrc/eps3d.cu, adds in the same order: same bits)
+                inv = np.moveaxis(1.0 / es, 1 + c, 1)                   # (m, along, r1, r2)
+                acc = inv[:, 0]
+                for a in range(1, NSub):
+                    acc = acc + inv[:, a]
+                r = (1.0 / (acc / NSub)).reshape(mq, NSub * NSub)
+                tot = r[:, 0]
+                for q in range(1, NSub * NSub):
+                    tot = tot + r[:, q]
+                val[q0:q1] = tot / (NSub * NSub)
             elif Method == "kottke":
                 mean_e = es.reshape(mq, -1).mean(axis=1)
                 mean_inv = (1.0 / es).reshape(mq, -1).mean(axis=1)

@@ -91,7 +91,7 @@ def _header_struct_fields(name):
 @pytest.mark.parametrize("cname,pyname", [
     ("orf_sim2d", "OrfSim2D"), ("orf_out2d", "OrfOut2D"), ("orf_sim3d", "OrfSim3D"), ("orf_out3d", "OrfOut3D"),
     ("orf_tuning", "OrfTuning"), ("orf_kernel_stats", "OrfKernelStats"), ("orf_serve_cfg", "OrfServeCfg"),
-    ("orf_serve_job_info", "OrfServeJobInfo"),
+    ("orf_serve_job_info", "OrfServeJobInfo"), ("orf_eps_shape", "OrfEpsShape"),
 ])
 def test_ctypes_mirrors_match_header_structs(cname, pyname):
     fields = [f[0] for f in getattr(_abi, pyname)._fields_]

@@ -121,3 +121,24 @@ def test_eps_components_3d_band_covers_every_interface():
     for c, k in enumerate("xyz"):
         ref = _eps3d_every_cell_sampled(x, y, z, 1.0, shapes, c)
         np.testing.assert_allclose(e[k], ref, rtol=1e-13, atol=0)
+
+
+def test_3d_plane_classes_change_no_bit(monkeypatch):
+    """epsComponents3D computes one plane per class of z-extruded planes and
+    copies it; the copies must equal planes computed one by one, also where a
+    shape's top lies on a grid plane (the component shifted by h then sits a
+    rounding away from the band test's threshold)."""
+    from opticrcwafdtd_b200 import geometry
+    d = 0.02
+    x = (np.arange(40) + 0.5) * d
+    y = x.copy()
+    z = np.arange(120) * d
+    R = np.random.default_rng(3).uniform(0.06, 0.18, (2, 2))
+    shapes = [["box", [-np.inf, np.inf, -np.inf, np.inf, -np.inf, 0.9, 1.46]],
+              ["lattice", dict(x0=0.2, y0=0.2, period=0.4, R=R, z1=0.9, z2=1.5, n=2.4)],
+              ["cyl", [0.4, 0.4, 0.1, 1.71, 2.0, 3.0]]]
+    a = geometry.epsComponents3D(x, y, z, 1.0, shapes)
+    monkeypatch.setattr(geometry, "_z_classes", lambda Z, sh, h: (np.arange(Z.size), np.arange(Z.size)))
+    b = geometry.epsComponents3D(x, y, z, 1.0, shapes)
+    for k in "xyz":
+        assert np.array_equal(a[k], b[k]), k
