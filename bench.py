@@ -349,7 +349,8 @@ def bench_pillar3d(args, rank, world, local, dist):
     from opticrcwafdtd_b200 import Context, Job, workloads
     nsteps = args.time_steps if args.time_steps != 30000 else 6000
     nx3, ny3, nz3 = (int(v) for v in args.size3d.split(","))
-    sim = workloads.pillar_lattice_sim(nx=nx3, ny=ny3, nz=nz3, steps=nsteps, precision=args.precision)
+    sim = workloads.pillar_lattice_sim(nx=nx3, ny=ny3, nz=nz3, steps=nsteps, precision=args.precision,
+                                       device=True)   # permittivity by the GPU generator (orf_eps3d)
     cells = sim["x"].size * sim["y"].size * sim["z"].size
     stream = torch.cuda.current_stream()
     ctx = Context(local, stream=stream.cuda_stream)

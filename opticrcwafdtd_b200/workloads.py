@@ -168,7 +168,8 @@ def coupler_batch_sims(n: int = 256, seed: int = 4, steps: int = 10000, precisio
 
 
 def pillar_lattice_sim(nx: int = 600, ny: int = 600, nz: int = 300, d: float = 0.02, seed: int = 3,
-                       steps: int = 6000, precision: str = "single", n_lambda: int = 1, npml_z: int = 20):
+                       steps: int = 6000, precision: str = "single", n_lambda: int = 1, npml_z: int = 20,
+                       device=None):
     """3D periodic TiO2 pillar array (n = 2.4, 600 nm tall, lattice 400 nm,
     radius U[60, 180] nm) on SiO2 (n = 1.46), periodic x/y, CPML in z, 532 nm
     x-polarised plane wave toward +z, 3 planar DFT monitors."""
@@ -182,7 +183,7 @@ def pillar_lattice_sim(nx: int = 600, ny: int = 600, nz: int = 300, d: float = 0
     zsub = 0.3 * nz * d
     shapes = [["box", [-np.inf, np.inf, -np.inf, np.inf, -np.inf, zsub, 1.46]],
               ["lattice", dict(x0=P / 2, y0=P / 2, period=P, R=R, z1=zsub, z2=zsub + 0.6, n=N_TIO2)]]
-    e = epsComponents3D(x, y, z, 1.0, shapes)
+    e = epsComponents3D(x, y, z, 1.0, shapes, device=device)   # device: the GPU generator, same bits
     iz_src = int(zsub / d) - 15
     S = 0.99 / math.sqrt(3) * d
     src = dict(axis=3, index=iz_src, Ea=1.0, Eb=0.0, Ha=0.0, Hb=1.46, neff=1.46, lambda0=0.532, bw=0.1)
