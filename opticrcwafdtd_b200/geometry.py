@@ -127,6 +127,7 @@ def epsComponents2D(x, z, nBg: float, boxes, NSub: int = 4, PeriodicZ: bool = Fa
            (numel(x) x numel(z)-1, or numel(z) when PeriodicZ);
     e["z"] at (x_i+1/2, z_k): harmonic along z, arithmetic along x
            ((numel(x)-1) x numel(z)).
+    Column-major arrays (MATLAB's layout): the engine takes them without a copy.
     """
     x = np.asarray(x, dtype=float).ravel()
     z = np.asarray(z, dtype=float).ravel()
@@ -135,9 +136,9 @@ def epsComponents2D(x, z, nBg: float, boxes, NSub: int = 4, PeriodicZ: bool = Fa
     zh = z + dz / 2 if PeriodicZ else z[:-1] + dz / 2
     xh = x[:-1] + dx / 2
     return {
-        "y": epsCellMean(x, z, dx, dz, boxes, nBg, "none", NSub, wrap),
-        "x": epsCellMean(x, zh, dx, dz, boxes, nBg, "x", NSub, wrap),
-        "z": epsCellMean(xh, z, dx, dz, boxes, nBg, "y", NSub, wrap),
+        "y": np.asfortranarray(epsCellMean(x, z, dx, dz, boxes, nBg, "none", NSub, wrap)),
+        "x": np.asfortranarray(epsCellMean(x, zh, dx, dz, boxes, nBg, "x", NSub, wrap)),
+        "z": np.asfortranarray(epsCellMean(xh, z, dx, dz, boxes, nBg, "y", NSub, wrap)),
     }
 
 
