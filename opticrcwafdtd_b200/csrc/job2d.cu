@@ -270,15 +270,19 @@ int Job2D<R>::create(const orf_sim2d* s) {
 
     // ---- upload
     std::vector<unsigned char> ib0(cellsP * isz), ib1(te ? 0 : cellsP * isz);
-    for (size_t q = 0; q < cellsP; ++q) {
+    // the device index: the 16-bit table index as is, or narrowed to bytes
+    // (plain loops, one per plane, so the compiler vectorises them)
+    auto narrow = [&](const std::vector<uint16_t>& src, std::vector<unsigned char>& dst) {
         if (idx16) {
-            std::memcpy(&ib0[2 * q], &ix0[q], 2);
-            if (!te) std::memcpy(&ib1[2 * q], &ix1[q], 2);
+            std::memcpy(dst.data(), src.data(), cellsP * 2);
         } else {
-            ib0[q] = (unsigned char)ix0[q];
-            if (!te) ib1[q] = (unsigned char)ix1[q];
+            unsigned char* d = dst.data();
+            const uint16_t* v = src.data();
+            for (size_t q = 0; q < cellsP; ++q) d[q] = (unsigned char)v[q];
         }
-    }
+    };
+    narrow(ix0, ib0);
+    if (!te) narrow(ix1, ib1);
     auto up = [&](void* d, const void* hsrc, size_t bytes) -> int {
         if (bytes == 0) return ORF_OK;
         ORF_CUDA(cudaMemcpyAsync(d, hsrc, bytes, cudaMemcpyHostToDevice, st));
