@@ -142,3 +142,23 @@ def test_3d_plane_classes_change_no_bit(monkeypatch):
     b = geometry.epsComponents3D(x, y, z, 1.0, shapes)
     for k in "xyz":
         assert np.array_equal(a[k], b[k]), k
+
+
+def test_3d_kottke_reduces_to_directional_on_planar_faces():
+    """Method "kottke" (epsComponents3D.m:19-24: 1/eps_cc = n_c^2 <1/eps> +
+    (1 - n_c^2)/<eps>, n from the first moment of eps): on the faces of a z
+    slab the normal is z, so eps_zz is the harmonic mean of the samples and
+    eps_xx, eps_yy the arithmetic one -- the directional form's values."""
+    from opticrcwafdtd_b200 import geometry
+    d = 0.02
+    x = (np.arange(6) + 0.5) * d
+    y = x.copy()
+    z = np.arange(40) * d
+    slab = [["box", [-np.inf, np.inf, -np.inf, np.inf, 0.213, 0.517, 2.2]]]
+    k = geometry.epsComponents3D(x, y, z, 1.3, slab, Method="kottke")
+    dr = geometry.epsComponents3D(x, y, z, 1.3, slab)
+    for c in "xyz":
+        assert np.allclose(k[c], dr[c], rtol=1e-12, atol=0), c
+    # the interface planes are sub-sampled: their values lie between the materials
+    mid = k["z"][0, 0, :]
+    assert np.any((mid > 1.3 ** 2 + 1e-9) & (mid < 2.2 ** 2 - 1e-9))
