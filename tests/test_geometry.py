@@ -162,3 +162,35 @@ def test_3d_kottke_reduces_to_directional_on_planar_faces():
     # the interface planes are sub-sampled: their values lie between the materials
     mid = k["z"][0, 0, :]
     assert np.any((mid > 1.3 ** 2 + 1e-9) & (mid < 2.2 ** 2 - 1e-9))
+
+
+def test_3d_shape_cross_sections():
+    """Each 3D shape covers its documented cross-section: on a plane inside
+    its z range the z component (harmonic along z over one material, then
+    arithmetic over the in-plane sub-samples) is the in-plane fill fraction,
+    whose sum is the area -- pi r^2 for a cylinder, the cone's radius at that
+    height, a triangle's area, sum pi R^2 for a lattice (missing site R = 0)."""
+    from opticrcwafdtd_b200 import geometry
+    d = 0.01
+    x = (np.arange(-60, 60) + 0.5) * d
+    y = x.copy()
+    z = np.arange(40) * d
+    bg, n = 1.0, 2.0
+
+    def area(shape, k):
+        e = geometry.epsComponents3D(x, y, z, bg, [shape])["z"][:, :, k]
+        return float(np.sum((e - bg ** 2) / (n ** 2 - bg ** 2))) * d * d
+
+    k = 20   # the plane at z = 0.2 + h, inside every shape below
+    zc = z[k] + d / 2
+    assert abs(area(["cyl", [0.03, -0.05, 0.31, 0.05, 0.35, n]], k) / (np.pi * 0.31 ** 2) - 1) < 5e-3
+    # a gentle cone: on a steep wall the radius changes within a cell's
+    # height and the harmonic mean along z no longer measures the fill
+    r = 0.2 + (0.26 - 0.2) * (zc - 0.05) / (0.35 - 0.05)
+    assert abs(area(["cone", [0.0, 0.0, 0.2, 0.26, 0.05, 0.35, n]], k) / (np.pi * r * r) - 1) < 5e-3
+    tri = dict(xy=[[-0.4, -0.3], [0.45, -0.2], [0.05, 0.5]], z1=0.05, z2=0.35, n=n)
+    tri_area = 0.5 * abs((0.45 + 0.4) * (0.5 + 0.3) - (0.05 + 0.4) * (-0.2 + 0.3))
+    assert abs(area(["polygon", tri], k) / tri_area - 1) < 5e-3
+    R = np.array([[0.1, 0.12], [0.0, 0.09]])
+    lat = dict(x0=-0.25, y0=-0.25, period=0.5, R=R, z1=0.05, z2=0.35, n=n)
+    assert abs(area(["lattice", lat], k) / (np.pi * np.sum(R ** 2)) - 1) < 1e-2
