@@ -96,3 +96,33 @@ def _header_struct_fields(name):
 def test_ctypes_mirrors_match_header_structs(cname, pyname):
     fields = [f[0] for f in getattr(_abi, pyname)._fields_]
     assert fields == _header_struct_fields(cname)
+
+
+def _sim3d(**kw):
+    from tests import cases
+    s = cases.box3d_sim(n=(20, 18, 24), steps=10)
+    s.update(kw)
+    return s
+
+
+@pytest.mark.parametrize("change,frag", [
+    (lambda s: s["eps"].update(x=-np.ones_like(s["eps"]["x"])), "positive"),
+    (lambda s: s.update(courant=0.6), "stability"),
+    (lambda s: s.update(npml=[12, 5, 7]), "does not fit"),
+    (lambda s: s["source"].update(index=2), "inside the CPML"),
+    (lambda s: s.update(monitors=[dict(axis=3, index=25)]), "outside the grid"),
+    (lambda s: s.update(lambdas=[0.6, -1.0]), "positive"),
+])
+def test_host_validation_rejects_bad_3d_sims(change, frag):
+    """3D sims are validated on the host before any device work
+    (fdtd3D.m:11-24 field rules), with the reference's messages."""
+    lib = _lib.load()
+    s = _sim3d()
+    s["eps"] = dict(s["eps"])
+    s["source"] = dict(s["source"])
+    change(s)
+    m = _abi.marshal_sim3d(s)
+    o, _ = _abi.alloc_out3d(m)
+    st = lib.orf_fdtd3d_run(C.byref(m.struct), C.byref(o), _abi.PROGRESS_FN(0), None)
+    assert st == 1, _lib.last_error()
+    assert frag in _lib.last_error()
