@@ -69,6 +69,15 @@ def test_no_device_fails_loudly_without_fallback():
     with pytest.raises(_abi.OrfError) as e:
         orf.fdtd2DTE(_sim())
     assert e.value.identifier == "orf:noDevice"
+    # the GPU permittivity generator and 3D runs refuse as well: no host path
+    x = (np.arange(8) + 0.5) * 0.02
+    with pytest.raises(_abi.OrfError) as e:
+        orf.epsComponents3D(x, x, x, 1.0, [["box", [0, 0.1, 0, 0.1, 0, 0.1, 2.0]]], device=True)
+    assert e.value.identifier == "orf:noDevice"
+    from tests import cases
+    with pytest.raises(_abi.OrfError) as e:
+        orf.fdtd3D(cases.box3d_sim(n=(20, 18, 24), steps=10))
+    assert e.value.identifier == "orf:noDevice"
 
 
 def _header_struct_fields(name):
