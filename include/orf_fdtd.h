@@ -192,7 +192,10 @@ ORF_API int32_t orf_ctx_create(int32_t device, void* stream, orf_ctx** out);
 /* Releases the caller's reference.  Every job and server built on the
  * context holds one more, so the context (its stream, tuning and counters)
  * lives until the last of them is destroyed: contexts, jobs and servers may
- * be destroyed in any order. */
+ * be destroyed in any order.  The device memory of finished runs is kept for
+ * reuse by later runs (up to 8 GiB per process, released blocks first wait
+ * for the device to be idle); releasing the last reference to a context
+ * returns its device's cached memory to the driver. */
 ORF_API int32_t orf_ctx_destroy(orf_ctx* ctx);
 ORF_API int32_t orf_ctx_set_tuning(orf_ctx* ctx, const orf_tuning* t);
 ORF_API int32_t orf_ctx_set_timing(orf_ctx* ctx, int32_t on);
