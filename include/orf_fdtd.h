@@ -332,11 +332,12 @@ ORF_API double  orf_serve_clock(orf_server* srv);
 ORF_API int32_t orf_serve_close(orf_server* srv);
 
 /* Subpixel-averaged permittivity of a 3D grid on the GPU (the device form
- * of epsComponents3D, toolbox/+orf/epsComponents3D.m:1-27, Method
- * "directional"): for each Yee E component, cells whose centre an interface
- * passes near are sampled at nsub^3 points and take the harmonic mean along
- * the component's axis, then the arithmetic mean over the other two; shapes
- * paint in order over the background nbg.  x, y, z are the cell centres
+ * of epsComponents3D, toolbox/+orf/epsComponents3D.m:1-27): for each Yee E
+ * component, cells whose centre an interface passes near are sampled at
+ * nsub^3 points; method 0 ("directional") takes the harmonic mean along the
+ * component's axis, then the arithmetic mean over the other two; method 1
+ * ("kottke") 1/eps_cc = n_c^2 <1/eps> + (1 - n_c^2)/<eps> with n the first
+ * moment of the samples; shapes paint in order over the background nbg.  x, y, z are the cell centres
  * (uniform, one spacing); period = {Lx, Ly} folds x and y into [-L/2, L/2)
  * (NULL: no folding).  ex, ey, ez receive nx*ny*nz doubles each, column-major
  * (x fastest), at (x+d/2, y, z), (x, y+d/2, z), (x, y, z+d/2).  The values
@@ -357,7 +358,8 @@ typedef struct orf_eps_shape {
     const double* data;
 } orf_eps_shape;
 ORF_API int32_t orf_eps3d(orf_ctx* ctx, const double* x, const double* y, const double* z, int32_t nx,
-                          int32_t ny, int32_t nz, double nbg, int32_t nsub, const double* period,
+                          int32_t ny, int32_t nz, double nbg, int32_t nsub, int32_t method,
+                          const double* period,
                           int32_t nshape, const orf_eps_shape* shapes, double* ex, double* ey, double* ez);
 
 #ifdef __cplusplus

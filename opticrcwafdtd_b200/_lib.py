@@ -59,7 +59,7 @@ _SIGS = {
     "orf_serve_pending": (C.c_int32, [C.c_void_p, P(C.c_int32), P(C.c_int32)]),
     "orf_serve_preempt": (C.c_int32, [C.c_void_p, C.c_int64]),
     "orf_eps3d": (C.c_int32, [C.c_void_p, P(C.c_double), P(C.c_double), P(C.c_double), C.c_int32, C.c_int32,
-                              C.c_int32, C.c_double, C.c_int32, P(C.c_double), C.c_int32, C.c_void_p,
+                              C.c_int32, C.c_double, C.c_int32, C.c_int32, P(C.c_double), C.c_int32, C.c_void_p,
                               P(C.c_double), P(C.c_double), P(C.c_double)]),
     "orf_serve_clock": (C.c_double, [C.c_void_p]),
     "orf_serve_close": (C.c_int32, [C.c_void_p]),

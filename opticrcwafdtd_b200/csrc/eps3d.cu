@@ -6,7 +6,8 @@
 // the shapes in order at its centre; cells an interface may cross (the
 // shapes' band tests) are sub-sampled at NSub^3 points and take the
 // directional mean -- harmonic along c, then arithmetic over the other two
-// axes.  One thread per cell; the sub-samples are painted on the fly.
+// axes -- or the Kottke diagonal.  One thread per cell; the sub-samples are
+// painted on the fly.
 //
 // Every operation is the host generator's, in its order, with explicit
 // round-to-nearest intrinsics (no contraction): the two produce the same
@@ -33,6 +34,7 @@ struct EpsArgs {
     double bg2;        // background n^2
     double Lx, Ly;     // fold periods (0: none)
     int nsub, nshape;
+    int method;        // 0 directional, 1 Kottke
     const double* off; // sub-sample offsets, nsub
     const DevShape* sh;
 };
@@ -173,7 +175,44 @@ __global__ void k_eps3d(EpsArgs a, double* __restrict__ out) {
             if (inside(a.sh[q], Xf, Yf, Z)) e = a.sh[q].n2;
             bnd = bnd || band(a.sh[q], Xf, Yf, Z, a.h);
         }
-        if (a.nsub > 1 && bnd) {
+        if (a.nsub > 1 && bnd && a.method == 1) {
+            // Kottke: <eps>, <1/eps> and the first moment g of the samples,
+            // each summed sequentially in row-major (x, y, z) order;
+            // 1/eps_cc = n_c^2 <1/eps> + (1 - n_c^2)/<eps>, n = g / |g|
+            const int N = a.nsub, N3 = N * N * N;
+            double se = 0.0, si = 0.0, g[3] = {0.0, 0.0, 0.0};
+            for (int u = 0; u < N; ++u)
+                for (int v = 0; v < N; ++v)
+                    for (int w = 0; w < N; ++w) {
+                        const double sx = fold(add(X, mul(a.off[u], a.d)), a.Lx);
+                        const double sy = fold(add(Y, mul(a.off[v], a.d)), a.Ly);
+                        const double sz = add(Z, mul(a.off[w], a.d));
+                        const double ev = paint(a, sx, sy, sz);
+                        const double iv = dvd(1.0, ev);
+                        const double p0 = mul(ev, a.off[u]), p1 = mul(ev, a.off[v]), p2 = mul(ev, a.off[w]);
+                        if (u == 0 && v == 0 && w == 0) {
+                            se = ev;
+                            si = iv;
+                            g[0] = p0;
+                            g[1] = p1;
+                            g[2] = p2;
+                        } else {
+                            se = add(se, ev);
+                            si = add(si, iv);
+                            g[0] = add(g[0], p0);
+                            g[1] = add(g[1], p1);
+                            g[2] = add(g[2], p2);
+                        }
+                    }
+            const double me = dvd(se, (double)N3), mi = dvd(si, (double)N3);
+            const double gn = sqrt(add(add(mul(g[0], g[0]), mul(g[1], g[1])), mul(g[2], g[2])));
+            double nc2 = 0.0;
+            if (gn > 0.0) {
+                const double r = dvd(g[a.c], gn);
+                nc2 = mul(r, r);
+            }
+            e = dvd(1.0, add(mul(nc2, mi), dvd(sub(1.0, nc2), me)));
+        } else if (a.nsub > 1 && bnd) {
             // sample (s0, s1, s2) along (x, y, z); the sum along c is
             // sequential, then the NSub^2 harmonic means are summed in
             // row-major order of the two remaining axes
@@ -206,10 +245,11 @@ __global__ void k_eps3d(EpsArgs a, double* __restrict__ out) {
 }  // namespace
 
 int eps3d(orf_ctx* ctx, const double* x, const double* y, const double* z, int nx, int ny, int nz, double nbg,
-          int nsub, const double* period, int nshape, const orf_eps_shape* shapes, double* const* outs) {
+          int nsub, int method, const double* period, int nshape, const orf_eps_shape* shapes,
+          double* const* outs) {
     if (nx < 2 || ny < 1 || nz < 1 || nsub < 1 || nsub > 16 || nshape < 0 || (nshape && !shapes) || !x || !y ||
-        !z) {
-        set_error("orf_eps3d: invalid grid, NSub (1..16) or shape list");
+        !z || method < 0 || method > 1) {
+        set_error("orf_eps3d: invalid grid, NSub (1..16), method (0, 1) or shape list");
         return ORF_EINVAL;
     }
     cudaStream_t st = ctx->stream;
@@ -291,6 +331,7 @@ int eps3d(orf_ctx* ctx, const double* x, const double* y, const double* z, int n
     a.Lx = period ? period[0] : 0.0;
     a.Ly = period ? period[1] : 0.0;
     a.nsub = nsub;
+    a.method = method;
     a.nshape = nshape;
     a.off = d_off;
     a.sh = d_sh;
@@ -310,8 +351,8 @@ int eps3d(orf_ctx* ctx, const double* x, const double* y, const double* z, int n
 }  // namespace orf
 
 extern "C" int32_t orf_eps3d(orf_ctx* ctx, const double* x, const double* y, const double* z, int32_t nx, int32_t ny,
-                             int32_t nz, double nbg, int32_t nsub, const double* period, int32_t nshape,
-                             const orf_eps_shape* shapes, double* ex, double* ey, double* ez) {
+                             int32_t nz, double nbg, int32_t nsub, int32_t method, const double* period,
+                             int32_t nshape, const orf_eps_shape* shapes, double* ex, double* ey, double* ez) {
     int st = ORF_OK;
     if (!ctx) ctx = orf::default_ctx(&st);
     if (!ctx) return st;
@@ -323,5 +364,5 @@ extern "C" int32_t orf_eps3d(orf_ctx* ctx, const double* x, const double* y, con
     cudaGetDevice(&dev);
     if (dev != ctx->device) ORF_CUDA(cudaSetDevice(ctx->device));
     double* outs[3] = {ex, ey, ez};
-    return orf::eps3d(ctx, x, y, z, nx, ny, nz, nbg, nsub, period, nshape, shapes, outs);
+    return orf::eps3d(ctx, x, y, z, nx, ny, nz, nbg, nsub, method, period, nshape, shapes, outs);
 }

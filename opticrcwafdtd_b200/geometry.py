@@ -312,8 +312,8 @@ def epsComponents3D(x, y, z, nBg: float, shapes, NSub: int = 4, Period=None,
     folds x, y into [-L/2, L/2).
 
     device: a Context (or True for the current device's default context)
-    computes the "directional" form on the GPU (orf_eps3d), bitwise the same
-    values, in milliseconds per component instead of seconds.
+    computes either form on the GPU (orf_eps3d), bitwise the same values, in
+    milliseconds per component instead of seconds.
     """
     x = np.asarray(x, dtype=float).ravel()
     y = np.asarray(y, dtype=float).ravel()
@@ -325,9 +325,9 @@ def epsComponents3D(x, y, z, nBg: float, shapes, NSub: int = 4, Period=None,
     if Period is not None:
         Lx, Ly = (float(Period[0]), float(Period[1]))
     if device is not None and device is not False:
-        if Method != "directional":
-            raise ValueError('the GPU generator computes Method "directional" only')
-        return _eps3d_device(x, y, z, nBg, sh, NSub, Period, device)
+        if Method not in ("directional", "kottke"):
+            raise ValueError('Method must be "directional" or "kottke"')
+        return _eps3d_device(x, y, z, nBg, sh, NSub, Period, device, Method)
     off = _offsets(NSub)
     out = {}
     for c, name in enumerate(("x", "y", "z")):
@@ -352,7 +352,7 @@ def epsComponents3D(x, y, z, nBg: float, shapes, NSub: int = 4, Period=None,
     return out
 
 
-def _eps3d_device(x, y, z, nBg, sh, NSub, Period, device) -> dict:
+def _eps3d_device(x, y, z, nBg, sh, NSub, Period, device, Method="directional") -> dict:
     """epsComponents3D on the GPU through orf_eps3d (csrc/eps3d.cu)."""
     import ctypes as C
     from . import _abi, _lib
@@ -387,7 +387,8 @@ def _eps3d_device(x, y, z, nBg, sh, NSub, Period, device) -> dict:
     per = None if Period is None else np.array([float(Period[0]), float(Period[1])])
     ctx = getattr(device, "handle", None)
     st = lib.orf_eps3d(ctx, _abi._ptr(x), _abi._ptr(y), _abi._ptr(z), x.size, y.size, z.size, float(nBg),
-                       int(NSub), _abi._ptr(per), len(sh), C.cast(arr, C.c_void_p),
+                       int(NSub), 1 if Method == "kottke" else 0, _abi._ptr(per), len(sh),
+                       C.cast(arr, C.c_void_p),
                        _abi._ptr(out["x"]), _abi._ptr(out["y"]), _abi._ptr(out["z"]))
     _lib.check(st, "epsComponents3D")
     return out
@@ -473,12 +474,21 @@ def _component(c, X, Y, Z, sh, nBg, h, d, off, NSub, Lx, Ly, Method):
                     tot = tot + r[:, q]
                 val[q0:q1] = tot / (NSub * NSub)
             elif Method == "kottke":
-                mean_e = es.reshape(mq, -1).mean(axis=1)
-                mean_inv = (1.0 / es).reshape(mq, -1).mean(axis=1)
-                grads = []
-                for ax in range(3):
-                    w = off.reshape([-1 if a == ax else 1 for a in range(3)])
-                    grads.append((es * w[None]).reshape(mq, -1).sum(axis=1))
+                # sums sequential over the samples in row-major (x, y, z)
+                # order, as the GPU generator adds them
+                flat = es.reshape(mq, -1)
+                inv = 1.0 / flat
+                n3 = NSub ** 3
+                q3 = np.arange(n3)
+                w = [off[q3 // (NSub * NSub)], off[(q3 // NSub) % NSub], off[q3 % NSub]]
+                se, si = flat[:, 0], inv[:, 0]
+                grads = [flat[:, 0] * w[ax][0] for ax in range(3)]
+                for q in range(1, n3):
+                    se = se + flat[:, q]
+                    si = si + inv[:, q]
+                    for ax in range(3):
+                        grads[ax] = grads[ax] + flat[:, q] * w[ax][q]
+                mean_e, mean_inv = se / n3, si / n3
                 gn = np.sqrt(sum(g * g for g in grads))
                 nc2 = np.where(gn > 0, (grads[c] / np.where(gn > 0, gn, 1.0)) ** 2, 0.0)
                 val[q0:q1] = 1.0 / (nc2 * mean_inv + (1.0 - nc2) / mean_e)

@@ -25,9 +25,10 @@ def _shapes(rng):
     ]
 
 
+@pytest.mark.parametrize("method", ["directional", "kottke"])
 @pytest.mark.parametrize("nsub", [1, 2, 4, 5])
 @pytest.mark.parametrize("periodic", [False, True])
-def test_gpu_eps_matches_host_bitwise(nsub, periodic):
+def test_gpu_eps_matches_host_bitwise(nsub, periodic, method):
     rng = np.random.default_rng(7)
     d = 0.025
     x = (np.arange(40) + 0.5) * d
@@ -35,9 +36,9 @@ def test_gpu_eps_matches_host_bitwise(nsub, periodic):
     z = np.arange(26) * d
     per = [40 * d, 36 * d] if periodic else None
     sh = _shapes(rng)
-    host = epsComponents3D(x, y, z, 1.0, sh, NSub=nsub, Period=per)
+    host = epsComponents3D(x, y, z, 1.0, sh, NSub=nsub, Period=per, Method=method)
     ctx = Context(0)
-    dev = epsComponents3D(x, y, z, 1.0, sh, NSub=nsub, Period=per, device=ctx)
+    dev = epsComponents3D(x, y, z, 1.0, sh, NSub=nsub, Period=per, Method=method, device=ctx)
     ctx.close()
     for k in "xyz":
         assert dev[k].flags["F_CONTIGUOUS"]
