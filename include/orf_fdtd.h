@@ -200,6 +200,18 @@ ORF_API int32_t orf_ctx_destroy(orf_ctx* ctx);
 ORF_API int32_t orf_ctx_set_tuning(orf_ctx* ctx, const orf_tuning* t);
 ORF_API int32_t orf_ctx_set_timing(orf_ctx* ctx, int32_t on);
 ORF_API int32_t orf_ctx_get_stats(orf_ctx* ctx, orf_kernel_stats* st);
+/* No counterpart in the reference (whose CPU / gpuArray loop has no device
+ * waits).  Bounds of the 3D kernel's only device-side waits, the TMA plane
+ * loads of its z-march: each wait gives up after wait_ns nanoseconds (0 = one
+ * second, the default) and the run then returns ORF_ETIMEOUT_DEVICE from its
+ * finish (the CTA that gave up first waits, with the same bound, for the
+ * plane copies it still has in flight, and later launches of the run return
+ * at once).  stall_plane >= 0 is a failure-detection test hook: in 3D jobs
+ * created on this context afterwards, every tile loaded by TMA arms the ring
+ * slot of its z-plane k0 + stall_plane without issuing the copies, so that
+ * wait runs out; -1 (the default) turns it off.  Runs created before the call
+ * keep their launch arguments (CUDA graphs). */
+ORF_API int32_t orf_ctx_set_wait_injection(orf_ctx* ctx, int32_t stall_plane, int64_t wait_ns);
 ORF_API int32_t orf_ctx_reset_stats(orf_ctx* ctx);
 /* No counterpart in the reference.  Times every 2D kernel variant and fused
  * step depth (4, 6, 8, 10) on `steps` steps (0 = 200) of the n sims (shutoff
@@ -207,6 +219,28 @@ ORF_API int32_t orf_ctx_reset_stats(orf_ctx* ctx);
  * the fastest in ctx's tuning and returns it in *best (may be NULL).  Only
  * speed depends on the choice: every candidate computes the same values. */
 ORF_API int32_t orf_autotune2d(orf_ctx* ctx, int32_t n, const orf_sim2d* sims, int32_t steps, orf_tuning* best);
+
+/* One tile of a 2D run's plan (orf_plan2d): a CTA loads the lx x lz window at
+ * (li0, lk0), advances it by the fused depth and stores the output rectangle
+ * (oi0, ok0, ow, oh).  kind 0: interior tile (no CPML code), 1: frame tile
+ * (CPML and boundary masks).  flags: 1 the loaded columns hold the TF/SF
+ * plane, 2 / 4 the output holds an x / z monitor line, 8 / 16 (frame) the
+ * loaded cells reach an x / z CPML slab. */
+typedef struct orf_tile2d {
+    int32_t kind;
+    int32_t li0, lk0, lx, lz;
+    int32_t oi0, ok0, ow, oh;
+    int32_t flags;
+} orf_tile2d;
+
+/* No counterpart in the reference.  Host-only view of the tiles a 2D run of
+ * `sim` would use under `tuning` (NULL: the defaults): the fused depth, the
+ * interior kernel variant and every tile, interior tiles first.  Needs no
+ * device, so tests and tools can check the tiling on any host.  The counts
+ * are always written; the tiles only when tiles != NULL and cap holds them
+ * all (ORF_ETOOLARGE when cap > 0 is too small). */
+ORF_API int32_t orf_plan2d(const orf_sim2d* sim, const orf_tuning* tuning, orf_tile2d* tiles, int32_t cap,
+                           int32_t* n_interior, int32_t* n_frame, int32_t* tsteps, int32_t* variant);
 
 /* ------------------------------------------------------------ 2D runs --- */
 /* Element counts of the caller-allocated out arrays (complex counts are in
@@ -263,12 +297,17 @@ ORF_API int32_t orf_job_restore(orf_job* job, const void* buf, size_t bytes);
  * __device__ array that every GPU loading this library reserves until exit.
  * Runs needing more return ORF_ETOOLARGE, before any device work (the
  * 800 x 300 FP64 grating coupler with 51 wavelengths needs
- * about 20 MiB).  The first
- * call on a device looks up the array's address and should come before any
- * stream capture.  Calls share the array: calls that overlap on the GPU race,
- * and each call zeroes what it uses first.  There is no progress callback;
- * work is queued on `stream` (a cudaStream_t; NULL = per-thread default
- * stream) and the call returns when the run is done. */
+ * about 20 MiB).  The first call on a device does a one-time set-up there:
+ * it looks up the array's address and, CUDA loading modules lazily, loads the
+ * module that holds the array (which reserves it) and the 2D kernels' code.
+ * Make that first call (a small run is enough) at start-up, before the
+ * device's memory goes to the caller's pool and before any stream capture;
+ * later calls take no device memory.  `stream` (a cudaStream_t; NULL = the
+ * per-thread default stream) must belong to the current device (ORF_EINVAL
+ * otherwise): the array's address is the current device's.  Calls share the
+ * array: calls that overlap on the GPU race, and each call zeroes what it
+ * uses first.  There is no progress callback; the call returns when the run
+ * is done. */
 ORF_API int32_t orf_fdtd2d_run_noalloc(const orf_sim2d* sim, orf_out2d* out, void* stream);
 
 /* ------------------------------------------------------------ 3D runs --- */

@@ -95,6 +95,10 @@ class OrfTuning(C.Structure):
                 ("use_graph", C.c_int32), ("_pad", C.c_int32)]
 
 
+class OrfTile2D(C.Structure):
+    _fields_ = [(k, C.c_int32) for k in ("kind", "li0", "lk0", "lx", "lz", "oi0", "ok0", "ow", "oh", "flags")]
+
+
 class OrfKernelStats(C.Structure):
     _fields_ = [("interior_ms", C.c_double), ("interior_launches", C.c_int64),
                 ("interior_cell_updates", C.c_int64),

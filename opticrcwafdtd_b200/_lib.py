@@ -26,6 +26,7 @@ _SIGS = {
     "orf_ctx_set_tuning": (C.c_int32, [C.c_void_p, P(_abi.OrfTuning)]),
     "orf_ctx_set_timing": (C.c_int32, [C.c_void_p, C.c_int32]),
     "orf_ctx_get_stats": (C.c_int32, [C.c_void_p, P(_abi.OrfKernelStats)]),
+    "orf_ctx_set_wait_injection": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int64]),
     "orf_ctx_reset_stats": (C.c_int32, [C.c_void_p]),
     "orf_out2d_sizes": (C.c_int32, [P(_abi.OrfSim2D), P(C.c_int64), P(C.c_int64), P(C.c_int64), P(C.c_int64)]),
     "orf_fdtd2d_run": (C.c_int32, [P(_abi.OrfSim2D), P(_abi.OrfOut2D), _abi.PROGRESS_FN, C.c_void_p]),
@@ -51,6 +52,8 @@ _SIGS = {
     "orf_batch2d_run": (C.c_int32, [C.c_void_p, C.c_int32, P(_abi.OrfSim2D), P(_abi.OrfOut2D), _abi.PROGRESS_FN,
                                     C.c_void_p]),
     "orf_autotune2d": (C.c_int32, [C.c_void_p, C.c_int32, P(_abi.OrfSim2D), C.c_int32, P(_abi.OrfTuning)]),
+    "orf_plan2d": (C.c_int32, [P(_abi.OrfSim2D), P(_abi.OrfTuning), P(_abi.OrfTile2D), C.c_int32, P(C.c_int32),
+                               P(C.c_int32), P(C.c_int32), P(C.c_int32)]),
     "orf_serve_open": (C.c_int32, [C.c_void_p, P(_abi.OrfServeCfg), P(C.c_void_p)]),
     "orf_serve_submit2d": (C.c_int32, [C.c_void_p, P(_abi.OrfSim2D), P(_abi.OrfOut2D), P(C.c_int64)]),
     "orf_serve_submit3d": (C.c_int32, [C.c_void_p, P(_abi.OrfSim3D), P(_abi.OrfOut3D), P(C.c_int64)]),

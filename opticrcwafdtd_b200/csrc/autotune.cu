@@ -58,6 +58,7 @@ extern "C" int32_t orf_autotune2d(orf_ctx* ctx, int32_t n, const orf_sim2d* sims
         return ORF_EINVAL;
     }
     for (int q = 0; q < n; ++q) ORF_TRY(validate2d(&sims[q]));
+    ORF_ON_DEVICE(ctx->device);
     if (steps <= 0) steps = 4 * kChunk;
     // time a bounded piece of each run: no candidate may stop early on the
     // shutoff or the step budget

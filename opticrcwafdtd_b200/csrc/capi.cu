@@ -1,5 +1,6 @@
 // capi.cu -- the extern "C" entry points of liborf_fdtd.so (include/orf_fdtd.h).
 #include "engine.cuh"
+#include "job2d.cuh"
 
 using namespace orf;
 
@@ -78,7 +79,7 @@ int32_t orf_ctx_create(int32_t device, void* stream, orf_ctx** out) {
     int n = orf_device_count();
     if (n <= 0) { set_error("no CUDA device available"); return ORF_ENODEV; }
     if (device < 0 || device >= n) { set_error("device %d outside 0..%d", device, n - 1); return ORF_EINVAL; }
-    ORF_CUDA(cudaSetDevice(device));
+    ORF_ON_DEVICE(device);
     auto c = new orf_ctx();
     c->device = device;
     cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
@@ -113,6 +114,14 @@ int32_t orf_ctx_set_timing(orf_ctx* c, int32_t on) {
     return ORF_OK;
 }
 
+int32_t orf_ctx_set_wait_injection(orf_ctx* c, int32_t stall_plane, int64_t wait_ns) {
+    if (!c) return ORF_EINVAL;
+    if (wait_ns < 0) { set_error("wait_ns must be >= 0"); return ORF_EINVAL; }
+    c->stall_plane = stall_plane < 0 ? -1 : stall_plane;
+    c->wait_ns = (unsigned long long)wait_ns;
+    return ORF_OK;
+}
+
 int32_t orf_ctx_get_stats(orf_ctx* c, orf_kernel_stats* st) {
     if (!c || !st) return ORF_EINVAL;
     *st = c->stats;
@@ -137,6 +146,7 @@ int32_t orf_out2d_sizes(const orf_sim2d* s, int64_t* n_flux, int64_t* n_flux_z, 
 int32_t orf_fdtd2d_run_ctx(orf_ctx* ctx, const orf_sim2d* sim, orf_out2d* out, orf_progress_fn progress,
                            void* user) {
     if (!ctx || !sim || !out) { set_error("NULL argument"); return ORF_EINVAL; }
+    ORF_ON_DEVICE(ctx->device);
     const double t0 = now_s();
     orf_job* job = nullptr;
     ORF_TRY(make_job2d(ctx, sim, &job));
@@ -158,6 +168,7 @@ int32_t orf_fdtd2d_run(const orf_sim2d* sim, orf_out2d* out, orf_progress_fn pro
 
 int32_t orf_job2d_create(orf_ctx* ctx, const orf_sim2d* sim, orf_job** job) {
     if (!ctx || !job) return ORF_EINVAL;
+    ORF_ON_DEVICE(ctx->device);
     const int st = make_job2d(ctx, sim, job);
     if (st == ORF_OK) ctx_retain(ctx);
     return st;
@@ -165,6 +176,7 @@ int32_t orf_job2d_create(orf_ctx* ctx, const orf_sim2d* sim, orf_job** job) {
 
 int32_t orf_job3d_create(orf_ctx* ctx, const orf_sim3d* sim, orf_job** job) {
     if (!ctx || !job) return ORF_EINVAL;
+    ORF_ON_DEVICE(ctx->device);
     const int st = make_job3d(ctx, sim, job);
     if (st == ORF_OK) ctx_retain(ctx);
     return st;
@@ -172,28 +184,47 @@ int32_t orf_job3d_create(orf_ctx* ctx, const orf_sim3d* sim, orf_job** job) {
 
 int32_t orf_job_advance(orf_job* job, int64_t nsteps) {
     if (!job || nsteps < 0) return ORF_EINVAL;
+    ORF_ON_DEVICE(job->ctx->device);
     return job->advance(nsteps, nullptr, nullptr);
 }
 
 int32_t orf_job_sync(orf_job* job) {
     if (!job) return ORF_EINVAL;
+    ORF_ON_DEVICE(job->ctx->device);
     ORF_CUDA(cudaStreamSynchronize(job->ctx->stream));
     return ORF_OK;
 }
 
-int32_t orf_job_reset(orf_job* job) { return job ? job->reset() : ORF_EINVAL; }
+int32_t orf_job_reset(orf_job* job) {
+    if (!job) return ORF_EINVAL;
+    ORF_ON_DEVICE(job->ctx->device);
+    return job->reset();
+}
 int64_t orf_job_steps_done(orf_job* job) { return job ? job->steps_done() : -1; }
 int64_t orf_job_cells(orf_job* job) { return job ? job->cells() : -1; }
-int32_t orf_job2d_finish(orf_job* job, orf_out2d* out) { return (job && out) ? job->finish2d(out) : ORF_EINVAL; }
-int32_t orf_job3d_finish(orf_job* job, orf_out3d* out) { return (job && out) ? job->finish3d(out) : ORF_EINVAL; }
+int32_t orf_job2d_finish(orf_job* job, orf_out2d* out) {
+    if (!job || !out) return ORF_EINVAL;
+    ORF_ON_DEVICE(job->ctx->device);
+    return job->finish2d(out);
+}
+int32_t orf_job3d_finish(orf_job* job, orf_out3d* out) {
+    if (!job || !out) return ORF_EINVAL;
+    ORF_ON_DEVICE(job->ctx->device);
+    return job->finish3d(out);
+}
 int32_t orf_job_get_fields(orf_job* job, double* const* f, int32_t nf) {
-    return (job && f) ? job->get_fields(f, nf) : ORF_EINVAL;
+    if (!job || !f) return ORF_EINVAL;
+    ORF_ON_DEVICE(job->ctx->device);
+    return job->get_fields(f, nf);
 }
 int32_t orf_job_destroy(orf_job* job) {
     if (!job) return ORF_OK;
     orf_ctx* c = job->ctx;
-    delete job;
-    ctx_release(c);
+    {
+        ORF_ON_DEVICE(c->device);
+        delete job;
+        ctx_release(c);
+    }
     return ORF_OK;
 }
 
@@ -212,6 +243,7 @@ int32_t orf_out3d_sizes(const orf_sim3d* s, int32_t* na, int32_t* nb) {
 int32_t orf_fdtd3d_run_ctx(orf_ctx* ctx, const orf_sim3d* sim, orf_out3d* out, orf_progress_fn progress,
                            void* user) {
     if (!ctx || !sim || !out) { set_error("NULL argument"); return ORF_EINVAL; }
+    ORF_ON_DEVICE(ctx->device);
     const double t0 = now_s();
     orf_job* job = nullptr;
     ORF_TRY(make_job3d(ctx, sim, &job));
@@ -231,9 +263,42 @@ int32_t orf_fdtd3d_run(const orf_sim3d* sim, orf_out3d* out, orf_progress_fn pro
     return orf_fdtd3d_run_ctx(c, sim, out, progress, user);
 }
 
+int32_t orf_plan2d(const orf_sim2d* sim, const orf_tuning* tuning, orf_tile2d* tiles, int32_t cap,
+                   int32_t* n_interior, int32_t* n_frame, int32_t* tsteps, int32_t* variant) {
+    ORF_TRY(validate2d(sim));
+    orf_tuning tu{};
+    if (tuning) tu = *tuning;
+    if (tu.tsteps < 0 || tu.tsteps > kMaxSub) { set_error("tsteps must be 0..%d", kMaxSub); return ORF_EINVAL; }
+    Plan2D p;
+    ORF_TRY(plan2d(sim, tu, &p));
+    if (n_interior) *n_interior = p.nfast;
+    if (n_frame) *n_frame = p.nframe;
+    if (tsteps) *tsteps = p.T;
+    if (variant) *variant = p.fvariant;
+    const int n = p.nfast + p.nframe;
+    if (!tiles) return ORF_OK;
+    if (cap < n) {
+        set_error("orf_plan2d: %d tiles, room for %d", n, cap);
+        return cap > 0 ? ORF_ETOOLARGE : ORF_OK;
+    }
+    for (int q = 0; q < n; ++q) {
+        const FastTile2D& t = p.tiles[q];
+        const bool fr = q >= p.nfast;
+        tiles[q] = orf_tile2d{fr ? 1 : 0, t.li0, t.lk0, fr ? p.lx_pml : p.lx_int,
+                              fr ? p.lz_pml : 0, t.oi0, t.ok0, t.ow, t.oh, t.flags};
+        if (!fr) {
+            Variant2D v;
+            fast2d_info(p.fvariant, sim->precision == ORF_DOUBLE, false, &v);
+            tiles[q].lz = v.lz();
+        }
+    }
+    return ORF_OK;
+}
+
 int32_t orf_batch2d_run(orf_ctx* ctx, int32_t n, const orf_sim2d* sims, orf_out2d* outs, orf_progress_fn progress,
                         void* user) {
     if (!ctx || n < 0 || (n > 0 && (!sims || !outs))) { set_error("NULL argument"); return ORF_EINVAL; }
+    ORF_ON_DEVICE(ctx->device);
     return batch2d_run(ctx, n, sims, outs, progress, user);
 }
 

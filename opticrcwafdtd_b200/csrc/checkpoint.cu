@@ -149,16 +149,19 @@ extern "C" {
 
 int32_t orf_job_checkpoint_size(orf_job* job, size_t* bytes) {
     if (!job || !bytes) return ORF_EINVAL;
+    ORF_ON_DEVICE(job->ctx->device);
     return orf::job_checkpoint_size(job, bytes);
 }
 
 int32_t orf_job_checkpoint(orf_job* job, void* buf, size_t bytes) {
     if (!job || !buf) return ORF_EINVAL;
+    ORF_ON_DEVICE(job->ctx->device);
     return orf::job_checkpoint(job, buf, bytes);
 }
 
 int32_t orf_job_restore(orf_job* job, const void* buf, size_t bytes) {
     if (!job || !buf) return ORF_EINVAL;
+    ORF_ON_DEVICE(job->ctx->device);
     return orf::job_restore(job, buf, bytes, 0);
 }
 

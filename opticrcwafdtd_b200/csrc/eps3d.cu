@@ -360,9 +360,7 @@ extern "C" int32_t orf_eps3d(orf_ctx* ctx, const double* x, const double* y, con
         orf::set_error("orf_eps3d: output arrays are NULL");
         return ORF_EINVAL;
     }
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev != ctx->device) ORF_CUDA(cudaSetDevice(ctx->device));
+    ORF_ON_DEVICE(ctx->device);
     double* outs[3] = {ex, ey, ez};
     return orf::eps3d(ctx, x, y, z, nx, ny, nz, nbg, nsub, method, period, nshape, shapes, outs);
 }

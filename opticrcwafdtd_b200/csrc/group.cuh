@@ -254,9 +254,10 @@ struct Group3D : Group {
             if (tm && tm->begin(s, &a) != ORF_OK) return cudaErrorUnknown;
             const bool overlap = !tm && side.ok() && nt && ntp;
             cudaError_t e = overlap ? side.fork(s) : cudaSuccess;
-            if (e == cudaSuccess) e = launch_step3d(f64, false, idxw, d_insts, d_tiles, nt, par, off, we, s);
+            if (e == cudaSuccess) e = launch_step3d(f64, false, idxw, d_insts, d_tiles, nt, par, off, we, wait_ctl(ctx), s);
             if (e == cudaSuccess)
-                e = launch_step3d(f64, true, idxw, d_insts, d_tiles_pml, ntp, par, off, we, overlap ? side.s2 : s);
+                e = launch_step3d(f64, true, idxw, d_insts, d_tiles_pml, ntp, par, off, we, wait_ctl(ctx),
+                                  overlap ? side.s2 : s);
             if (e == cudaSuccess && overlap) e = side.join(s);
             if (e != cudaSuccess) return e;
             if (tm && tm->end(s, 0, all_cells, a) != ORF_OK) return cudaErrorUnknown;

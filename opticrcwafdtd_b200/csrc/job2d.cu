@@ -88,6 +88,146 @@ struct Lut {
     }
 };
 
+// Host-only plan of a run's 2D tiles: the interior kernel variant and fused
+// depth, the interior rectangle and the frame strips, and every tile's loaded
+// window, output rectangle and flags (pointers left unset).  Needs no device;
+// orf_plan2d exposes it for checks of the tiling.
+int plan2d(const orf_sim2d* s, const orf_tuning& tuning, Plan2D* plan) {
+
+    const bool f64 = s->precision == ORF_DOUBLE;
+    const bool per = s->periodic_z != 0;
+    const int nx = s->nx, nz = s->nz, npx = s->npml_x, npz = per ? 0 : s->npml_z;
+    const int pitch = (nx + 31) & ~31;
+    // defaults from the variant / depth sweeps on the 4000 x 1500 workload
+    const int fvariant = tuning.variant > 0 ? tuning.variant : (f64 ? 2 : 1);
+    Variant2D fv, pv;
+    if (!fast2d_info(fvariant, f64, false, &fv)) {
+        set_error("unknown 2D kernel variant %d", fvariant);
+        return ORF_EINVAL;
+    }
+    fast2d_info(0, f64, true, &pv);
+    // a tile's output keeps T cells (plus up to 3 of x alignment) from its edges
+    const int tmax = std::min({kMaxSub, (pv.lz() - 1) / 2, (pv.lx() - 4) / 2, (fv.lz() - 1) / 2, (fv.lx() - 4) / 2});
+    int T = tuning.tsteps > 0 ? tuning.tsteps : (f64 ? 6 : 8);
+    if (T > tmax) T = tmax;
+    if (T < 1) T = 1;
+
+    // An output cell's T-step dependency cone needs correct (CPML-free,
+    // unmasked) updates of P within distance T-1 and of A (B) within distance
+    // T on the low side: A at rows >= npz, B at columns >= npx, P at rows and
+    // columns >= 1.  On the high side P, A and B within distance T-1 must lie
+    // below the upper slabs (A starts at nz-1-npz, B at nx-1-npx) and exist.
+    int ax = npx + T, bx = nx - npx - T;
+    int az = per ? 0 : npz + T, bz = per ? nz : nz - npz - T;
+    // Frame tiles at the edge of the grid: outside the grid every field is
+    // zero at every step (the mask keeps it so), so a tile whose loaded
+    // window starts at the edge, or reaches past it, needs no T-cell margin
+    // on that side: its output runs up to the edge.  The x / z strips are
+    // widened to what whole frame tiles output anyway (the frame costs the
+    // same number of tiles and the interior shrinks by the cells the frame
+    // covers): a strip of one tile row is LZ - T rows high at the edge,
+    // each further row adds LZ - 2T (x: LX - T, then LX - 2T - 3 at worst).
+    {
+        const int lzp = pv.lz(), lxp = pv.lx();
+        if (!per && lzp - 2 * T > 0) {
+            int h = lzp - T;
+            while (h < az) h += lzp - 2 * T;
+            az = h;
+            bz = nz - h;
+        }
+        if (lxp - 2 * T - 3 > 0) {
+            int w = lxp - T;
+            while (w < ax) w += lxp - 2 * T - 3;
+            ax = w;
+            // the right strip: its first tile loads from ceil4(nx - LX) and so
+            // reaches the edge, if that still leaves the npx + T columns the
+            // interior needs; otherwise whole tiles of worst-case output
+            const int c4 = ((nx - lxp) + 3) & ~3;
+            if (nx - (c4 + T) >= npx + T) {
+                bx = c4 + T;
+            } else {
+                int wr = lxp - 2 * T - 3;
+                while (wr < nx - bx) wr += lxp - 2 * T - 3;
+                bx = nx - wr;
+            }
+        }
+    }
+    if (bx - ax < 8 || bz - az < 4) { ax = bx = 0; az = bz = 0; }   // everything is frame
+    std::vector<FastTile2D> inner, frame;
+    // tile the rectangle [x0,x1) x [z0,z1) with a geometry of LX x LZ cells;
+    // the loaded origin li0 is rounded down to a multiple of 4 cells.  Frame
+    // tiles (edge = true) load from the grid edge when they start there and
+    // output up to the edge when their window reaches it.
+    auto tile_rect = [&](std::vector<FastTile2D>& out, const Variant2D& v, int x0, int x1, int z0, int z1,
+                         bool edge) {
+        for (int ok0 = z0; ok0 < z1;) {
+            const bool zlo = edge && !per && ok0 == 0;
+            const int lk0 = zlo ? 0 : ok0 - T;
+            const bool zhi = edge && !per && lk0 + v.lz() >= nz;
+            const int oh = std::min((zhi ? nz : lk0 + v.lz() - T) - ok0, z1 - ok0);
+            for (int oi0 = x0; oi0 < x1;) {
+                const int a = oi0 - T;
+                const int li0 = (edge && oi0 == 0) ? 0 : a - ((a % 4) + 4) % 4;
+                const bool xhi = edge && li0 + v.lx() >= nx;
+                const int ow = std::min((xhi ? nx : li0 + v.lx() - T) - oi0, x1 - oi0);
+                FastTile2D t{};
+                t.pitch = pitch;
+                t.nz = nz;
+                t.nx = nx;
+                t.periodic = per ? 1 : 0;
+                t.li0 = li0;
+                t.lk0 = lk0;
+                t.oi0 = oi0;
+                t.ok0 = ok0;
+                t.ow = ow;
+                t.oh = oh;
+                out.push_back(t);
+                oi0 += ow;
+            }
+            ok0 += oh;
+        }
+    };
+    if (bx > ax) {
+        tile_rect(inner, fv, ax, bx, az, bz, false);
+        tile_rect(frame, pv, 0, nx, 0, az, true);
+        tile_rect(frame, pv, 0, nx, bz, nz, true);
+        tile_rect(frame, pv, 0, ax, az, bz, true);
+        tile_rect(frame, pv, bx, nx, az, bz, true);
+    } else {
+        tile_rect(frame, pv, 0, nx, 0, nz, true);
+    }
+    plan->fvariant = fvariant;
+    plan->T = T;
+    plan->nfast = (int)inner.size();
+    plan->nframe = (int)frame.size();
+    plan->lx_int = fv.lx();
+    plan->lx_pml = pv.lx();
+    plan->lz_pml = pv.lz();
+    plan->tiles = inner;
+    plan->tiles.insert(plan->tiles.end(), frame.begin(), frame.end());
+    const int sx = s->src_ix;
+    for (size_t q = 0; q < plan->tiles.size(); ++q) {
+        FastTile2D& t = plan->tiles[q];
+        const int lxt = (int)q < plan->nfast ? plan->lx_int : plan->lx_pml;
+        t.flags = 0;
+        if ((sx - 1 >= t.li0 && sx - 1 < t.li0 + lxt) || (sx >= t.li0 && sx < t.li0 + lxt)) t.flags |= 1;
+        if ((int)q >= plan->nfast) {
+            // frame tile: CPML slabs of x (columns < npx, >= nx-1-npx) and of
+            // z (rows < npz, >= nz-1-npz) that its loaded cells reach, with a
+            // cell of margin; the kernel skips the psi updates of an axis
+            // whose slabs the tile does not reach (they would leave every
+            // value unchanged: psi 0, profile (1, 0, 1))
+            if (npx > 0 && (t.li0 < npx + 1 || t.li0 + lxt > nx - npx - 2)) t.flags |= 8;
+            if (npz > 0 && (t.lk0 < npz + 1 || t.lk0 + plan->lz_pml > nz - npz - 2)) t.flags |= 16;
+        }
+        for (int m = 0; m < s->n_mon; ++m)
+            if (s->monitors[m] >= t.oi0 && s->monitors[m] < t.oi0 + t.ow) t.flags |= 2;
+        for (int m = 0; m < s->n_monz; ++m)
+            if (s->monitors_z[m] >= t.ok0 && s->monitors_z[m] < t.ok0 + t.oh) t.flags |= 4;
+    }
+    return ORF_OK;
+}
+
 template <class R>
 int Job2D<R>::create(const orf_sim2d* s) {
     ORF_TRY(validate2d(s));
@@ -171,16 +311,7 @@ int Job2D<R>::create(const orf_sim2d* s) {
     shutoff = s->shutoff;
 
     // ---- tiles
-    ORF_TRY(pick_tiling(npx, npz));
-    int lx_int = 32, lx_pml = 32, lz_pml = 0;
-    {
-        Variant2D fv;
-        if (fast2d_info(fvariant, sizeof(R) == 8, false, &fv)) lx_int = fv.lx();
-        if (fast2d_info(0, sizeof(R) == 8, true, &fv)) {
-            lx_pml = fv.lx();
-            lz_pml = fv.lz();
-        }
-    }
+    ORF_TRY(pick_tiling(s));
 
     // ---- DFT streams: x monitors (P, B lines), z monitors (P, A lines)
     const int sstride = 2 * nz * nM + 2 * nx * nMZ;
@@ -320,9 +451,7 @@ int Job2D<R>::create(const orf_sim2d* s) {
     h.samples = d_samples;
     h.st = d_st;
     ORF_TRY(up(d_inst, &h, sizeof(h)));
-    for (size_t q = 0; q < ftiles_host.size(); ++q) {
-        FastTile2D& t = ftiles_host[q];
-        const int lxt = (int)q < nfast ? lx_int : lx_pml;
+    for (FastTile2D& t : ftiles_host) {   // flags come from the plan
         for (int b = 0; b < 2; ++b) {
             t.f[b][0] = h.P[b];
             t.f[b][1] = h.A[b];
@@ -332,21 +461,6 @@ int Job2D<R>::create(const orf_sim2d* s) {
         t.idx1 = te ? d_ix0 : d_ix1;
         t.st = d_st;
         t.inst = d_inst;
-        t.flags = 0;
-        if ((sx - 1 >= t.li0 && sx - 1 < t.li0 + lxt) || (sx >= t.li0 && sx < t.li0 + lxt)) t.flags |= 1;
-        if ((int)q >= nfast) {
-            // frame tile: CPML slabs of x (columns < npx, >= nx-1-npx) and of
-            // z (rows < npz, >= nz-1-npz) that its loaded cells reach, with a
-            // cell of margin; the kernel skips the psi updates of an axis
-            // whose slabs the tile does not reach (they would leave every
-            // value unchanged: psi 0, profile (1, 0, 1))
-            if (npx > 0 && (t.li0 < npx + 1 || t.li0 + lxt > nx - npx - 2)) t.flags |= 8;
-            if (npz > 0 && (t.lk0 < npz + 1 || t.lk0 + lz_pml > nz - npz - 2)) t.flags |= 16;
-        }
-        for (int m = 0; m < nM; ++m)
-            if (s->monitors[m] >= t.oi0 && s->monitors[m] < t.oi0 + t.ow) t.flags |= 2;
-        for (int m = 0; m < nMZ; ++m)
-            if (s->monitors_z[m] >= t.ok0 && s->monitors_z[m] < t.ok0 + t.oh) t.flags |= 4;
     }
     ORF_TRY(up(d_ftiles, ftiles_host.data(), ftiles_host.size() * sizeof(FastTile2D)));
     std::vector<DftStream> hs(nstreams);
@@ -419,85 +533,15 @@ int Job2D<R>::create(const orf_sim2d* s) {
 }
 
 template <class R>
-int Job2D<R>::pick_tiling(int npx, int npz) {
+int Job2D<R>::pick_tiling(const orf_sim2d* s) {
     const bool f64 = sizeof(R) == 8;
-    // defaults from the variant / depth sweeps on the 4000 x 1500 workload
-    fvariant = ctx->tuning.variant > 0 ? ctx->tuning.variant : (f64 ? 2 : 1);
-    Variant2D fv, pv;
-    if (!fast2d_info(fvariant, f64, false, &fv)) {
-        set_error("unknown 2D kernel variant %d", fvariant);
-        return ORF_EINVAL;
-    }
-    fast2d_info(0, f64, true, &pv);
-    // a tile's output keeps T cells (plus up to 3 of x alignment) from its edges
-    const int tmax = std::min({kMaxSub, (pv.lz() - 1) / 2, (pv.lx() - 4) / 2, (fv.lz() - 1) / 2, (fv.lx() - 4) / 2});
-    T = ctx->tuning.tsteps > 0 ? ctx->tuning.tsteps : (f64 ? 6 : 8);
-    if (T > tmax) T = tmax;
-    if (T < 1) T = 1;
-
-    // An output cell's T-step dependency cone needs correct (CPML-free,
-    // unmasked) updates of P within distance T-1 and of A (B) within distance
-    // T on the low side: A at rows >= npz, B at columns >= npx, P at rows and
-    // columns >= 1.  On the high side P, A and B within distance T-1 must lie
-    // below the upper slabs (A starts at nz-1-npz, B at nx-1-npx) and exist.
-    int ax = npx + T, bx = nx - npx - T;
-    int az = per ? 0 : npz + T, bz = per ? nz : nz - npz - T;
-    // A frame tile outputs a fixed extent whatever the strip needs, so widen
-    // the strips to whole frame tiles: the frame costs the same number of
-    // tiles and the interior shrinks by the cells the frame covers anyway.
-    {
-        const int ohp = pv.lz() - 2 * T;                       // frame tile output rows
-        const int l0 = -T - (((-T) % 4) + 4) % 4;               // loaded origin of a tile at x = 0
-        const int owl = l0 + pv.lx() - T;                       // its output columns
-        const int owr = pv.lx() - 2 * T - 3;                    // output columns, worst x alignment
-        if (ohp > 0 && !per) {
-            az = ((az + ohp - 1) / ohp) * ohp;
-            bz = nz - ((nz - bz + ohp - 1) / ohp) * ohp;
-        }
-        if (owl > 0 && ax < owl) ax = owl;
-        if (owr > 0 && nx - bx < owr) bx = nx - owr;
-    }
-    if (bx - ax < 8 || bz - az < 4) { ax = bx = 0; az = bz = 0; }   // everything is frame
-    std::vector<FastTile2D> inner, frame;
-    // tile the rectangle [x0,x1) x [z0,z1) with a geometry of LX x LZ cells;
-    // the loaded origin li0 is rounded down to a multiple of 4 cells
-    auto tile_rect = [&](std::vector<FastTile2D>& out, const Variant2D& v, int x0, int x1, int z0, int z1) {
-        for (int ok0 = z0; ok0 < z1;) {
-            const int oh = std::min(v.lz() - 2 * T, z1 - ok0);
-            for (int oi0 = x0; oi0 < x1;) {
-                const int a = oi0 - T;
-                const int li0 = a - ((a % 4) + 4) % 4;
-                const int ow = std::min(li0 + v.lx() - T - oi0, x1 - oi0);
-                FastTile2D t{};
-                t.pitch = pitch;
-                t.nz = nz;
-                t.nx = nx;
-                t.periodic = per ? 1 : 0;
-                t.li0 = li0;
-                t.lk0 = ok0 - T;
-                t.oi0 = oi0;
-                t.ok0 = ok0;
-                t.ow = ow;
-                t.oh = oh;
-                out.push_back(t);
-                oi0 += ow;
-            }
-            ok0 += oh;
-        }
-    };
-    if (bx > ax) {
-        tile_rect(inner, fv, ax, bx, az, bz);
-        tile_rect(frame, pv, 0, nx, 0, az);
-        tile_rect(frame, pv, 0, nx, bz, nz);
-        tile_rect(frame, pv, 0, ax, az, bz);
-        tile_rect(frame, pv, bx, nx, az, bz);
-    } else {
-        tile_rect(frame, pv, 0, nx, 0, nz);
-    }
-    nfast = (int)inner.size();
-    nframe = (int)frame.size();
-    ftiles_host = inner;
-    ftiles_host.insert(ftiles_host.end(), frame.begin(), frame.end());
+    Plan2D plan;
+    ORF_TRY(plan2d(s, ctx->tuning, &plan));
+    fvariant = plan.fvariant;
+    T = plan.T;
+    nfast = plan.nfast;
+    nframe = plan.nframe;
+    ftiles_host = std::move(plan.tiles);
     const int bps_f = nfast ? fast2d_blocks_per_sm(f64, te, idx16, false, fvariant) : 1;
     const int bps_p = nframe ? fast2d_blocks_per_sm(f64, te, idx16, true, 0) : 1;
     if (bps_f < 1 || bps_p < 1) {

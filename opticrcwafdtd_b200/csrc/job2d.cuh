@@ -4,6 +4,16 @@
 
 namespace orf {
 
+// Host-only tile plan of a 2D run (job2d.cu, plan2d): tiles are
+// [interior | frame] with loaded windows, output rectangles and flags.
+struct Plan2D {
+    int fvariant = 1, T = 1;
+    int nfast = 0, nframe = 0;
+    int lx_int = 0, lx_pml = 0, lz_pml = 0;
+    std::vector<FastTile2D> tiles;
+};
+int plan2d(const orf_sim2d* s, const orf_tuning& tuning, Plan2D* plan);
+
 template <class R>
 struct Job2D : orf_job {
     // geometry / options
@@ -50,7 +60,7 @@ struct Job2D : orf_job {
     Job2D() { dims = 2; }
     ~Job2D() override;
     int create(const orf_sim2d* s);
-    int pick_tiling(int npx, int npz);
+    int pick_tiling(const orf_sim2d* s);
     int init_state();
     int advance(int64_t nsteps, orf_progress_fn progress, void* user) override;
     int64_t steps_done() override;

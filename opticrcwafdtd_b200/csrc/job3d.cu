@@ -463,25 +463,33 @@ int Job3D<R>::create(const orf_sim3d* s) {
     eng.nitems = nitems;
     eng.d_states = d_states;
     eng.nstates = 1;
-    const int64_t ncell = (int64_t)N();
+    // cells of the interior and of the CPML tile launches (timing records)
+    int64_t ncell_int = 0, ncell_pml = 0;
+    for (const Tile3D& t : tiles) ncell_int += (int64_t)t.tw * t.th * (t.k1 - t.k0);
+    for (const Tile3D& t : tiles_pml) ncell_pml += (int64_t)t.tw * t.th * (t.k1 - t.k0);
     if (!tiles.empty() && !tiles_pml.empty()) ORF_TRY(side.init());
-    eng.step = [this, ncell](int off, int nsub, int par, int we, cudaStream_t stream, KernelTimer* tm) -> cudaError_t {
+    eng.step = [this, ncell_int, ncell_pml](int off, int nsub, int par, int we, cudaStream_t stream,
+                                            KernelTimer* tm) -> cudaError_t {
         (void)nsub;
         cudaEvent_t a = nullptr;
-        if (tm && tm->begin(stream, &a) != ORF_OK) return cudaErrorUnknown;
         const bool f64 = sizeof(R) == 8;
         // the CPML tiles run next to the interior tiles (disjoint cells, both
-        // read buffer par) unless launches are being timed
+        // read buffer par) unless launches are being timed (then one after
+        // the other, each between its own events: kind 0 interior, 1 CPML)
         const bool overlap = !tm && side.ok();
         cudaError_t e = overlap ? side.fork(stream) : cudaSuccess;
-        if (e == cudaSuccess)
-            e = launch_step3d(f64, false, idxw, d_inst, d_tiles, (int)tiles.size(), par, off, we, stream);
-        if (e == cudaSuccess)
+        if (e == cudaSuccess && !tiles.empty()) {
+            if (tm && tm->begin(stream, &a) != ORF_OK) return cudaErrorUnknown;
+            e = launch_step3d(f64, false, idxw, d_inst, d_tiles, (int)tiles.size(), par, off, we, wait_ctl(ctx), stream);
+            if (e == cudaSuccess && tm && tm->end(stream, 0, ncell_int, a) != ORF_OK) return cudaErrorUnknown;
+        }
+        if (e == cudaSuccess && !tiles_pml.empty()) {
+            if (tm && tm->begin(stream, &a) != ORF_OK) return cudaErrorUnknown;
             e = launch_step3d(f64, true, idxw, d_inst, d_tiles_pml, (int)tiles_pml.size(), par, off, we,
-                              overlap ? side.s2 : stream);
+                              wait_ctl(ctx), overlap ? side.s2 : stream);
+            if (e == cudaSuccess && tm && tm->end(stream, 1, ncell_pml, a) != ORF_OK) return cudaErrorUnknown;
+        }
         if (e == cudaSuccess && overlap) e = side.join(stream);
-        if (e != cudaSuccess) return e;
-        if (tm && tm->end(stream, 0, ncell, a) != ORF_OK) return cudaErrorUnknown;
         return e;
     };
     ORF_CUDA(cudaStreamSynchronize(st));

@@ -8,13 +8,17 @@
 // kernels as orf_fdtd2d_run, but every device buffer of the run (fields and
 // their ping-pong copies, CPML state, material index and tables, DFT samples
 // and sums, flux) is carved from one file-scope static __device__ array of
-// kNoAllocBytes.  The driver reserves that array on every GPU that loads this
-// library, and it stays reserved until the process exits.
+// kNoAllocBytes.  The driver reserves that array on a GPU when this file's
+// module is loaded there, and it stays reserved until the process exits.
 //
 // Set-up: the first call on a device, with that device current, looks up the
 // array's device address with cudaGetSymbolAddress (host code cannot use the
-// symbol itself: on the host it names a stand-in, not device memory).  Make
-// that first call before any stream capture.
+// symbol itself: on the host it names a stand-in, not device memory).  CUDA
+// loads modules lazily, so that first call is also the one that loads this
+// module (reserving the array) and the 2D kernels (their code), on that
+// device: make it at start-up, a small run is enough, before the device's
+// memory is handed to the caller's pool and before any stream capture.  Later
+// calls take no device memory at all.
 //
 // Limits and sharing: a run whose state exceeds kNoAllocBytes is rejected
 // with ORF_ETOOLARGE before any device work.  Every call shares the one
@@ -105,6 +109,18 @@ extern "C" int32_t orf_fdtd2d_run_noalloc(const orf_sim2d* sim, orf_out2d* out, 
         return ORF_ENODEV;
     }
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : cudaStreamPerThread;
+    // the scratch address is the current device's: the stream must be on it
+    int sdev = dev;
+    e = cudaStreamGetDevice(s, &sdev);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        set_error("cudaStreamGetDevice: %s", cudaGetErrorString(e));
+        return ORF_EINVAL;
+    }
+    if (sdev != dev) {
+        set_error("stream belongs to device %d but the current device is %d", sdev, dev);
+        return ORF_EINVAL;
+    }
     if (sim->precision == ORF_SINGLE) return run_noalloc<float>(sim, out, s, dev);
     return run_noalloc<double>(sim, out, s, dev);
 }

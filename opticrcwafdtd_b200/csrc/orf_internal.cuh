@@ -214,8 +214,16 @@ constexpr int kSeg3 = 60;                  // z planes marched by one 3D CTA
 // One 3D time step (step3d_fused.cu): reads fields and psi of buffer par,
 // writes buffer par^1.  pml = false only for tiles with no cell (halo and
 // the plane below the segment included) near a CPML slab.
+// Bounds of the 3D kernel's plane waits: wait_ns per plane (0: one second);
+// stall_plane >= 0 is the failure-detection test hook (the plane k0 +
+// stall_plane of every TMA tile is armed but never loaded, so its wait runs
+// out), -1 in every production launch.
+struct WaitCtl {
+    unsigned long long wait_ns;
+    int stall_plane;
+};
 cudaError_t launch_step3d(bool fp64, bool pml, int idxw, const void* insts, const Tile3D* tiles, int ntiles, int par,
-                          int launch_off, int want_energy, cudaStream_t s);
+                          int launch_off, int want_energy, WaitCtl wc, cudaStream_t s);
 
 cudaError_t launch_flush(bool fp64, const DftStream* streams, const FlushItem* items, int nitems,
                          cudaStream_t s);

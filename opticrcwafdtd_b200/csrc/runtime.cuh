@@ -46,6 +46,34 @@ inline double now_s() {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
+// Makes `device` current for the scope of a C entry point and gives the
+// calling thread its own current device back on every return path, so a call
+// on a context of another GPU leaves the caller where it was.
+struct DeviceScope {
+    int prev = -1;
+    cudaError_t err = cudaSuccess;
+    explicit DeviceScope(int device) {
+        if (cudaGetDevice(&prev) != cudaSuccess) {
+            cudaGetLastError();
+            prev = -1;
+        }
+        if (prev != device) err = cudaSetDevice(device);
+    }
+    DeviceScope(const DeviceScope&) = delete;
+    DeviceScope& operator=(const DeviceScope&) = delete;
+    ~DeviceScope() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+#define ORF_ON_DEVICE(dev)                                                             \
+    ::orf::DeviceScope orf_devscope_(dev);                                             \
+    if (orf_devscope_.err != cudaSuccess) {                                            \
+        ::orf::set_error("cudaSetDevice(%d): %s", (int)(dev), cudaGetErrorString(orf_devscope_.err)); \
+        cudaGetLastError();                                                            \
+        return ORF_ECUDA;                                                              \
+    }
+
 // --------------------------------------------------------- shared physics --
 // These restate the reference's documented formulas; the CPU oracle holds an
 // independent copy of the same definitions.
@@ -164,12 +192,17 @@ struct orf_ctx {
     bool timing = false;
     orf_kernel_stats stats{};
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // bounded device waits of the 3D kernel (orf_ctx_set_wait_injection):
+    // limit per plane wait in ns (0: one second), test-hook stall plane (-1: off)
+    unsigned long long wait_ns = 0;
+    int stall_plane = -1;
     // references: the creator's, plus one per job or server built on the
     // context; the context is freed when the last one is released
     std::atomic<int> refs{1};
 };
 
 namespace orf {
+inline WaitCtl wait_ctl(const orf_ctx* c) { return WaitCtl{c->wait_ns, c->stall_plane}; }
 void ctx_retain(orf_ctx* c);
 void ctx_release(orf_ctx* c);
 }  // namespace orf

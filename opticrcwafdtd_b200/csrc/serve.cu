@@ -373,9 +373,7 @@ int32_t orf_serve_open(orf_ctx* ctx, const orf_serve_cfg* cfg, orf_server** srv)
         set_error("orf_serve_cfg fields must be >= 0");
         return ORF_EINVAL;
     }
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev != ctx->device) ORF_CUDA(cudaSetDevice(ctx->device));
+    ORF_ON_DEVICE(ctx->device);
     auto s = std::make_unique<orf_server>();
     s->ctx = ctx;
     if (c.max_device_bytes > 0) {
@@ -437,6 +435,7 @@ int32_t orf_serve_step(orf_server* srv) {
         set_error("srv is NULL");
         return ORF_EINVAL;
     }
+    ORF_ON_DEVICE(srv->ctx->device);
     return srv->step();
 }
 
@@ -463,9 +462,7 @@ int32_t orf_serve_preempt(orf_server* srv, int64_t ticket) {
         set_error("srv is NULL");
         return ORF_EINVAL;
     }
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev != srv->ctx->device) ORF_CUDA(cudaSetDevice(srv->ctx->device));
+    ORF_ON_DEVICE(srv->ctx->device);
     return srv->preempt(ticket);
 }
 
@@ -485,8 +482,11 @@ double orf_serve_clock(orf_server* srv) { return srv ? srv->clock() : 0.0; }
 int32_t orf_serve_close(orf_server* srv) {
     if (!srv) return ORF_OK;
     orf_ctx* c = srv->ctx;
-    delete srv;
-    ctx_release(c);
+    {
+        ORF_ON_DEVICE(c->device);
+        delete srv;
+        ctx_release(c);
+    }
     return ORF_OK;
 }
 

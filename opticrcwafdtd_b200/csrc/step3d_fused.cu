@@ -38,7 +38,8 @@ constexpr int CX = 3;                                     // smem column of x = 
 template <class R>
 constexpr int NS = sizeof(R) == 4 ? 4 : 3;               // planes in the ring (FP64: 3, for occupancy)
 constexpr int RPT = (RC + NT - 1) / NT;                   // region cells per thread
-constexpr long long kSpinMax = 1ll << 20;                 // bounded mbarrier wait (try_wait polls)
+constexpr long long kSpinMax = 1ll << 20;                 // bounded mbarrier wait: at most this many polls,
+constexpr unsigned long long kWaitNsDefault = 1000000000ull;   // and at most this long (ns) per plane
 constexpr int kIssuer = NT - 32;   // issues the TMA copies and polls their mbarriers: lane 0 of the
                                    // last warp, which has no halo H cell to recompute
 
@@ -164,6 +165,24 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long* b, unsigned pa
         : "memory");
     return ok != 0;
 }
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;\n" : "=l"(t));
+    return t;
+}
+// Wait for the phase of parity `parity` of mbarrier b to complete, giving up
+// after kSpinMax polls or limit_ns nanoseconds; true when it completed.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* b, unsigned parity,
+                                                  unsigned long long limit_ns) {
+    if (mbar_try_wait(b, parity)) return true;
+    const unsigned long long t0 = global_ns();
+    for (long long spins = 1; spins < kSpinMax; ++spins) {
+        if (mbar_try_wait(b, parity)) return true;
+        if ((spins & 63) == 0 && global_ns() - t0 > limit_ns) return false;
+    }
+    return false;
+}
+
 // 3D tiled TMA load of the box at (x, y, z) into shared memory, completing on b
 __device__ __forceinline__ void tma_load3(void* sdst, const void* tmap, int x, int y, int z, unsigned long long* b) {
     asm volatile(
@@ -209,11 +228,11 @@ __device__ __forceinline__ R coef(const R* slut, const R* __restrict__ lutc, int
 template <class R, class IT, bool PML>
 __global__ void __launch_bounds__(NT, sizeof(R) == 4 ? 4 : 3)
 k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, int par, int launch_off,
-         int want_energy) {
+         int want_energy, WaitCtl wc) {
     const Tile3D tile = tiles[blockIdx.x];
     const Inst3D<R>* __restrict__ I = insts + tile.inst;
     JobState* st = I->st;
-    if (st->done) return;
+    if (st->done || st->fault) return;   // finished, or an earlier launch gave up a wait
     const long long n = st->step + launch_off;
     if (n >= st->nmax) return;
 
@@ -235,6 +254,10 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
     __shared__ R slut[sizeof(IT) == 1 ? 256 : 1];
     __shared__ __align__(8) unsigned long long sbar[ns];
     __shared__ Cpml3<R> sx;
+    __shared__ int s_abort;   // set by the issuer when a plane wait runs out
+    // planes the issuer has armed (TMA) and the last one whose wait completed
+    // (the planes in between are in flight); only the issuer touches them
+    __shared__ int s_issued, s_waited;
 
     const int t = threadIdx.x;
     if (PML && t < 18) {   // CPML context: thread (kind, c, q) copies one psi pair
@@ -265,6 +288,8 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
     const bool use_tma = I->tmap != nullptr && !wrapx && !wrapy;
     const char* tm = reinterpret_cast<const char*>(I->tmap);
     constexpr unsigned kTx = (unsigned)(3 * SX * RY * sizeof(R) + 3 * SX * (RY - 1) * sizeof(R) + 3 * NT * sizeof(IT));
+    if (t == 0) s_abort = 0;
+    if (t == kIssuer) s_issued = s_waited = k0 - 1;
     if (use_tma && t == 0) {
         for (int q = 0; q < ns; ++q) mbar_init(&sbar[q], 1);
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
@@ -291,6 +316,7 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
     constexpr int WPR = TX * (int)sizeof(IT) / 4;   // words per row
     constexpr int NWI = 3 * TY * WPR;
 
+    const unsigned long long wait_ns = wc.wait_ns ? wc.wait_ns : kWaitNsDefault;
     // ---- plane p (wrapped or zero outside the grid) into slot s
     auto load_plane = [&](int p, int s2) {
         bool pok;
@@ -301,6 +327,10 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
                 // order the block's earlier generic reads of this slot before the async writes
                 asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
                 mbar_expect_tx(&sbar[s2], kTx);
+                s_issued = p;
+                // failure-detection test hook (off unless set on the host):
+                // the slot is armed but its copies are never issued
+                if (wc.stall_plane >= 0 && p == k0 + wc.stall_plane) return;
                 for (int q = 0; q < 3; ++q) {
                     tma_load3(sEq(s2, q), tm + 128 * (3 * par + q), i0 - 4, j0 - 1, zc, &sbar[s2]);
                     tma_load3(sHq(s2, q), tm + 128 * (6 + 3 * par + q), i0 - 4, j0 - 1, zc, &sbar[s2]);
@@ -340,14 +370,13 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
     bool timed_out = false;
     auto wait_plane = [&](int p, int s2) {
         if (use_tma) {
-            if (t != kIssuer) return;
+            if (t != kIssuer || timed_out) return;
             const unsigned parity = (unsigned)(((p - k0) / ns) & 1);
-            long long spins = 0;
-            while (!mbar_try_wait(&sbar[s2], parity)) {
-                if (++spins > kSpinMax) {
-                    timed_out = true;
-                    break;
-                }
+            if (mbar_wait_bounded(&sbar[s2], parity, wait_ns)) {
+                s_waited = p;
+            } else {
+                timed_out = true;
+                s_abort = 1;   // read by every thread after the next barrier
             }
         } else {
             cp_wait<ns - 3>();   // all but the planes issued after p
@@ -434,6 +463,7 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
         if (it == 0) wait_plane(k, s0);
         wait_plane(k + 1, s1);   // planes k and k+1 have landed (later ones may be in flight)
         __syncthreads();         // ... for every thread; everyone is done with plane k-1
+        if (s_abort) break;      // a wait ran out: the whole CTA leaves the march here
         if (k + ns - 1 <= k1) load_plane(k + ns - 1, sn);   // into the slot of plane k-1
         cp_commit();
         const R* E0x = sEq(s0, 0);
@@ -556,8 +586,18 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
         // the next iteration's first barrier separates these reads of the
         // new-H plane and slot s0 from their reuse
     }
-    asm volatile("cp.async.wait_all;\n" ::: "memory");   // no copy outlives the CTA
-    // (every TMA plane issued, k0 .. k1, was waited for inside the loop)
+    asm volatile("cp.async.wait_all;\n" ::: "memory");   // no cp.async copy outlives the CTA
+    // Every TMA plane armed, k0 .. k1, was waited for inside the march unless
+    // a wait ran out; then the planes armed after the last completed wait may
+    // still be writing into this CTA's shared memory: the issuer (which keeps
+    // the CTA resident) waits for each of them, with the same bound, before
+    // the CTA exits.
+    if (use_tma && t == kIssuer) {
+        for (int p = s_waited + 1; p <= s_issued; ++p) {
+            const int s2 = (p - k0) % ns;
+            if (!mbar_wait_bounded(&sbar[s2], (unsigned)(((p - k0) / ns) & 1), wait_ns)) timed_out = true;
+        }
+    }
     if (timed_out) st->fault = 1;
     if (t == 0) st->cur = par ^ 1;   // every CTA of the instance writes the same value
     if (want_energy) {   // warp reduction, one atomic per warp
@@ -568,7 +608,8 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
 }
 
 template <class R, class IT, bool PML>
-cudaError_t launch_one(const void* insts, const Tile3D* tiles, int ntiles, int par, int off, int we, cudaStream_t s) {
+cudaError_t launch_one(const void* insts, const Tile3D* tiles, int ntiles, int par, int off, int we, WaitCtl wc,
+                       cudaStream_t s) {
     constexpr size_t smem = smem_bytes<R, IT>();
     static int done[64] = {0};
     int dev = 0;
@@ -579,28 +620,28 @@ cudaError_t launch_one(const void* insts, const Tile3D* tiles, int ntiles, int p
         if (e != cudaSuccess) return e;
         done[dev] = 1;
     }
-    k_step3d<R, IT, PML><<<ntiles, NT, smem, s>>>(reinterpret_cast<const Inst3D<R>*>(insts), tiles, par, off, we);
+    k_step3d<R, IT, PML><<<ntiles, NT, smem, s>>>(reinterpret_cast<const Inst3D<R>*>(insts), tiles, par, off, we, wc);
     return cudaGetLastError();
 }
 
 template <class R, bool PML>
 cudaError_t launch_idx(int idxw, const void* insts, const Tile3D* tiles, int ntiles, int par, int off, int we,
-                       cudaStream_t s) {
-    if (idxw == 1) return launch_one<R, uint8_t, PML>(insts, tiles, ntiles, par, off, we, s);
-    if (idxw == 2) return launch_one<R, uint16_t, PML>(insts, tiles, ntiles, par, off, we, s);
-    return launch_one<R, uint32_t, PML>(insts, tiles, ntiles, par, off, we, s);
+                       WaitCtl wc, cudaStream_t s) {
+    if (idxw == 1) return launch_one<R, uint8_t, PML>(insts, tiles, ntiles, par, off, we, wc, s);
+    if (idxw == 2) return launch_one<R, uint16_t, PML>(insts, tiles, ntiles, par, off, we, wc, s);
+    return launch_one<R, uint32_t, PML>(insts, tiles, ntiles, par, off, we, wc, s);
 }
 
 }  // namespace
 
 cudaError_t launch_step3d(bool fp64, bool pml, int idxw, const void* insts, const Tile3D* tiles, int ntiles, int par,
-                          int launch_off, int want_energy, cudaStream_t s) {
+                          int launch_off, int want_energy, WaitCtl wc, cudaStream_t s) {
     if (ntiles <= 0) return cudaSuccess;
     if (fp64)
-        return pml ? launch_idx<double, true>(idxw, insts, tiles, ntiles, par, launch_off, want_energy, s)
-                   : launch_idx<double, false>(idxw, insts, tiles, ntiles, par, launch_off, want_energy, s);
-    return pml ? launch_idx<float, true>(idxw, insts, tiles, ntiles, par, launch_off, want_energy, s)
-               : launch_idx<float, false>(idxw, insts, tiles, ntiles, par, launch_off, want_energy, s);
+        return pml ? launch_idx<double, true>(idxw, insts, tiles, ntiles, par, launch_off, want_energy, wc, s)
+                   : launch_idx<double, false>(idxw, insts, tiles, ntiles, par, launch_off, want_energy, wc, s);
+    return pml ? launch_idx<float, true>(idxw, insts, tiles, ntiles, par, launch_off, want_energy, wc, s)
+               : launch_idx<float, false>(idxw, insts, tiles, ntiles, par, launch_off, want_energy, wc, s);
 }
 
 }  // namespace orf

@@ -43,6 +43,15 @@ class Context:
         _lib.check(self._lib.orf_autotune2d(self.handle, len(ms), arr, int(steps), C.byref(t)), "autotune2d")
         return {"tsteps": t.tsteps, "variant": t.variant, "use_graph": bool(t.use_graph)}
 
+    def set_wait_injection(self, stall_plane: int = -1, wait_ns: int = 0) -> None:
+        """Bounds of the 3D kernel's device-side plane waits (wait_ns per
+        wait; 0 = one second) and the failure-detection test hook: with
+        stall_plane >= 0, 3D jobs created afterwards on this context never
+        load that z-plane of their tiles, so the wait runs out and the run
+        ends with orf:deviceTimeout (orf_ctx_set_wait_injection)."""
+        _lib.check(self._lib.orf_ctx_set_wait_injection(self.handle, int(stall_plane), int(wait_ns)),
+                   "orf_ctx_set_wait_injection")
+
     def set_timing(self, on: bool) -> None:
         _lib.check(self._lib.orf_ctx_set_timing(self.handle, 1 if on else 0))
 
@@ -116,6 +125,25 @@ def fdtd3D(sim, ctx: Context | None = None) -> dict:
     out = _abi.finish_out3d(m, o, bufs)
     _warn_nc(out, "fdtd3D")
     return out
+
+
+def plan2d(sim, tsteps: int = 0, variant: int = 0) -> dict:
+    """The tiles a 2D run of sim would use (orf_plan2d; host only, no
+    device): {"tsteps", "variant", "n_interior", "n_frame", "tiles"}, tiles
+    as a dict of int arrays (kind, li0, lk0, lx, lz, oi0, ok0, ow, oh, flags),
+    interior tiles first, indices 0-based."""
+    lib = _lib.load()
+    m = _abi.marshal_sim2d(sim)
+    t = _abi.OrfTuning(int(tsteps), int(variant), 1, 0)
+    ni, nf, T, v = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32()
+    _lib.check(lib.orf_plan2d(C.byref(m.struct), C.byref(t), None, 0, C.byref(ni), C.byref(nf), C.byref(T),
+                              C.byref(v)), "orf_plan2d")
+    n = ni.value + nf.value
+    arr = (_abi.OrfTile2D * max(1, n))()
+    _lib.check(lib.orf_plan2d(C.byref(m.struct), C.byref(t), arr, n, C.byref(ni), C.byref(nf), C.byref(T),
+                              C.byref(v)), "orf_plan2d")
+    tiles = {k: np.array([getattr(arr[q], k) for q in range(n)], dtype=np.int64) for k, _ in _abi.OrfTile2D._fields_}
+    return {"tsteps": T.value, "variant": v.value, "n_interior": ni.value, "n_frame": nf.value, "tiles": tiles}
 
 
 def fdtd2D_batch(sims, ctx: Context | None = None, progress=None, autotune: bool = False) -> list[dict]:

@@ -2,7 +2,9 @@
 memory at call time (their device memory belongs to their own pool, or they
 may not block on the allocator).  Its device state lives in a fixed static
 array inside the library, so this checks, through the C ABI, that two calls in
-a row each give the same result as the allocating orf_fdtd2d_run, and that an
+a row each give bitwise the result of the allocating orf_fdtd2d_run (the same
+kernels, the same launch order of the chunks), that after the first call on
+the device no further call changes the device's free memory, and that an
 oversized run is refused cleanly.  Kept in its own file, collected last."""
 import ctypes as C
 
@@ -13,8 +15,6 @@ from opticrcwafdtd_b200 import _abi, _lib, workloads
 from tests import cases
 
 pytestmark = pytest.mark.gpu
-
-TOL = 1e-9   # the DFT/flux tolerance of the parity tests
 
 
 def _run(sim, noalloc):
@@ -30,10 +30,14 @@ def _run(sim, noalloc):
 
 def _same(a, b):
     for k in ("flux", "fluxZ", "P", "B", "PZ", "AZ"):
-        if b[k].size:
-            scale = max(np.max(np.abs(b[k])), 1e-300)
-            assert np.max(np.abs(a[k] - b[k])) / scale <= TOL, k
+        assert np.array_equal(a[k], b[k]), k
     assert a["steps"] == b["steps"]
+    assert a["converged"] == b["converged"]
+
+
+def _free_bytes():
+    import torch
+    return torch.cuda.mem_get_info(0)[0]
 
 
 @pytest.mark.parametrize("make", [
@@ -49,6 +53,18 @@ def test_noalloc_matches_allocating_run_twice(make):
         st, out = _run(sim, noalloc=True)
         assert st == 0, _lib.last_error()
         _same(out, ref)
+
+
+def test_noalloc_takes_no_device_memory_after_the_first_call():
+    sim = cases.mixed_te_sim(nx=300, nz=160, steps=300, seed=24)
+    st, first = _run(sim, noalloc=True)        # the one-time set-up on this device
+    assert st == 0, _lib.last_error()
+    free0 = _free_bytes()
+    for _ in range(2):
+        st, out = _run(sim, noalloc=True)
+        assert st == 0, _lib.last_error()
+        _same(out, first)
+    assert _free_bytes() == free0
 
 
 def test_noalloc_rejects_runs_above_its_limit():
