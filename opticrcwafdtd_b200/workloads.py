@@ -218,6 +218,22 @@ def _coupler_instance(nx: int, nz: int, period: float, ff: float, etch: float, s
     return sim
 
 
+def coupler_instance_eta(out: dict, sim: dict, theta_deg=None, x_step: float = 0.5, w0: float = 5.2) -> np.ndarray:
+    """Fiber coupling efficiency of one coupler_batch_sims / serve_stream 2D
+    coupler from its DFT lines: Pinc = flux after the source + R with
+    R = -flux behind it, Pup = up-line flux / Pinc, and eta = overlap of the
+    up-line Ey with a tilted Gaussian fiber mode times Pup (fiberCoupling.m:16-31),
+    on a theta (default 5..15 deg) x fiber centre x lambda grid."""
+    from .coupler import fiberCoupling
+    pinc = out["flux"][1] - out["flux"][0]
+    res = dict(xUp=sim["x"], lambdas=np.asarray(sim["lambdas"]), EyUp=out["PZ"][:, :, 0],
+               Pup=out["fluxZ"][0] / pinc, nClad=N_SIO2)
+    th = np.arange(5.0, 15.01, 1.0) if theta_deg is None else np.asarray(theta_deg, dtype=float)
+    x0 = np.arange(3.0, sim["x"][-1] - 3.0, x_step)
+    eta, _ = fiberCoupling(res, np.deg2rad(th), x0, w0)
+    return eta
+
+
 def serve_stream(n_jobs: int = 32, seed: int = 5, rate: float = 1.0, cells=(2e5, 5e7), steps=(2000, 20000),
                  frac3d: float = 0.2, precision: str = "single", n_lambda: int = 21) -> list[dict]:
     """A served stream: Poisson arrivals (rate jobs/s) of mixed jobs, frac3d
