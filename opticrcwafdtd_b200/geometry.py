@@ -464,14 +464,11 @@ def _component(c, X, Y, Z, sh, nBg, h, d, off, NSub, Lx, Ly, Method):
                 # harmonic mean along c, then arithmetic over the other two
                 # axes, each sum sequential in index order (the GPU generator,
                 # csrc/eps3d.cu, adds in the same order: same bits)
+                # (np.cumsum accumulates left to right, one addition at a time)
                 inv = np.moveaxis(1.0 / es, 1 + c, 1)                   # (m, along, r1, r2)
-                acc = inv[:, 0]
-                for a in range(1, NSub):
-                    acc = acc + inv[:, a]
+                acc = np.cumsum(inv, axis=1)[:, -1]
                 r = (1.0 / (acc / NSub)).reshape(mq, NSub * NSub)
-                tot = r[:, 0]
-                for q in range(1, NSub * NSub):
-                    tot = tot + r[:, q]
+                tot = np.cumsum(r, axis=1)[:, -1]
                 val[q0:q1] = tot / (NSub * NSub)
             elif Method == "kottke":
                 # sums sequential over the samples in row-major (x, y, z)
@@ -481,13 +478,9 @@ def _component(c, X, Y, Z, sh, nBg, h, d, off, NSub, Lx, Ly, Method):
                 n3 = NSub ** 3
                 q3 = np.arange(n3)
                 w = [off[q3 // (NSub * NSub)], off[(q3 // NSub) % NSub], off[q3 % NSub]]
-                se, si = flat[:, 0], inv[:, 0]
-                grads = [flat[:, 0] * w[ax][0] for ax in range(3)]
-                for q in range(1, n3):
-                    se = se + flat[:, q]
-                    si = si + inv[:, q]
-                    for ax in range(3):
-                        grads[ax] = grads[ax] + flat[:, q] * w[ax][q]
+                se = np.cumsum(flat, axis=1)[:, -1]
+                si = np.cumsum(inv, axis=1)[:, -1]
+                grads = [np.cumsum(flat * w[ax][None, :], axis=1)[:, -1] for ax in range(3)]
                 mean_e, mean_inv = se / n3, si / n3
                 gn = np.sqrt(sum(g * g for g in grads))
                 nc2 = np.where(gn > 0, (grads[c] / np.where(gn > 0, gn, 1.0)) ** 2, 0.0)
