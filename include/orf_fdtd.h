@@ -242,6 +242,24 @@ typedef struct orf_tile2d {
 ORF_API int32_t orf_plan2d(const orf_sim2d* sim, const orf_tuning* tuning, orf_tile2d* tiles, int32_t cap,
                            int32_t* n_interior, int32_t* n_frame, int32_t* tsteps, int32_t* variant);
 
+/* One tile of a 3D run's plan (orf_plan3d): a CTA marches the tw x th column
+ * at (i0, j0) through the z planes [k0, k1).  kind 0: interior tile (no CPML
+ * code), 1: CPML tile.  tma: 1 when its planes arrive by TMA tensor copies
+ * (every tile whose halo does not wrap around a periodic x / y edge), whose
+ * boxes start at x = tma_x (fields) and x = tma_index_x (material index). */
+typedef struct orf_tile3d {
+    int32_t kind;
+    int32_t i0, j0, tw, th, k0, k1;
+    int32_t tma, tma_x, tma_index_x;
+} orf_tile3d;
+
+/* No counterpart in the reference.  Host-only view of the tiles a 3D run of
+ * `sim` would use, interior tiles first; needs no device.  Counts always
+ * written; tiles when tiles != NULL and cap holds them all (ORF_ETOOLARGE
+ * when cap > 0 is too small). */
+ORF_API int32_t orf_plan3d(const orf_sim3d* sim, orf_tile3d* tiles, int32_t cap, int32_t* n_interior,
+                           int32_t* n_cpml);
+
 /* ------------------------------------------------------------ 2D runs --- */
 /* Element counts of the caller-allocated out arrays (complex counts are in
  * complex elements; allocate twice as many doubles). */

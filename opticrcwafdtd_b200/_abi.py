@@ -99,6 +99,10 @@ class OrfTile2D(C.Structure):
     _fields_ = [(k, C.c_int32) for k in ("kind", "li0", "lk0", "lx", "lz", "oi0", "ok0", "ow", "oh", "flags")]
 
 
+class OrfTile3D(C.Structure):
+    _fields_ = [(k, C.c_int32) for k in ("kind", "i0", "j0", "tw", "th", "k0", "k1", "tma", "tma_x", "tma_index_x")]
+
+
 class OrfKernelStats(C.Structure):
     _fields_ = [("interior_ms", C.c_double), ("interior_launches", C.c_int64),
                 ("interior_cell_updates", C.c_int64),

@@ -54,6 +54,7 @@ _SIGS = {
     "orf_autotune2d": (C.c_int32, [C.c_void_p, C.c_int32, P(_abi.OrfSim2D), C.c_int32, P(_abi.OrfTuning)]),
     "orf_plan2d": (C.c_int32, [P(_abi.OrfSim2D), P(_abi.OrfTuning), P(_abi.OrfTile2D), C.c_int32, P(C.c_int32),
                                P(C.c_int32), P(C.c_int32), P(C.c_int32)]),
+    "orf_plan3d": (C.c_int32, [P(_abi.OrfSim3D), P(_abi.OrfTile3D), C.c_int32, P(C.c_int32), P(C.c_int32)]),
     "orf_serve_open": (C.c_int32, [C.c_void_p, P(_abi.OrfServeCfg), P(C.c_void_p)]),
     "orf_serve_submit2d": (C.c_int32, [C.c_void_p, P(_abi.OrfSim2D), P(_abi.OrfOut2D), P(C.c_int64)]),
     "orf_serve_submit3d": (C.c_int32, [C.c_void_p, P(_abi.OrfSim3D), P(_abi.OrfOut3D), P(C.c_int64)]),

@@ -1,6 +1,7 @@
 // capi.cu -- the extern "C" entry points of liborf_fdtd.so (include/orf_fdtd.h).
 #include "engine.cuh"
 #include "job2d.cuh"
+#include "job3d.cuh"
 
 using namespace orf;
 
@@ -291,6 +292,31 @@ int32_t orf_plan2d(const orf_sim2d* sim, const orf_tuning* tuning, orf_tile2d* t
             fast2d_info(p.fvariant, sim->precision == ORF_DOUBLE, false, &v);
             tiles[q].lz = v.lz();
         }
+    }
+    return ORF_OK;
+}
+
+int32_t orf_plan3d(const orf_sim3d* sim, orf_tile3d* tiles, int32_t cap, int32_t* n_interior, int32_t* n_cpml) {
+    ORF_TRY(validate3d(sim));
+    std::vector<Tile3D> ti, tp;
+    plan3d(sim, ti, tp);
+    if (n_interior) *n_interior = (int32_t)ti.size();
+    if (n_cpml) *n_cpml = (int32_t)tp.size();
+    const size_t n = ti.size() + tp.size();
+    if (!tiles) return ORF_OK;
+    if ((size_t)cap < n) {
+        set_error("orf_plan3d: %zu tiles, room for %d", n, cap);
+        return cap > 0 ? ORF_ETOOLARGE : ORF_OK;
+    }
+    const bool px = sim->periodic[0] != 0, py = sim->periodic[1] != 0;
+    for (size_t q = 0; q < n; ++q) {
+        const bool pml = q >= ti.size();
+        const Tile3D& t = pml ? tp[q - ti.size()] : ti[q];
+        // the kernel's choice (step3d_fused.cu): TMA unless the halo wraps
+        const bool wrapx = px && (t.i0 == 0 || t.i0 + kTile3X >= sim->nx);
+        const bool wrapy = py && (t.j0 == 0 || t.j0 + kTile3Y >= sim->ny);
+        tiles[q] = orf_tile3d{pml ? 1 : 0, t.i0, t.j0, t.tw, t.th, t.k0, t.k1, (wrapx || wrapy) ? 0 : 1,
+                              t.i0 - 4, t.i0};
     }
     return ORF_OK;
 }

@@ -130,6 +130,49 @@ int Job3D<R>::encode_tmap3(CUtensorMap* m, CUtensorMapDataType t, const void* ba
     return ORF_OK;
 }
 
+// Host-only plan of a 3D run's tiles: kTile3X x kTile3Y columns, a segment
+// of up to kSeg3 planes each; a tile takes the CPML instantiation if any cell
+// it updates or recomputes (one halo cell in x and y, the plane below the
+// segment) lies within one cell of an absorbing slab along any axis.  z
+// segments of at most kSeg3 planes never mix planes near a z slab with planes
+// away from it, so only the planes that need CPML code run it.  Needs no
+// device; orf_plan3d exposes it for checks of the tiling.
+void plan3d(const orf_sim3d* s, std::vector<Tile3D>& tiles, std::vector<Tile3D>& tiles_pml) {
+    const int n[3] = {s->nx, s->ny, s->nz};
+    bool per[3];
+    for (int q = 0; q < 3; ++q) per[q] = s->periodic[q] != 0;
+    tiles.clear();
+    tiles_pml.clear();
+    auto near_pml = [&](int q, int lo, int hi) {   // cells [lo, hi) along axis q
+        const int np = per[q] ? 0 : s->npml[q];
+        if (np <= 0) return false;
+        return lo < np + 1 || hi > n[q] - np - 2;
+    };
+    std::vector<std::pair<int, int>> segs;
+    for (int k0 = 0; k0 < n[2];) {
+        const bool pz0 = near_pml(2, k0 - 1, k0 + 2);
+        int k1 = k0 + 1;
+        while (k1 < n[2] && k1 - k0 < kSeg3 && near_pml(2, k1 - 1, k1 + 2) == pz0) ++k1;
+        segs.push_back({k0, k1});
+        k0 = k1;
+    }
+    for (auto [k0, k1] : segs)
+        for (int j0 = 0; j0 < n[1]; j0 += kTile3Y)
+            for (int i0 = 0; i0 < n[0]; i0 += kTile3X) {
+                Tile3D t;
+                t.inst = 0;
+                t.i0 = i0;
+                t.j0 = j0;
+                t.tw = (short)std::min(kTile3X, n[0] - i0);
+                t.th = (short)std::min(kTile3Y, n[1] - j0);
+                t.k0 = k0;
+                t.k1 = k1;
+                const bool pm = near_pml(0, t.i0 - 1, t.i0 + t.tw + 1) || near_pml(1, t.j0 - 1, t.j0 + t.th + 1) ||
+                                near_pml(2, t.k0 - 1, t.k1 + 1);
+                (pm ? tiles_pml : tiles).push_back(t);
+            }
+}
+
 template <class R>
 int Job3D<R>::create(const orf_sim3d* s) {
     ORF_TRY(validate3d(s));
@@ -240,43 +283,9 @@ int Job3D<R>::create(const orf_sim3d* s) {
         pairs.push_back({4 * m, 4 * m + 3, 4 * m + 1, 4 * m + 2, m, nM, 0.5 * d * d});
     npairs = (int)pairs.size();
 
-    // ---- tiles: kTile3X x kTile3Y columns, a segment of up to kSeg3 planes
-    // each; a tile takes the CPML instantiation if any cell it updates or
-    // recomputes (one halo cell in x and y, the plane below the segment) lies
-    // within one cell of an absorbing slab along any axis
-    tiles.clear();
-    tiles_pml.clear();
-    auto near_pml = [&](int q, int lo, int hi) {   // cells [lo, hi) along axis q
-        const int np = per[q] ? 0 : s->npml[q];
-        if (np <= 0) return false;
-        return lo < np + 1 || hi > n[q] - np - 2;
-    };
+    // ---- tiles (plan3d)
+    plan3d(s, tiles, tiles_pml);
     zc = kSeg3;
-    // z segments of at most kSeg3 planes that never mix planes near a z slab
-    // with planes away from it, so only the planes that need CPML code run it
-    std::vector<std::pair<int, int>> segs;
-    for (int k0 = 0; k0 < n[2];) {
-        const bool pz0 = near_pml(2, k0 - 1, k0 + 2);
-        int k1 = k0 + 1;
-        while (k1 < n[2] && k1 - k0 < kSeg3 && near_pml(2, k1 - 1, k1 + 2) == pz0) ++k1;
-        segs.push_back({k0, k1});
-        k0 = k1;
-    }
-    for (auto [k0, k1] : segs)
-        for (int j0 = 0; j0 < n[1]; j0 += kTile3Y)
-            for (int i0 = 0; i0 < n[0]; i0 += kTile3X) {
-                Tile3D t;
-                t.inst = 0;
-                t.i0 = i0;
-                t.j0 = j0;
-                t.tw = (short)std::min(kTile3X, n[0] - i0);
-                t.th = (short)std::min(kTile3Y, n[1] - j0);
-                t.k0 = k0;
-                t.k1 = k1;
-                const bool pm = near_pml(0, t.i0 - 1, t.i0 + t.tw + 1) || near_pml(1, t.j0 - 1, t.j0 + t.th + 1) ||
-                                near_pml(2, t.k0 - 1, t.k1 + 1);
-                (pm ? tiles_pml : tiles).push_back(t);
-            }
 
     // ---- device arena
     // fields and psi ping-pong: a step reads buffer par and writes par^1

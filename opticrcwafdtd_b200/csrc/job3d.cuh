@@ -6,6 +6,9 @@
 
 namespace orf {
 
+// Host-only tile plan of a 3D run (job3d.cu): interior tiles and CPML tiles.
+void plan3d(const orf_sim3d* s, std::vector<Tile3D>& tiles, std::vector<Tile3D>& tiles_pml);
+
 template <class R>
 struct Job3D : orf_job {
     int n[3] = {0, 0, 0};

@@ -146,6 +146,21 @@ def plan2d(sim, tsteps: int = 0, variant: int = 0) -> dict:
     return {"tsteps": T.value, "variant": v.value, "n_interior": ni.value, "n_frame": nf.value, "tiles": tiles}
 
 
+def plan3d(sim) -> dict:
+    """The tiles a 3D run of sim would use (orf_plan3d; host only):
+    {"n_interior", "n_cpml", "tiles"}, tiles as a dict of int arrays (kind,
+    i0, j0, tw, th, k0, k1, tma, tma_x, tma_index_x), interior tiles first."""
+    lib = _lib.load()
+    m = _abi.marshal_sim3d(sim)
+    ni, nc = C.c_int32(), C.c_int32()
+    _lib.check(lib.orf_plan3d(C.byref(m.struct), None, 0, C.byref(ni), C.byref(nc)), "orf_plan3d")
+    n = ni.value + nc.value
+    arr = (_abi.OrfTile3D * max(1, n))()
+    _lib.check(lib.orf_plan3d(C.byref(m.struct), arr, n, C.byref(ni), C.byref(nc)), "orf_plan3d")
+    tiles = {k: np.array([getattr(arr[q], k) for q in range(n)], dtype=np.int64) for k, _ in _abi.OrfTile3D._fields_}
+    return {"n_interior": ni.value, "n_cpml": nc.value, "tiles": tiles}
+
+
 def fdtd2D_batch(sims, ctx: Context | None = None, progress=None, autotune: bool = False) -> list[dict]:
     """Run many 2D sims (same precision; TE and TM may mix) together: one
     persistent-kernel launch per fused step block advances every instance of

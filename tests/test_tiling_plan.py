@@ -136,3 +136,67 @@ def test_one_frame_tile_row_covers_the_cpml_strip():
     assert np.all(t["ok0"][bottom] == 0) and np.all(t["lk0"][bottom] == 0) and np.all(t["oh"][bottom] == 32)
     top = fr & (t["ok0"] + t["oh"] > 268)
     assert np.all(t["ok0"][top] == 268) and np.all(t["lk0"][top] + 40 == 300)
+
+
+# --------------------------------------------------------------------- 3D ---
+def _sim3d(n, npml, per):
+    d = 0.04
+    x, y, z = (np.arange(m) * d for m in n)
+    src = dict(axis=3, index=max(2, npml[2] + 2) if not per[2] else 3, Ea=1.0, Hb=1.0, lambda0=0.6)
+    return dict(x=x, y=y, z=z, eps={c: np.ones(n) for c in "xyz"}, npml=list(npml), periodic=list(per),
+                source=src, lambdas=[0.6], monitors=[], maxTime=1.0, shutoff=0.0)
+
+
+def _check3d(sim):
+    from opticrcwafdtd_b200.fdtd import plan3d
+    p = plan3d(sim)
+    t = p["tiles"]
+    n = (sim["x"].size, sim["y"].size, sim["z"].size)
+    per = [bool(v) for v in sim["periodic"]]
+    npml = [0 if per[q] else int(sim["npml"][q]) for q in range(3)]
+    cover = np.zeros(n, dtype=np.int32)
+    for q in range(t["kind"].size):
+        kind, i0, j0, tw, th, k0, k1, tma, tx, tix = (int(t[k][q]) for k in
+                                                      ("kind", "i0", "j0", "tw", "th", "k0", "k1", "tma", "tma_x",
+                                                       "tma_index_x"))
+        assert i0 % 32 == 0 and j0 % 8 == 0 and 1 <= tw <= 32 and 1 <= th <= 8, q
+        assert 1 <= k1 - k0 <= 60, ("segment longer than the kernel's 64-bit plane mask allows", q)
+        cover[i0:i0 + tw, j0:j0 + th, k0:k1] += 1
+        if tma:
+            # a TMA tile's halo (one cell each side in x and y) must not wrap ...
+            if per[0]:
+                assert i0 - 1 >= 0 and i0 + 32 < n[0], q
+            if per[1]:
+                assert j0 - 1 >= 0 and j0 + 8 < n[1], q
+            # ... and every box must start on a 16-byte boundary in x
+            for esz in (4, 8):
+                assert (tx * esz) % 16 == 0, (q, tx, esz)
+            for isz in (1, 2, 4):
+                assert (tix * isz) % 16 == 0, (q, tix, isz)
+        else:
+            assert (per[0] and (i0 == 0 or i0 + 32 >= n[0])) or (per[1] and (j0 == 0 or j0 + 8 >= n[1])), q
+        if kind == 0:
+            # interior: every cell it updates or recomputes (halo of one cell,
+            # the plane below the segment) keeps a cell of distance from the
+            # slabs of E (u < np, u >= n - np) and H (u >= n - 1 - np)
+            region = [(i0 - 1, i0 + tw + 1), (j0 - 1, j0 + th + 1), (k0 - 1, k1 + 1)]
+            for ax, (lo, hi) in enumerate(region):
+                if npml[ax] > 0:
+                    assert lo - 1 >= npml[ax] and hi + 1 <= n[ax] - 1 - npml[ax], ("interior tile near a slab", q, ax)
+    assert np.all(cover == 1)
+    return p
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_random_3d_plans(seed):
+    rng = np.random.default_rng(2000 + seed)
+    for _ in range(12):
+        n = tuple(int(v) for v in rng.integers(10, 170, 3))
+        per = tuple(bool(v) for v in rng.random(3) < 0.4)
+        npml = tuple(int(rng.integers(0, max(1, min(12, (m - 4) // 2)))) for m in n)
+        _check3d(_sim3d(n, npml, per))
+
+
+def test_pillar_lattice_3d_plan():
+    p = _check3d(_sim3d((600, 600, 300), (0, 0, 20), (True, True, False)))
+    assert p["n_interior"] > 0 and p["n_cpml"] > 0
