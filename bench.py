@@ -542,7 +542,7 @@ def bench_coupler_batch(args, rank, world, local, dist):
                            "timed_path": "host sims -> device -> results on host (end to end)"},
                 "jobs_per_s": args.batch * args.steps * world / te,
                 "roofline": roof, "whole_job_roofline": _whole_frac(value * 1e6, bpc),
-                "eta_err_vs_fp64": eta_err, "clocks": clk.summary(),
+                "eta_err_vs_fp64": eta_err, "clocks": clk.summary(), "tuning_choice": getattr(ctx, "tuned", None),
                 "host_phase_ms": {"setup": st["setup_ms"], "loop": st["loop_ms"], "finish": st["finish_ms"]}}
     ctx.close()
     return line
@@ -578,9 +578,15 @@ def bench_serve(args, rank, world, local, dist):
     from opticrcwafdtd_b200 import Context, Server, fdtd2D_batch, fdtd3D, workloads
     warnings.simplefilter("ignore")
     cells = (2e5, args.serve_max_cells)
-    stream_jobs = workloads.serve_stream(n_jobs=args.serve_jobs, rate=1.0, seed=5 + rank, cells=cells)
-    cu = [j["cells"] * j["steps"] for j in stream_jobs]
     ctx = Context(local, stream=torch.cuda.current_stream().cuda_stream)
+    phase = {}
+    t = time.perf_counter()
+    # 3D permittivities from the GPU generator (bitwise the host generator's)
+    stream_jobs = workloads.serve_stream(n_jobs=args.serve_jobs, rate=1.0, seed=5 + rank, cells=cells, device=ctx)
+    cap_jobs = workloads.serve_stream(n_jobs=args.serve_capacity_jobs, rate=1.0, seed=1000 + rank, cells=cells,
+                                      device=ctx)
+    phase["build_sims"] = time.perf_counter() - t
+    cu = [j["cells"] * j["steps"] for j in stream_jobs]
     # warm the kernels once on a small job of each kind
     warm = workloads.serve_stream(n_jobs=4, seed=99, cells=(2e5, 4e5), steps=(200, 300), frac3d=0.5)
     srv = Server(ctx, macro_steps=args.serve_macro)
@@ -589,10 +595,11 @@ def bench_serve(args, rank, world, local, dist):
     srv.drain()
     srv.close()
     # capacity: a sample of the same distribution submitted all at once
-    cap_jobs = workloads.serve_stream(n_jobs=args.serve_capacity_jobs, rate=1.0, seed=1000 + rank, cells=cells)
+    t = time.perf_counter()
     srv = Server(ctx, macro_steps=args.serve_macro)
     _, cap_span = _serve_run(srv, cap_jobs, [0.0] * len(cap_jobs))
     srv.close()
+    phase["capacity"] = time.perf_counter() - t
     cap_cu_s = sum(j["cells"] * j["steps"] for j in cap_jobs) / cap_span
     capacity = cap_cu_s / (sum(cu) / len(cu))   # jobs/s of this stream's mean job
     rate = args.serve_rate if args.serve_rate > 0 else args.serve_load * capacity
@@ -601,8 +608,11 @@ def bench_serve(args, rank, world, local, dist):
     srv = Server(ctx, macro_steps=args.serve_macro)
     _barrier(dist)
     torch.cuda.synchronize()
+    t = time.perf_counter()
     with ClockSampler(local) as clk:
         tickets, span = _serve_run(srv, stream_jobs, t_arr)
+    phase["stream"] = time.perf_counter() - t
+    t = time.perf_counter()
     infos = [srv.info(t) for t in tickets]
     lat = np.array([i["t_done"] - i["t_submit"] for i in infos])
     bytes_alg = sum(c * (BYTES_3D["single"] if j["dims"] == 3 else 25) for c, j in zip(cu, stream_jobs))
@@ -630,6 +640,7 @@ def bench_serve(args, rank, world, local, dist):
         t_errs.append(float(np.max(np.abs(f32 - f64)) / max(1e-300, np.max(np.abs(f64)))))
     srv.close()
     ctx.close()
+    phase["fp64_checks"] = time.perf_counter() - t
     if rank != 0:
         return None
     n2 = len(idx2)
@@ -655,7 +666,7 @@ def bench_serve(args, rank, world, local, dist):
                                 "sample": f"every {k}-th 2D coupler job, FP64 batched run on the GPU"},
             "flux_T_err_vs_fp64_3d": {"jobs": len(t_errs), "max": max(t_errs) if t_errs else None,
                                       "sample": "the two smallest 3D jobs, T = flux / largest |flux|"},
-            "clocks": clk.summary()}
+            "phase_s": phase, "clocks": clk.summary()}
 
 
 WORKLOADS = {"pixel2d": bench_pixel2d, "coupler": bench_pixel2d, "pillar3d": bench_pillar3d,

@@ -10,12 +10,15 @@
 //   submit  copies the sim (all arrays) into a FIFO queue and returns a ticket;
 //   step    (one scheduling round) admits queued jobs in FIFO order while
 //           their device arenas fit the budget, adds each to the group of
-//           resident jobs sharing its kernel configuration (group.cuh), runs
-//           up to macro_steps time steps of every group -- each group on its
-//           own stream, so 2D and 3D groups overlap -- and retires the jobs
-//           whose device state reports done (shutoff or step budget): their
-//           results go to the caller's out struct, their memory back to the
-//           budget;
+//           resident jobs sharing its kernel configuration and size class
+//           (group.cuh; a class spans a factor of 4 in cells), runs chunks of
+//           every group -- each group on its own stream, so groups overlap --
+//           and retires the jobs whose device state reports done (shutoff or
+//           step budget): their results go to the caller's out struct, their
+//           memory back to the budget.  The group whose chunk costs most runs
+//           macro_steps time steps per round; a group of smaller jobs runs
+//           proportionally more chunks (at most half the status ring), so
+//           small jobs are not held to the pace of the largest ones;
 //   poll    reports a finished ticket with its submit/admit/done times.
 //
 // A job is admitted only between chunks and starts from zeroed fields, so its
@@ -136,6 +139,36 @@ struct orf_server {
         }
     }
 
+    // size class of a job: floor(log4(cells))
+    static int64_t size_class(int64_t cells) {
+        int64_t c = 0;
+        while (cells >= 4) {
+            cells >>= 2;
+            ++c;
+        }
+        return c;
+    }
+
+    // chunks of each group in this round: the group whose chunk costs most
+    // (cells x the rough cost of a cell update of its kind; only the ratios
+    // matter) runs chunks_per_step, cheaper ones proportionally more, up to
+    // half the status ring read between rounds
+    void plan_round(std::vector<int>& nch) const {
+        nch.assign(groups.size(), chunks_per_step);
+        std::vector<double> cost(groups.size());
+        double top = 0.0;
+        for (size_t q = 0; q < groups.size(); ++q) {
+            const bool is3d = (groups[q].key & 3) == 3;
+            cost[q] = (double)groups[q].g->cells() * (is3d ? 2.0 : 1.0);
+            top = std::max(top, cost[q]);
+        }
+        for (size_t q = 0; q < groups.size(); ++q) {
+            const double r = cost[q] > 0 ? top / cost[q] : 1.0;
+            nch[q] = (int)std::min<double>(kStatusRing / 2, std::max<double>(chunks_per_step,
+                                                                              std::floor(chunks_per_step * r)));
+        }
+    }
+
     Group* group_for(int64_t key) {
         for (auto& s : groups)
             if (s.key == key) return s.g.get();
@@ -167,7 +200,7 @@ struct orf_server {
             return st;
         }
         const int64_t key = 2 | (int64_t)(sizeof(R) == 8) << 2 | (int64_t)j->te << 3 | (int64_t)j->idx16 << 4 |
-                            (int64_t)j->T << 8 | (int64_t)j->fvariant << 16;
+                            (int64_t)j->T << 8 | (int64_t)j->fvariant << 16 | size_class(j->cells()) << 24;
         Group* g = group_for(key);
         if (!g) {
             ORF_TRY(new_group(key, std::make_unique<Group2D<R>>()));
@@ -191,7 +224,8 @@ struct orf_server {
             *fits = !((st == ORF_ETOOLARGE && j->need > left) || st == ORF_ENOMEM_DEVICE);
             return st;
         }
-        const int64_t key = 3 | (int64_t)(sizeof(R) == 8) << 2 | (int64_t)j->idxw << 8 | (int64_t)j->zc << 16;
+        const int64_t key = 3 | (int64_t)(sizeof(R) == 8) << 2 | (int64_t)j->idxw << 8 | (int64_t)j->zc << 16 |
+                            size_class(j->cells()) << 24;
         Group* g = group_for(key);
         if (!g) {
             ORF_TRY(new_group(key, std::make_unique<Group3D<R>>()));
@@ -348,7 +382,9 @@ struct orf_server {
             if (groups[q].g->dirty) ORF_TRY(groups[q].g->build(groups[q].stream));
             ++q;
         }
-        for (auto& s : groups) ORF_TRY(s.g->enqueue(chunks_per_step, s.stream));
+        std::vector<int> nch;
+        plan_round(nch);
+        for (size_t q = 0; q < groups.size(); ++q) ORF_TRY(groups[q].g->enqueue(nch[q], groups[q].stream));
         for (auto& s : groups) ORF_CUDA(cudaStreamSynchronize(s.stream));
         for (auto& s : groups) s.g->eng.collect_timing();
         return retire();

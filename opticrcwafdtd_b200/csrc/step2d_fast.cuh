@@ -176,20 +176,43 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
         const R* gP = reinterpret_cast<const R*>(d.f[par][0]);
         const R* gA = reinterpret_cast<const R*>(d.f[par][1]);
         const R* gB = reinterpret_cast<const R*>(d.f[par][2]);
-        const int i = d.li0 + cx;
-        const bool cv = !PML || (i >= 0 && i < d.nx);
-        const int col = PML ? min(max(i, 0), d.nx - 1) : min(i, d.pitch - 1);
+        if constexpr (!PML) {
+            // interior tiles: 16-byte chunks of rows (li0 is a multiple of 4
+            // cells and the pitch of 32, so every chunk is 16-byte aligned);
+            // chunks past the row end are clamped onto its last chunk, cells
+            // no output's dependency cone reaches
+            constexpr int VE = 16 / (int)sizeof(R);
+            constexpr int CPR = LX / VE;
+            constexpr int NCH = LZ * CPR;
+            static_assert(NCH % NT == 0, "whole chunks per thread");
 #pragma unroll
-        for (int j = 0; j < KS; ++j) {
-            const int row = d.lk0 + ck0 + j;
-            const bool rv = d.periodic || (row >= 0 && row < d.nz);
-            const int kk = d.periodic ? pmod(row, d.nz) : min(max(row, 0), d.nz - 1);
-            const size_t off = (size_t)kk * d.pitch + col;
-            const int c = (ck0 + j) * LX + cx;
-            const bool v = !PML || (cv && rv);
-            cp_field(pfP + c, gP + off, v);
-            cp_field(pfA + c, gA + off, v);
-            cp_field(pfB + c, gB + off, v);
+            for (int r = 0; r < NCH / NT; ++r) {
+                const int c = (int)threadIdx.x + r * NT;
+                const int row = c / CPR, cc = c - row * CPR;
+                const int grow = d.lk0 + row;
+                const int kk = d.periodic ? pmod(grow, d.nz) : min(max(grow, 0), d.nz - 1);
+                const size_t off = (size_t)kk * d.pitch + min(d.li0 + VE * cc, d.pitch - VE);
+                const int s = row * LX + VE * cc;
+                cp_async16(pfP + s, gP + off);
+                cp_async16(pfA + s, gA + off);
+                cp_async16(pfB + s, gB + off);
+            }
+        } else {
+            const int i = d.li0 + cx;
+            const bool cv = i >= 0 && i < d.nx;
+            const int col = min(max(i, 0), d.nx - 1);
+#pragma unroll
+            for (int j = 0; j < KS; ++j) {
+                const int row = d.lk0 + ck0 + j;
+                const bool rv = d.periodic || (row >= 0 && row < d.nz);
+                const int kk = d.periodic ? pmod(row, d.nz) : min(max(row, 0), d.nz - 1);
+                const size_t off = (size_t)kk * d.pitch + col;
+                const int c = (ck0 + j) * LX + cx;
+                const bool v = cv && rv;
+                cp_field(pfP + c, gP + off, v);
+                cp_field(pfA + c, gA + off, v);
+                cp_field(pfB + c, gB + off, v);
+            }
         }
         // material index rows: 4-byte copies (li0 and pitch are multiples of 4 cells)
         constexpr int W4 = LX * (int)sizeof(IT) / 4;

@@ -184,6 +184,7 @@ def fdtd2D_batch(sims, ctx: Context | None = None, progress=None, autotune: bool
         sarr = (_abi.OrfSim2D * len(sample))(*[m.struct for m in sample])
         t = _abi.OrfTuning()
         _lib.check(lib.orf_autotune2d(ctx.handle, len(sample), sarr, 1000, C.byref(t)), "autotune2d")
+        ctx.tuned = {"tsteps": t.tsteps, "variant": t.variant}   # the choice, for reports
     cb, box = _abi.make_progress(progress)
     st = lib.orf_batch2d_run(ctx.handle, len(ms), arr, oarr, cb or _abi.PROGRESS_FN(0), None)
     if own:

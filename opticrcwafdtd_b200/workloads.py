@@ -235,12 +235,13 @@ def coupler_instance_eta(out: dict, sim: dict, theta_deg=None, x_step: float = 0
 
 
 def serve_stream(n_jobs: int = 32, seed: int = 5, rate: float = 1.0, cells=(2e5, 5e7), steps=(2000, 20000),
-                 frac3d: float = 0.2, precision: str = "single", n_lambda: int = 21) -> list[dict]:
+                 frac3d: float = 0.2, precision: str = "single", n_lambda: int = 21, device=None) -> list[dict]:
     """A served stream: Poisson arrivals (rate jobs/s) of mixed jobs, frac3d
     of them 3D pillar lattices and the rest 2D grating couplers, cell counts
     log-uniform in [cells], step budgets uniform in [steps] (shutoff off, so
     every job runs its budget).  Returns [{"t", "dims", "cells", "steps",
-    "sim"}] in arrival order."""
+    "sim"}] in arrival order.  device: as in pillar_lattice_sim (the 3D
+    permittivity from the GPU generator, the same values as the host's)."""
     rng = np.random.default_rng(seed)
     t = 0.0
     jobs = []
@@ -254,7 +255,7 @@ def serve_stream(n_jobs: int = 32, seed: int = 5, rate: float = 1.0, cells=(2e5,
             nz = max(120, int(round((nc / 4) ** (1 / 3))))
             nxy = max(20, int(round(math.sqrt(nc / nz) / 20)) * 20)
             sim = pillar_lattice_sim(nx=nxy, ny=nxy, nz=nz, seed=int(rng.integers(1 << 30)), steps=st,
-                                     precision=precision, n_lambda=3)
+                                     precision=precision, n_lambda=3, device=device)
             jobs.append(dict(t=t, dims=3, cells=nxy * nxy * nz, steps=st, sim=sim))
         else:
             nz = max(150, int(round(math.sqrt(nc / 3))))

@@ -12,7 +12,7 @@ at their full grid sizes (the other parity tests use small grids).
       reads the same budget).
 
 Bars: fields within 1e-10 relative L2; every DFT line within 1e-9 of its
-largest magnitude; the monitored transmission T = flux / incident flux
+largest magnitude (3D: of the plane's largest E or H); the monitored transmission T = flux / incident flux
 within 1e-9 absolute.  Where the run covers the whole pulse (C1, C4) the
 incident flux is the one through the monitor just after the source, per
 wavelength; C2 and C3 stop on the rising edge of the pulse, where a
@@ -112,8 +112,17 @@ def test_c3_pillar_lattice_fp64_full_grid():
         a, b = out["fields"].pop(0), ref["fields"].pop(0)
         assert _rel_l2(a, b) <= FIELD_TOL, ("EH"[q // 3] + "xyz"[q % 3], _rel_l2(a, b))
         del a, b
+    # each plane's E lines against the plane's largest E, its H lines against
+    # its largest H: a component that vanishes by symmetry on a plane (Ey of
+    # the x-polarised wave behind the source reads 1e-18 of Ex, rounding
+    # noise that a 1e-15 change of the source amplitude moves by its own
+    # size) is compared on the scale of the field there
     for mo, mr in zip(out["mon"], ref["mon"]):
-        _check_lines(mo, mr, ("Ea", "Eb", "Ha", "Hb"))
+        for pair in (("Ea", "Eb"), ("Ha", "Hb")):
+            s = max(max(np.max(np.abs(mr[k])) for k in pair), 1e-300)
+            for k in pair:
+                err = np.max(np.abs(mo[k] - mr[k])) / s
+                assert err <= LINE_TOL, (k, err)
     _check_transmission(out, ref, np.max(np.abs(ref["flux"])), keys=("flux",))
 
 
