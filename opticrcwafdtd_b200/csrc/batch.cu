@@ -12,6 +12,8 @@
 // instance's tiles turn into no-ops.  Instances of both polarisations, or
 // with more than 256 distinct permittivities, fall into further groups.
 #include <algorithm>
+#include <string>
+#include <thread>
 
 #include "group.cuh"
 
@@ -21,20 +23,37 @@ namespace {
 template <class R>
 int run_batch(orf_ctx* ctx, int n, const orf_sim2d* sims, orf_out2d* outs, orf_progress_fn progress, void* user) {
     double t0 = now_s();
-    std::vector<std::unique_ptr<Job2D<R>>> jobs;
-    jobs.reserve(n);
-    for (int q = 0; q < n; ++q) {
-        auto j = std::make_unique<Job2D<R>>();
-        j->ctx = ctx;
-        const int st = j->create(&sims[q]);
-        if (st != ORF_OK) {
-            char buf[600];
-            std::snprintf(buf, sizeof buf, "instance %d: %s", q + 1, last_error());
-            set_error("%s", buf);
-            return st;
+    // instance set-up (host tables, tile plans, device blocks, uploads) on
+    // several host threads: create() is safe to run concurrently (its errors
+    // are per thread, the block cache and the byte counter take locks)
+    std::vector<std::unique_ptr<Job2D<R>>> jobs(n);
+    std::vector<int> status(n, ORF_OK);
+    std::vector<std::string> why(n);
+    const int nthreads = (int)std::max(1u, std::min<unsigned>({16u, std::thread::hardware_concurrency(), (unsigned)n}));
+    auto work = [&](int tid) {
+        for (int q = tid; q < n; q += nthreads) {
+            auto j = std::make_unique<Job2D<R>>();
+            j->ctx = ctx;
+            status[q] = j->create(&sims[q]);
+            if (status[q] != ORF_OK) {
+                why[q] = last_error();
+                continue;
+            }
+            jobs[q] = std::move(j);
         }
-        jobs.push_back(std::move(j));
+    };
+    if (nthreads == 1) {
+        work(0);
+    } else {
+        std::vector<std::thread> pool;
+        for (int t = 0; t < nthreads; ++t) pool.emplace_back(work, t);
+        for (auto& t : pool) t.join();
     }
+    for (int q = 0; q < n; ++q)
+        if (status[q] != ORF_OK) {
+            set_error("instance %d: %s", q + 1, why[q].c_str());
+            return status[q];
+        }
     // instances sharing a kernel configuration (precision, index width,
     // fused step count, interior variant) form one group: one launch per
     // kernel advances all of its members

@@ -93,7 +93,6 @@ struct Lut {
 // window, output rectangle and flags (pointers left unset).  Needs no device;
 // orf_plan2d exposes it for checks of the tiling.
 int plan2d(const orf_sim2d* s, const orf_tuning& tuning, Plan2D* plan) {
-
     const bool f64 = s->precision == ORF_DOUBLE;
     const bool per = s->periodic_z != 0;
     const int nx = s->nx, nz = s->nz, npx = s->npml_x, npz = per ? 0 : s->npml_z;
@@ -414,10 +413,13 @@ int Job2D<R>::create(const orf_sim2d* s) {
     };
     narrow(ix0, ib0);
     if (!te) narrow(ix1, ib1);
+    // (bytes counted here and added to the context's counter once, under a
+    // lock: a batch creates its instances on several host threads)
+    int64_t h2d = 0;
     auto up = [&](void* d, const void* hsrc, size_t bytes) -> int {
         if (bytes == 0) return ORF_OK;
         ORF_CUDA(cudaMemcpyAsync(d, hsrc, bytes, cudaMemcpyHostToDevice, st));
-        ctx->stats.h2d_bytes += (int64_t)bytes;
+        h2d += (int64_t)bytes;
         return ORF_OK;
     };
     ORF_TRY(up(d_ix0, ib0.data(), ib0.size()));
@@ -529,6 +531,7 @@ int Job2D<R>::create(const orf_sim2d* s) {
         return e;
     };
     ORF_CUDA(cudaStreamSynchronize(st));
+    add_h2d(ctx, h2d);
     return ORF_OK;
 }
 

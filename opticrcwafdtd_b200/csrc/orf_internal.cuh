@@ -17,6 +17,10 @@ namespace orf {
 constexpr int kChunk = 50;        // steps between energy checks and progress calls
 constexpr int kMaxMon = 16;       // monitors per orientation per instance
 constexpr int kMaxSub = 32;       // max time steps fused in one step-kernel launch
+// The CPML grading uses kappa_max = 1, so 1/kappa is 1 at every position and
+// the stretched difference d/kappa + psi is d + psi: the step kernels skip the
+// 1/kappa factor (fma(d, 1, psi) and d + psi round alike).
+constexpr bool kUnitKappa = true;
 constexpr int kStatusRing = 64;   // status ring entries per job (mapped host memory)
 
 // Written by the check kernel into mapped pinned host memory.

@@ -11,6 +11,12 @@ namespace orf {
 
 namespace {
 thread_local std::string g_err;
+std::mutex g_stats_mu;
+}
+
+void add_h2d(orf_ctx* c, int64_t bytes) {
+    std::lock_guard<std::mutex> g(g_stats_mu);
+    c->stats.h2d_bytes += bytes;
 }
 
 namespace {

@@ -80,6 +80,7 @@ struct DeviceScope {
 constexpr double kPi = 3.14159265358979323846;
 constexpr double kPmlOrder = 3.0;          // cpmlCoefficients.m:6-8 grading law; constants chosen here
 constexpr double kPmlKappaMax = 1.0;
+static_assert(!kUnitKappa || kPmlKappaMax == 1.0, "the step kernels assume 1/kappa = 1 (kUnitKappa)");
 constexpr double kPmlAlphaMaxPerK0 = 0.0;
 
 // Gaussian pulse of relative 1/e spectral half-width bw (fdtd2DTE.m:14-15):
@@ -203,6 +204,8 @@ struct orf_ctx {
 
 namespace orf {
 inline WaitCtl wait_ctl(const orf_ctx* c) { return WaitCtl{c->wait_ns, c->stall_plane}; }
+// host-to-device byte counter of a context, safe from several host threads
+void add_h2d(orf_ctx* c, int64_t bytes);
 void ctx_retain(orf_ctx* c);
 void ctx_release(orf_ctx* c);
 }  // namespace orf

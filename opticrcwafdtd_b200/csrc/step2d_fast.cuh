@@ -441,12 +441,12 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
                             const R* pz = prz + (ck0 + j) * 6;
                             const R ps = fma(pz[3], psA[c], pz[4] * dz);
                             psA[c] = ps;
-                            dz = fma(dz, pz[5], ps);
+                            dz = kUnitKappa ? dz + ps : fma(dz, pz[5], ps);
                         }
                         if (XC) {
                             const R qs = fma(phb, psB[c], pha * dx);
                             psB[c] = qs;
-                            dx = fma(dx, phk, qs);
+                            dx = kUnitKappa ? dx + qs : fma(dx, phk, qs);
                         }
                         const R ca = TE ? C : K0[j];
                         const R cb = TE ? C : K1[j];
@@ -489,12 +489,12 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
                             const R* pz = prz + (ck0 + j) * 6;
                             const R ps = fma(pz[0], psPz[c], pz[1] * da);
                             psPz[c] = ps;
-                            da = fma(da, pz[2], ps);
+                            da = kUnitKappa ? da + ps : fma(da, pz[2], ps);
                         }
                         if (XC) {
                             const R qs = fma(pxb, psPx[c], pxa * db);
                             psPx[c] = qs;
-                            db = fma(db, pxk, qs);
+                            db = kUnitKappa ? db + qs : fma(db, pxk, qs);
                         }
                         const R cp = TE ? K0[j] : C;
                         if (PML) {

@@ -86,6 +86,8 @@ struct Cpml3 {
     const R* pin[2][3][3];      // psi of (component, axis), buffer par (read)
     R* pout[2][3][3];           // the same, buffer par^1 (written)
     int n[3], np[3], nsl[2][3];
+    const R* zp[2];             // z profile of the segment's planes zk0 .. in shared memory
+    int zk0;
 };
 
 // The six differences of one cell's H or E update, in the order
@@ -95,8 +97,11 @@ struct Cpml3 {
 // axis by axis: the two psi loads of an axis are issued together, and a cell
 // on the slab of a single axis (all but the slab corners) has all its psi
 // loads in flight at once.  psi of buffer par is read-only during the launch.
+// zpre: z0, z1 are this cell's two z-axis psi values, loaded ahead by the
+// caller (the same values the loads here would return).
 template <class R>
-__device__ __forceinline__ void cpml6(const Cpml3<R>& X, int kind, bool store, int i, int j, int k, R (&d)[6]) {
+__device__ __forceinline__ void cpml6(const Cpml3<R>& X, int kind, bool store, int i, int j, int k, R (&d)[6],
+                                      bool zpre = false, R z0 = R(0), R z1 = R(0)) {
     const bool half = kind == 1;
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
@@ -109,17 +114,34 @@ __device__ __forceinline__ void cpml6(const Cpml3<R>& X, int kind, bool store, i
         const int v0 = q == 0 ? sl : i, v1 = q == 1 ? sl : j, v2 = q == 2 ? sl : k;
         const int d0 = q == 0 ? X.nsl[kind][0] : X.n[0], d1 = q == 1 ? X.nsl[kind][1] : X.n[1];
         const size_t o = (size_t)v0 + (size_t)d0 * ((size_t)v1 + (size_t)d1 * v2);
-        const R* pr = X.prof[kind][q] + 3 * coord;
-        const R ps1 = __ldg(X.pin[kind][C1[q]][q] + o), ps2 = __ldg(X.pin[kind][C2[q]][q] + o);
-        const R b = __ldg(pr), a = __ldg(pr + 1), ki = __ldg(pr + 2);
+        const bool zs = q == 2 && X.zp[kind] != nullptr;   // z profile staged in shared memory
+        const R* pr = zs ? X.zp[kind] + 3 * (coord - X.zk0) : X.prof[kind][q] + 3 * coord;
+        R ps1, ps2;
+        if (q == 2 && zpre) {
+            ps1 = z0;
+            ps2 = z1;
+        } else {
+            ps1 = __ldg(X.pin[kind][C1[q]][q] + o);
+            ps2 = __ldg(X.pin[kind][C2[q]][q] + o);
+        }
+        R b, a, ki = R(1);
+        if (zs) {
+            b = pr[0];
+            a = pr[1];
+            if (!kUnitKappa) ki = pr[2];
+        } else {
+            b = __ldg(pr);
+            a = __ldg(pr + 1);
+            if (!kUnitKappa) ki = __ldg(pr + 2);
+        }
         const R p1 = b * ps1 + a * d[E1[q]];
         const R p2 = b * ps2 + a * d[E2[q]];
         if (store) {
             X.pout[kind][C1[q]][q][o] = p1;
             X.pout[kind][C2[q]][q][o] = p2;
         }
-        d[E1[q]] = d[E1[q]] * ki + p1;
-        d[E2[q]] = d[E2[q]] * ki + p2;
+        d[E1[q]] = kUnitKappa ? d[E1[q]] + p1 : d[E1[q]] * ki + p1;
+        d[E2[q]] = kUnitKappa ? d[E2[q]] + p2 : d[E2[q]] * ki + p2;
     }
 }
 
@@ -196,13 +218,14 @@ __device__ __forceinline__ void tma_load3(void* sdst, const void* tmap, int x, i
 template <bool PML, class R>
 __device__ __forceinline__ void h_cell(const Inst3D<R>* __restrict__ I, const Cpml3<R>& X, bool store, int i, int j,
                                        int k, R ex, R ey, R ez, R ex_k, R ey_k, R ez_i, R ey_i, R ez_j, R ex_j, R& hx,
-                                       R& hy, R& hz, R gE, bool src) {
+                                       R& hy, R& hz, R gE, bool src, bool zpre = false, R z0 = R(0),
+                                       R z1 = R(0)) {
     const R C = I->C;
     // Hx -= C ((Ez(j+1) - Ez) - (Ey(k+1) - Ey))
     // Hy -= C ((Ex(k+1) - Ex) - (Ez(i+1) - Ez))
     // Hz -= C ((Ey(i+1) - Ey) - (Ex(j+1) - Ex))
     R dd[6] = {ez_j - ez, ey_k - ey, ex_k - ex, ez_i - ez, ey_i - ey, ex_j - ex};
-    if (PML) cpml6(X, 1, store, i, j, k, dd);
+    if (PML) cpml6(X, 1, store, i, j, k, dd, zpre, z0, z1);
     hx = hx - C * (dd[0] - dd[1]);
     hy = hy - C * (dd[2] - dd[3]);
     hz = hz - C * (dd[4] - dd[5]);
@@ -225,8 +248,10 @@ __device__ __forceinline__ R coef(const R* slut, const R* __restrict__ lutc, int
     else return __ldg(lutc + v);
 }
 
+// Resident CTAs per SM: FP32 4 (interior) / 3 (CPML: the psi and profile
+// values loaded ahead need the registers), FP64 3.
 template <class R, class IT, bool PML>
-__global__ void __launch_bounds__(NT, sizeof(R) == 4 ? 4 : 3)
+__global__ void __launch_bounds__(NT, sizeof(R) == 4 ? (PML ? 3 : 4) : 3)
 k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, int par, int launch_off,
          int want_energy, WaitCtl wc) {
     const Tile3D tile = tiles[blockIdx.x];
@@ -296,6 +321,26 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     }
     __syncthreads();
+    // CPML tiles: the z profile (b, a, 1/kappa) of planes k0-1 .. k1 in shared
+    // memory, the entry every cell of a plane reads
+    __shared__ R szp[PML ? 2 : 1][PML ? 3 * (kSeg3 + 2) : 1];
+    const int np2 = PML ? sx.np[2] : 0;
+    if constexpr (PML) {
+        const int cnt = k1 - k0 + 2;
+        if (np2 > 0) {
+            for (int q = t; q < 6 * cnt; q += NT) {
+                const int kind = q / (3 * cnt), r = q - kind * 3 * cnt, c = r / 3 + k0 - 1, f = r - 3 * (r / 3);
+                szp[kind][r] = (c >= 0 && c < nz) ? sx.prof[kind][2][3 * c + f] : R(f == 1 ? 0 : 1);
+            }
+        }
+        __syncthreads();   // every thread has read sx.np
+        if (t == 0) {
+            sx.zk0 = k0 - 1;
+            sx.zp[0] = np2 > 0 ? &szp[0][0] : nullptr;
+            sx.zp[1] = np2 > 0 ? &szp[1][0] : nullptr;
+        }
+        __syncthreads();
+    }
 
     // ---- region addressing for the cp.async path, the same for every plane
     size_t roff[RPT];
@@ -457,6 +502,35 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
     const bool haloSrcH = sa != 2 && sel3(sa, hi, hj, 0) == ss - 1;
     double energy = 0.0;
     R* smp0 = I->samples + (size_t)launch_off * I->sstride;
+    // CPML tiles with a z slab: the z-axis psi of the own and the halo cell's
+    // H update are loaded a plane ahead, those of the own E update at the top
+    // of the plane's iteration, so the loads overlap the barriers and the H
+    // phase instead of stalling the update (psi of buffer par is read-only)
+    // (FP32: in FP64 the values held ahead would spill at three CTAs per SM)
+    const bool zpre = PML && sizeof(R) == 4 && np2 > 0;
+    R zHo0 = R(0), zHo1 = R(0), zHh0 = R(0), zHh1 = R(0), zEo0 = R(0), zEo1 = R(0);
+    auto load_zH = [&](int p) {
+        const int sl = slab(true, p, nz, np2);
+        if (sl < 0) return;
+        if (own) {
+            const size_t o = (size_t)i + (size_t)nx * ((size_t)j + (size_t)ny * sl);
+            zHo0 = __ldg(sx.pin[1][0][2] + o);
+            zHo1 = __ldg(sx.pin[1][1][2] + o);
+        }
+        if (haloValid) {
+            const size_t o = (size_t)hi + (size_t)nx * ((size_t)hj + (size_t)ny * sl);
+            zHh0 = __ldg(sx.pin[1][0][2] + o);
+            zHh1 = __ldg(sx.pin[1][1][2] + o);
+        }
+    };
+    auto load_zE = [&](int p) {
+        const int sl = slab(false, p, nz, np2);
+        if (sl < 0 || !own) return;
+        const size_t o = (size_t)i + (size_t)nx * ((size_t)j + (size_t)ny * sl);
+        zEo0 = __ldg(sx.pin[0][0][2] + o);
+        zEo1 = __ldg(sx.pin[0][1][2] + o);
+    };
+    if (zpre) load_zH(k0);
     for (int k = k0; k < k1; ++k) {
         const int it = k - k0;
         const int s0 = it % ns, s1 = (it + 1) % ns, sn = (it + ns - 1) % ns;
@@ -466,6 +540,7 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
         if (s_abort) break;      // a wait ran out: the whole CTA leaves the march here
         if (k + ns - 1 <= k1) load_plane(k + ns - 1, sn);   // into the slot of plane k-1
         cp_commit();
+        if (zpre) load_zE(k);
         const R* E0x = sEq(s0, 0);
         const R* E0y = sEq(s0, 1);
         const R* E0z = sEq(s0, 2);
@@ -484,7 +559,7 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
                 hy = H0y[e];
                 hz = H0z[e];
                 h_cell<PML>(I, sx, false, hi, hj, k, E0x[e], E0y[e], E0z[e], E1x[e], E1y[e], E0z[e + 1], E0y[e + 1],
-                            E0z[e + SX], E0x[e + SX], hx, hy, hz, gE, haloSrcH || k == kSrcH);
+                            E0z[e + SX], E0x[e + SX], hx, hy, hz, gE, haloSrcH || k == kSrcH, zpre, zHh0, zHh1);
             }
             sHn[e] = hx;
             sHn[EBr + e] = hy;
@@ -502,7 +577,7 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
                 hyk = H0y[e];
                 hzk = H0z[e];
                 h_cell<PML>(I, sx, true, i, j, k, exo, eyo, ezo, E1x[e], E1y[e], E0z[e + 1], E0y[e + 1], E0z[e + SX],
-                            E0x[e + SX], hxk, hyk, hzk, gE, ownSrcH || k == kSrcH);
+                            E0x[e + SX], hxk, hyk, hzk, gE, ownSrcH || k == kSrcH, zpre, zHo0, zHo1);
                 const size_t o = (size_t)k * plane + (size_t)j * pitch + i;
                 Hout[0][o] = hxk;
                 Hout[1][o] = hyk;
@@ -512,6 +587,7 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
             sHn[EBr + e] = hyk;
             sHn[2 * EBr + e] = hzk;
         }
+        if (zpre && k + 1 < k1) load_zH(k + 1);   // consumed at the next plane's H phase
         __syncthreads();
         // ---- E of plane k at the own cell
         if (own) {
@@ -523,7 +599,7 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
             // Ey += cy ((Hx - Hx(k-1)) - (Hz - Hz(i-1)))
             // Ez += cz ((Hy - Hy(i-1)) - (Hx - Hx(j-1)))
             R dd[6] = {hzk - hz_j, hyk - hym, hxk - hxm, hzk - hz_i, hyk - hy_i, hxk - hx_j};
-            if (PML) cpml6(sx, 0, true, i, j, k, dd);
+            if (PML) cpml6(sx, 0, true, i, j, k, dd, zpre, zEo0, zEo1);
             R ex = exo + coef<R, IT>(slut, I->lutc, v0) * (dd[0] - dd[1]);
             R ey = eyo + coef<R, IT>(slut, I->lutc, v1) * (dd[2] - dd[3]);
             R ez = ezo + coef<R, IT>(slut, I->lutc, v2) * (dd[4] - dd[5]);

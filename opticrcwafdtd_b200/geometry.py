@@ -86,6 +86,66 @@ def epsCellMean(xc, yc, dx: float, dy: float, boxes, nBg: float, harmonicDir: st
     boxes = _as_boxes(boxes)
     off = _offsets(NSub)
     wrap = None if WrapY is None else (float(WrapY[0]), float(WrapY[1]))
+    if harmonicDir not in ("none", "x", "y"):
+        raise ValueError('harmonicDir must be "none", "x" or "y"')
+    if wrap is None and NSub > 1 and xc.size * yc.size > 4096:
+        return _cell_mean_banded(xc, yc, dx, dy, boxes, nBg, harmonicDir, NSub, off)
+    return _cell_mean_full(xc, yc, dx, dy, boxes, nBg, harmonicDir, NSub, off, wrap)
+
+
+def _straddled(c: np.ndarray, lo: float, hi: float, edges) -> np.ndarray:
+    """Indices q whose sample span [c_q + lo, c_q + hi] puts samples on both
+    sides of an edge (some sample < e <= another sample), for sorted c."""
+    out = []
+    for e in edges:
+        if not np.isfinite(e):
+            continue
+        # c + lo < e <= c + hi  <=>  e - hi <= c < e - lo (up to rounding: widen by one)
+        a = max(0, int(np.searchsorted(c, e - hi, side="left")) - 1)
+        b = min(c.size, int(np.searchsorted(c, e - lo, side="left")) + 1)
+        q = np.arange(a, b)
+        if q.size:
+            out.append(q[(c[q] + lo < e) & (e <= c[q] + hi)])
+    return np.unique(np.concatenate(out)) if out else np.zeros(0, dtype=np.int64)
+
+
+def _cell_mean_banded(xc, yc, dx, dy, boxes, nBg, harmonicDir, NSub, off):
+    """epsCellMean without wrap, sub-sampling only where a box edge passes
+    between a cell's samples.  A cell whose samples all lie inside or all
+    outside every box has NSub^2 equal samples: its mean is formed from the
+    painted value by the same sequence of operations as the full sub-sampled
+    mean, and the cells an edge crosses (whole columns and rows) are computed
+    by that full mean, so the result is bitwise the full computation's."""
+    lo_x, hi_x = off[0] * dx, off[-1] * dx
+    lo_y, hi_y = off[0] * dy, off[-1] * dy
+    bx = [e for b in boxes if b[1] > b[0] and b[3] > b[2] for e in (b[0], b[1])]
+    by = [e for b in boxes if b[1] > b[0] and b[3] > b[2] for e in (b[2], b[3])]
+    cols = _straddled(xc, lo_x, hi_x, bx)
+    rows = _straddled(yc, lo_y, hi_y, by)
+    # uniform cells: the painted value at the cells' own samples (any one of them)
+    v = _paint2d(xc + off[0] * dx, yc + off[0] * dy, nBg, boxes, None)
+    if harmonicDir == "none":
+        acc = np.zeros_like(v)
+        for _ in range(NSub * NSub):
+            acc += v
+        out = acc / NSub ** 2
+    else:
+        inv = np.zeros_like(v)
+        for _ in range(NSub):
+            inv += 1.0 / v
+        acc = np.zeros_like(v)
+        for _ in range(NSub):
+            acc += NSub / inv
+        out = acc / NSub
+    if cols.size:
+        out[cols, :] = _cell_mean_full(xc[cols], yc, dx, dy, boxes, nBg, harmonicDir, NSub, off, None)
+    if rows.size:
+        out[:, rows] = _cell_mean_full(xc, yc[rows], dx, dy, boxes, nBg, harmonicDir, NSub, off, None)
+    return out
+
+
+def _cell_mean_full(xc, yc, dx, dy, boxes, nBg, harmonicDir, NSub, off, wrap):
+    """epsCellMean with every cell sub-sampled NSub x NSub times."""
     if harmonicDir == "none":
         acc = np.zeros((xc.size, yc.size))
         for ox in off:

@@ -222,15 +222,28 @@ def coupler_instance_eta(out: dict, sim: dict, theta_deg=None, x_step: float = 0
     """Fiber coupling efficiency of one coupler_batch_sims / serve_stream 2D
     coupler from its DFT lines: Pinc = flux after the source + R with
     R = -flux behind it, Pup = up-line flux / Pinc, and eta = overlap of the
-    up-line Ey with a tilted Gaussian fiber mode times Pup (fiberCoupling.m:16-31),
-    on a theta (default 5..15 deg) x fiber centre x lambda grid."""
-    from .coupler import fiberCoupling
+    up-line Ey with a tilted Gaussian fiber mode times Pup (the formula of
+    fiberCoupling.m:16-31), on a theta (default 5..15 deg) x fiber centre x
+    lambda grid.  The mode's phase exp(i k sin(theta) (x - x0)) is evaluated
+    as exp(i k sin(theta) x) exp(-i k sin(theta) x0), so each wavelength and
+    tilt is one real matrix-vector product over the fiber centres."""
     pinc = out["flux"][1] - out["flux"][0]
-    res = dict(xUp=sim["x"], lambdas=np.asarray(sim["lambdas"]), EyUp=out["PZ"][:, :, 0],
-               Pup=out["fluxZ"][0] / pinc, nClad=N_SIO2)
-    th = np.arange(5.0, 15.01, 1.0) if theta_deg is None else np.asarray(theta_deg, dtype=float)
-    x0 = np.arange(3.0, sim["x"][-1] - 3.0, x_step)
-    eta, _ = fiberCoupling(res, np.deg2rad(th), x0, w0)
+    pup = np.atleast_1d(out["fluxZ"][0] / pinc)
+    x = np.asarray(sim["x"], dtype=float).ravel()
+    lam = np.atleast_1d(np.asarray(sim["lambdas"], dtype=float))
+    E = np.asarray(out["PZ"][:, :, 0]).reshape(x.size, -1)
+    th = np.deg2rad(np.arange(5.0, 15.01, 1.0) if theta_deg is None else np.asarray(theta_deg, dtype=float))
+    x0 = np.arange(3.0, x[-1] - 3.0, x_step)
+    eta = np.zeros((th.size, x0.size, lam.size))
+    EE = np.real(np.sum(np.conj(E) * E, axis=0))
+    u = x[None, :] - x0[:, None]
+    for i, t in enumerate(th):
+        G = np.exp(-(u * np.cos(t) / w0) ** 2)            # |E_f|, real, (x0, x)
+        GG = np.sum(G * G, axis=1)
+        for l in range(lam.size):
+            ks = 2 * np.pi * N_SIO2 / lam[l] * np.sin(t)
+            v = G @ (np.exp(-1j * ks * x) * E[:, l])     # sum_x conj(E_f) E, up to the x0 phase
+            eta[i, :, l] = np.abs(v) ** 2 / (EE[l] * GG) * pup[l]
     return eta
 
 

@@ -46,7 +46,7 @@ def test_stalled_plane_wait_times_out_and_context_stays_usable():
     with pytest.raises(_abi.OrfError) as ei:
         _run(ctx, sim)
     dt = time.perf_counter() - t0
-    assert ei.value.args[0] == "orf:deviceTimeout"
+    assert ei.value.identifier == "orf:deviceTimeout"
     assert "gave up waiting" in _lib.last_error()
     assert dt < 30.0
     # the same context, hook off: bitwise the run of a fresh context
