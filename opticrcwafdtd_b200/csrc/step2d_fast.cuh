@@ -11,7 +11,7 @@
 //     keeps a vertical strip of KS cells of P, A and B in registers for the
 //     whole launch, so the T fused steps read and write HBM once per field;
 //   - x neighbours come from warp shuffles, neighbours across warps from small
-//     shared exchange buffers (one __syncthreads per half step);
+//     shared exchange buffers (one block barrier per half step);
 //   - tiles overlap by T cells (trapezoidal temporal blocking): after T steps
 //     only the inner output rectangle is valid and written back; fields
 //     ping-pong between two buffers so overlapping tiles never race;
@@ -27,7 +27,8 @@
 // the tile's dependency cone is a plain cell, no masks and no CPML code) and
 // frame tiles (PML = true: CPML psi in a shared working plane, boundary
 // masks, zero fill outside the grid), the latter specialised on the CPML axes
-// a tile reaches.  Every update is written with explicit fma, so each
+// a tile reaches and, within a tile, on those its warp's cells reach.  Every
+// update is written with explicit fma, so each
 // instantiation performs, cell by cell, the same roundings (no contraction
 // choice left to the compiler) and results do not depend on the tiling.
 #pragma once
@@ -63,6 +64,11 @@ __device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gsrc) : "memory");
 }
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+// The barrier of the fused-step loop (named barrier 1, all NT threads).  Warps
+// of a frame tile may run different specialisations of the loop; each reaches
+// this barrier twice per step, from its own copy of the loop body.
+template <int NT>
+__device__ __forceinline__ void step_barrier() { asm volatile("bar.sync 1, %0;\n" ::"n"(NT) : "memory"); }
 __device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 template <class R>
@@ -421,7 +427,7 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
                     // ----- H half step: A (d/dz P), B (d/dx P)
                     if (lane == 0) store_row<R, KS>(&xPc[warp][0], P);
                     xPr[warp][lane] = P[0];
-                    __syncthreads();
+                    step_barrier<NT>();
                     R Pdn = xPr[wDn][lane];
                     if (!hasDn) Pdn = PML ? R(0) : P[KS - 1];
                     constexpr int VEC = 16 / sizeof(R);
@@ -471,7 +477,7 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
                     // ----- E half step: P (branch-free stencil loop)
                     if (lane == 31) store_row<R, KS>(&xBc[warp][0], B);
                     xAr[warp][lane] = A[KS - 1];
-                    __syncthreads();
+                    step_barrier<NT>();
                     R Aup = xAr[wUp][lane];
                     if (!hasUp) Aup = PML ? R(0) : A[0];
                     R be[VEC];
@@ -544,7 +550,13 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
             if constexpr (!PML) {
                 steps(Flag<false>{}, Flag<false>{});
             } else {
-                const bool zc = (d.flags & 16) != 0, xc = (d.flags & 8) != 0;
+                // per warp: the CPML arithmetic of an axis runs only in warps
+                // whose cells (with a cell of margin) reach that axis's slabs;
+                // elsewhere psi stays 0 and the profile is the identity, so
+                // skipping it leaves every value unchanged
+                const int wi0 = d.li0 + 32 * wx;
+                const bool zc = (d.flags & 16) != 0 && (kb < I->npz + 1 || kb + KS > nz - I->npz - 2);
+                const bool xc = (d.flags & 8) != 0 && (wi0 < I->npx + 1 || wi0 + 32 > d.nx - I->npx - 2);
                 if (zc && xc) steps(Flag<true>{}, Flag<true>{});
                 else if (zc) steps(Flag<true>{}, Flag<false>{});
                 else if (xc) steps(Flag<false>{}, Flag<true>{});
