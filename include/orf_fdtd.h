@@ -260,6 +260,14 @@ typedef struct orf_tile3d {
 ORF_API int32_t orf_plan3d(const orf_sim3d* sim, orf_tile3d* tiles, int32_t cap, int32_t* n_interior,
                            int32_t* n_cpml);
 
+/* No counterpart in the reference.  The checked build of this library
+ * (lib/liborf_fdtd_check.so, compiled with ORF_CHECK) tests every global
+ * access of the 2D step kernels against its buffer and every stored cell
+ * against the grid; an access that fails is counted and skipped.  Writes the
+ * count on the current device since the last reset (reset != 0: clear it
+ * after reading).  The normal build returns ORF_EINVAL. */
+ORF_API int32_t orf_check_violations(uint64_t* count, int32_t reset);
+
 /* ------------------------------------------------------------ 2D runs --- */
 /* Element counts of the caller-allocated out arrays (complex counts are in
  * complex elements; allocate twice as many doubles). */

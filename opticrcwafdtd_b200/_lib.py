@@ -12,7 +12,9 @@ import os
 from . import _abi
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "lib", "liborf_fdtd.so")
+# ORF_FDTD_LIB selects another build of the library (the checked build
+# lib/liborf_fdtd_check.so, for instance)
+LIB_PATH = os.environ.get("ORF_FDTD_LIB") or os.path.join(_HERE, "lib", "liborf_fdtd.so")
 _lib = None
 
 P = C.POINTER
@@ -67,6 +69,7 @@ _SIGS = {
                               P(C.c_double), P(C.c_double), P(C.c_double)]),
     "orf_serve_clock": (C.c_double, [C.c_void_p]),
     "orf_serve_close": (C.c_int32, [C.c_void_p]),
+    "orf_check_violations": (C.c_int32, [P(C.c_uint64), C.c_int32]),
 }
 
 

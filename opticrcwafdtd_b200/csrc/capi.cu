@@ -321,6 +321,25 @@ int32_t orf_plan3d(const orf_sim3d* sim, orf_tile3d* tiles, int32_t cap, int32_t
     return ORF_OK;
 }
 
+int32_t orf_check_violations(uint64_t* count, int32_t reset) {
+    if (!count) return ORF_EINVAL;
+    *count = 0;
+#ifdef ORF_CHECK
+    unsigned long long a = 0, b = 0;
+    const int s1 = fast2d_violations_f32(&a, reset), s2 = fast2d_violations_f64(&b, reset);
+    if (s1 != ORF_OK || s2 != ORF_OK) {
+        set_error("reading the checked build's violation counters failed");
+        return ORF_ECUDA;
+    }
+    *count = a + b;
+    return ORF_OK;
+#else
+    (void)reset;
+    set_error("this library is the normal build; the checked one is lib/liborf_fdtd_check.so");
+    return ORF_EINVAL;
+#endif
+}
+
 int32_t orf_batch2d_run(orf_ctx* ctx, int32_t n, const orf_sim2d* sims, orf_out2d* outs, orf_progress_fn progress,
                         void* user) {
     if (!ctx || n < 0 || (n > 0 && (!sims || !outs))) { set_error("NULL argument"); return ORF_EINVAL; }

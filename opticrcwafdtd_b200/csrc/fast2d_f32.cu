@@ -1,4 +1,5 @@
 // fast2d_f32.cu -- float instantiations of the pipelined 2D step kernel (step2d_fast.cuh).
+#include "orf_fdtd.h"
 #include "step2d_fast.cuh"
 
 namespace orf {
@@ -60,6 +61,23 @@ cudaError_t launch_fast2d_f32(bool te, bool idx16, bool pml, int variant, const 
         case 2: return dispatch<false, 8, 4, 4>(te, idx16, tiles, ntiles, off, nsub, par, we, grid, s);
     }
     return cudaErrorInvalidValue;
+}
+
+// Out-of-bounds accesses caught by the checked build's float kernels (reset: set
+// the counter back to zero); ORF_EINVAL in the normal build.
+int fast2d_violations_f32(unsigned long long* n, int reset) {
+#ifdef ORF_CHECK
+    cudaError_t e = cudaMemcpyFromSymbol(n, fast::g_check_violations, sizeof *n);
+    if (e == cudaSuccess && reset) {
+        const unsigned long long z = 0;
+        e = cudaMemcpyToSymbol(fast::g_check_violations, &z, sizeof z);
+    }
+    return e == cudaSuccess ? ORF_OK : ORF_ECUDA;
+#else
+    (void)reset;
+    *n = 0;
+    return ORF_EINVAL;
+#endif
 }
 
 int occ_fast2d_f32(bool te, bool idx16, bool pml, int variant) {

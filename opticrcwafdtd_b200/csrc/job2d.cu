@@ -441,6 +441,7 @@ int Job2D<R>::create(const orf_sim2d* s) {
 
     h.nx = nx; h.nz = nz; h.pitch = pitch; h.nzA = nzA; h.nxB = nxB;
     h.periodic = per ? 1 : 0; h.te = te ? 1 : 0; h.npx = npx; h.npz = npz; h.idx16 = idx16 ? 1 : 0;
+    h.nlut = nlut;
     h.C = R(Cc);
     h.idx0 = d_ix0; h.idx1 = d_ix1; h.lutc = d_lutc; h.lute = d_lute;
     h.pmlx = d_px; h.pmlxh = d_pxh; h.pmlz = d_pz; h.pmlzh = d_pzh;

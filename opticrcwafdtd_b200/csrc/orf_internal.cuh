@@ -85,6 +85,7 @@ struct Inst2D {
     int periodic, te;
     int npx, npz;           // CPML cells per end (npz = 0 when periodic)
     int idx16;              // material index width: 0 = uint8, 1 = uint16
+    int nlut;               // distinct materials (entries of lutc / lute in use)
     R C;                    // courant number c0*dt/dx
     R* P[2];
     R* A[2];
@@ -212,6 +213,8 @@ bool fast2d_info(int id, bool fp64, bool pml, Variant2D* v);
 cudaError_t launch_fast2d(bool fp64, bool te, bool idx16, bool pml, int variant, const FastTile2D* tiles, int ntiles,
                           int launch_off, int nsub, int par, int want_energy, int grid, cudaStream_t s);
 int fast2d_blocks_per_sm(bool fp64, bool te, bool idx16, bool pml, int variant);
+int fast2d_violations_f32(unsigned long long* n, int reset);
+int fast2d_violations_f64(unsigned long long* n, int reset);
 
 constexpr int kTile3X = 32, kTile3Y = 8;   // 3D CTA tile (x, y)
 constexpr int kSeg3 = 60;                  // z planes marched by one 3D CTA

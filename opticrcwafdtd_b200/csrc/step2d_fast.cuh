@@ -11,7 +11,7 @@
 //     keeps a vertical strip of KS cells of P, A and B in registers for the
 //     whole launch, so the T fused steps read and write HBM once per field;
 //   - x neighbours come from warp shuffles, neighbours across warps from small
-//     shared exchange buffers (one block barrier per half step);
+//     shared exchange buffers (one __syncthreads per half step);
 //   - tiles overlap by T cells (trapezoidal temporal blocking): after T steps
 //     only the inner output rectangle is valid and written back; fields
 //     ping-pong between two buffers so overlapping tiles never race;
@@ -27,8 +27,7 @@
 // the tile's dependency cone is a plain cell, no masks and no CPML code) and
 // frame tiles (PML = true: CPML psi in a shared working plane, boundary
 // masks, zero fill outside the grid), the latter specialised on the CPML axes
-// a tile reaches and, within a tile, on those its warp's cells reach.  Every
-// update is written with explicit fma, so each
+// a tile reaches.  Every update is written with explicit fma, so each
 // instantiation performs, cell by cell, the same roundings (no contraction
 // choice left to the compiler) and results do not depend on the tiling.
 #pragma once
@@ -41,6 +40,23 @@ template <bool B>
 struct Flag {
     static constexpr bool value = B;
 };
+
+// Checked build (compiled with -DORF_CHECK, lib/liborf_fdtd_check.so): every
+// global access of the step kernel is tested against the extent of its
+// buffer (and every stored cell against the grid); an index outside is
+// counted here and the access skipped.  In the normal build the tests compile
+// away.  The counter of each translation unit is read by fast2d_violations.
+#ifdef ORF_CHECK
+static __device__ unsigned long long g_check_violations;
+__device__ __forceinline__ bool in_bounds(long long i, long long n) {
+    const bool ok = i >= 0 && i < n;
+    if (!ok) atomicAdd(&g_check_violations, 1ull);
+    return ok;
+}
+#define ORF_IN(i, n) ::orf::fast::in_bounds((long long)(i), (long long)(n))
+#else
+#define ORF_IN(i, n) true
+#endif
 
 __device__ __forceinline__ int pmod(int a, int n) {
     int r = a % n;
@@ -64,11 +80,7 @@ __device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gsrc) : "memory");
 }
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-// The barrier of the fused-step loop (named barrier 1, all NT threads).  Warps
-// of a frame tile may run different specialisations of the loop; each reaches
-// this barrier twice per step, from its own copy of the loop body.
-template <int NT>
-__device__ __forceinline__ void step_barrier() { asm volatile("bar.sync 1, %0;\n" ::"n"(NT) : "memory"); }
+
 __device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 template <class R>
@@ -199,6 +211,7 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
                 const int kk = d.periodic ? pmod(grow, d.nz) : min(max(grow, 0), d.nz - 1);
                 const size_t off = (size_t)kk * d.pitch + min(d.li0 + VE * cc, d.pitch - VE);
                 const int s = row * LX + VE * cc;
+                if (!ORF_IN(off + VE - 1, (size_t)d.pitch * d.nz)) continue;
                 cp_async16(pfP + s, gP + off);
                 cp_async16(pfA + s, gA + off);
                 cp_async16(pfB + s, gB + off);
@@ -214,7 +227,7 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
                 const int kk = d.periodic ? pmod(row, d.nz) : min(max(row, 0), d.nz - 1);
                 const size_t off = (size_t)kk * d.pitch + col;
                 const int c = (ck0 + j) * LX + cx;
-                const bool v = cv && rv;
+                const bool v = cv && rv && ORF_IN(off, (size_t)d.pitch * d.nz);
                 cp_field(pfP + c, gP + off, v);
                 cp_field(pfA + c, gA + off, v);
                 cp_field(pfB + c, gB + off, v);
@@ -236,6 +249,7 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
             const size_t rowend = base + (size_t)d.pitch * sizeof(IT);
             if (boff + 4 > rowend) boff = rowend - 4;
             const unsigned char* src = reinterpret_cast<const unsigned char*>(plane ? d.idx1 : d.idx0) + boff;
+            if (v && !ORF_IN(boff + 3, (size_t)d.pitch * d.nz * sizeof(IT))) continue;
             cp_async4(reinterpret_cast<unsigned char*>(pfI) + (size_t)plane * CELLS * sizeof(IT) +
                           ((size_t)r * LX) * sizeof(IT) + 4 * (size_t)c4,
                       src, v);
@@ -336,11 +350,13 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
                 if ((mP >> j) & 1u) {
                     const int szA = slab_half(kk, nz, npz);
                     const int szP = slab_int(kk, nz, npz);
-                    if (szA >= 0) a = gA[(size_t)szA * nx + i];
-                    if (szP >= 0) pz = gPz[(size_t)szP * nx + i];
-                    if (sxP >= 0) px = gPx[(size_t)kk * (2 * npx) + sxP];
+                    if (szA >= 0 && ORF_IN((size_t)szA * nx + i, (size_t)2 * npz * nx)) a = gA[(size_t)szA * nx + i];
+                    if (szP >= 0 && ORF_IN((size_t)szP * nx + i, (size_t)2 * npz * nx)) pz = gPz[(size_t)szP * nx + i];
+                    if (sxP >= 0 && ORF_IN((size_t)kk * (2 * npx) + sxP, (size_t)nz * 2 * npx))
+                        px = gPx[(size_t)kk * (2 * npx) + sxP];
                 }
-                if (((mB >> j) & 1u) && sxB >= 0) b = gB[(size_t)kk * (2 * npx) + sxB];
+                if (((mB >> j) & 1u) && sxB >= 0 && ORF_IN((size_t)kk * (2 * npx) + sxB, (size_t)nz * 2 * npx))
+                    b = gB[(size_t)kk * (2 * npx) + sxB];
                 psA[c] = a;
                 psB[c] = b;
                 psPx[c] = px;
@@ -352,16 +368,17 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
                 const bool rv = kk >= 0 && kk < nz;
                 for (int cc = 0; cc < 3; ++cc) {
                     const R id = R(cc == 1 ? 0 : 1);
-                    prz[q * 6 + cc] = rv ? I->pmlz[3 * kk + cc] : id;
-                    prz[q * 6 + 3 + cc] = (rv && kk < nzA) ? I->pmlzh[3 * kk + cc] : id;
+                    prz[q * 6 + cc] = (rv && ORF_IN(3 * kk + cc, 3 * nz)) ? I->pmlz[3 * kk + cc] : id;
+                    prz[q * 6 + 3 + cc] = (rv && kk < nzA && ORF_IN(3 * kk + cc, 3 * nzA)) ? I->pmlzh[3 * kk + cc] : id;
                 }
             }
             for (int q = threadIdx.x; q < LX; q += NT) {
                 const int ii = d.li0 + q;
                 for (int cc = 0; cc < 3; ++cc) {
                     const R id = R(cc == 1 ? 0 : 1);
-                    prx[q * 6 + cc] = (ii >= 0 && ii < nx) ? I->pmlx[3 * ii + cc] : id;
-                    prx[q * 6 + 3 + cc] = (ii >= 0 && ii < nx - 1) ? I->pmlxh[3 * ii + cc] : id;
+                    prx[q * 6 + cc] = (ii >= 0 && ii < nx && ORF_IN(3 * ii + cc, 3 * nx)) ? I->pmlx[3 * ii + cc] : id;
+                    prx[q * 6 + 3 + cc] =
+                        (ii >= 0 && ii < nx - 1 && ORF_IN(3 * ii + cc, 3 * (nx - 1))) ? I->pmlxh[3 * ii + cc] : id;
                 }
             }
         }
@@ -374,10 +391,15 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
             P[j] = pfP[c];
             A[j] = pfA[c];
             B[j] = pfB[c];
-            const int v0 = (int)pfI[c];
+            int v0 = (int)pfI[c];
+            // a material index outside the table is a fault wherever it lies:
+            // the loaded window holds cells of the grid, its zero padding or
+            // zero fill, whose index is 0
+            if (!ORF_IN(v0, max(I->nlut, 1))) v0 = 0;
             K0[j] = sizeof(IT) == 1 ? slut[v0] : __ldg(I->lutc + v0);
             if (!TE) {
-                const int v1 = (int)pfI[CELLS + c];
+                int v1 = (int)pfI[CELLS + c];
+                if (!ORF_IN(v1, max(I->nlut, 1))) v1 = 0;
                 K1[j] = sizeof(IT) == 1 ? slut[v1] : __ldg(I->lutc + v1);
             } else {
                 K1[j] = R(0);
@@ -427,7 +449,7 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
                     // ----- H half step: A (d/dz P), B (d/dx P)
                     if (lane == 0) store_row<R, KS>(&xPc[warp][0], P);
                     xPr[warp][lane] = P[0];
-                    step_barrier<NT>();
+                    __syncthreads();
                     R Pdn = xPr[wDn][lane];
                     if (!hasDn) Pdn = PML ? R(0) : P[KS - 1];
                     constexpr int VEC = 16 / sizeof(R);
@@ -470,14 +492,14 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
                         for (int j = 0; j < KS; ++j) {
                             if ((mB >> j) & 1u) {
                                 const int kk = d.periodic ? pmod(kb + j, nz) : kb + j;
-                                B[j] = fma(__ldg(I->srcB + kk), ge, B[j]);
+                                if (ORF_IN(kk, nz)) B[j] = fma(__ldg(I->srcB + kk), ge, B[j]);
                             }
                         }
                     }
                     // ----- E half step: P (branch-free stencil loop)
                     if (lane == 31) store_row<R, KS>(&xBc[warp][0], B);
                     xAr[warp][lane] = A[KS - 1];
-                    step_barrier<NT>();
+                    __syncthreads();
                     R Aup = xAr[wUp][lane];
                     if (!hasUp) Aup = PML ? R(0) : A[0];
                     R be[VEC];
@@ -516,7 +538,7 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
                         for (int j = 0; j < KS; ++j) {
                             if ((mP >> j) & 1u) {
                                 const int kk = d.periodic ? pmod(kb + j, nz) : kb + j;
-                                P[j] = fma(__ldg(I->srcP + kk), gh, P[j]);
+                                if (ORF_IN(kk, nz)) P[j] = fma(__ldg(I->srcP + kk), gh, P[j]);
                             }
                         }
                     }
@@ -531,14 +553,21 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
                             bl = (lane == 0) ? bej : bl;
                             if (xm >= 0 && ((own >> j) & 1u)) {
                                 R* smp = smp0 + (size_t)xm * 2 * nz;
-                                smp[kb + j] = P[j];
-                                smp[nz + kb + j] = R(0.5) * (bl + B[j]);
+                                if (ORF_IN((size_t)sslot * I->sstride + (size_t)xm * 2 * nz + nz + kb + j,
+                                           (size_t)kChunk * I->sstride)) {
+                                    smp[kb + j] = P[j];
+                                    smp[nz + kb + j] = R(0.5) * (bl + B[j]);
+                                }
                             }
                             if ((zmask >> j) & 1u) {
                                 const R am = (j > 0) ? A[j - 1] : Aup;
                                 for (int m = 0; m < I->nmonz; ++m) {
                                     if (I->monz[m] != kb + j) continue;
                                     R* smp = smp0 + (size_t)I->nmon * 2 * nz + (size_t)m * 2 * d.nx;
+                                    if (!ORF_IN((size_t)sslot * I->sstride + (size_t)I->nmon * 2 * nz +
+                                                    (size_t)m * 2 * d.nx + d.nx + i,
+                                                (size_t)kChunk * I->sstride))
+                                        continue;
                                     smp[i] = P[j];
                                     smp[d.nx + i] = R(0.5) * (am + A[j]);
                                 }
@@ -550,13 +579,7 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
             if constexpr (!PML) {
                 steps(Flag<false>{}, Flag<false>{});
             } else {
-                // per warp: the CPML arithmetic of an axis runs only in warps
-                // whose cells (with a cell of margin) reach that axis's slabs;
-                // elsewhere psi stays 0 and the profile is the identity, so
-                // skipping it leaves every value unchanged
-                const int wi0 = d.li0 + 32 * wx;
-                const bool zc = (d.flags & 16) != 0 && (kb < I->npz + 1 || kb + KS > nz - I->npz - 2);
-                const bool xc = (d.flags & 8) != 0 && (wi0 < I->npx + 1 || wi0 + 32 > d.nx - I->npx - 2);
+                const bool zc = (d.flags & 16) != 0, xc = (d.flags & 8) != 0;
                 if (zc && xc) steps(Flag<true>{}, Flag<true>{});
                 else if (zc) steps(Flag<true>{}, Flag<false>{});
                 else if (xc) steps(Flag<false>{}, Flag<true>{});
@@ -569,6 +592,7 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
                 for (int j = 0; j < KS; ++j) {
                     if ((own >> j) & 1u) {
                         const size_t o = (size_t)(kb + j) * d.pitch + i;
+                        if (!(ORF_IN(i, d.nx) && ORF_IN(kb + j, nz))) continue;
                         const double p = P[j], a = A[j], b = B[j];
                         const int v0 = (int)reinterpret_cast<const IT*>(d.idx0)[o];
                         if (TE) {
@@ -598,6 +622,8 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
             for (int j = 0; j < KS; ++j) {
                 if ((own >> j) & 1u) {
                     const size_t o = (size_t)(kb + j) * d.pitch + i;
+                    // an owned cell must be a cell of the grid
+                    if (!(ORF_IN(i, d.nx) && ORF_IN(kb + j, nz))) continue;
                     Pout[o] = P[j];
                     Aout[o] = A[j];
                     Bout[o] = B[j];
@@ -616,10 +642,12 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
                     const int kk = kb + j;
                     const int szA = slab_half(kk, nz, npz);
                     const int szP = slab_int(kk, nz, npz);
-                    if (szA >= 0) gA[(size_t)szA * nx + i] = psA[c];
-                    if (szP >= 0) gPz[(size_t)szP * nx + i] = psPz[c];
-                    if (sxP >= 0) gPx[(size_t)kk * (2 * npx) + sxP] = psPx[c];
-                    if (sxB >= 0) gB[(size_t)kk * (2 * npx) + sxB] = psB[c];
+                    if (szA >= 0 && ORF_IN((size_t)szA * nx + i, (size_t)2 * npz * nx)) gA[(size_t)szA * nx + i] = psA[c];
+                    if (szP >= 0 && ORF_IN((size_t)szP * nx + i, (size_t)2 * npz * nx)) gPz[(size_t)szP * nx + i] = psPz[c];
+                    if (sxP >= 0 && ORF_IN((size_t)kk * (2 * npx) + sxP, (size_t)nz * 2 * npx))
+                        gPx[(size_t)kk * (2 * npx) + sxP] = psPx[c];
+                    if (sxB >= 0 && ORF_IN((size_t)kk * (2 * npx) + sxB, (size_t)nz * 2 * npx))
+                        gB[(size_t)kk * (2 * npx) + sxB] = psB[c];
                 }
             }
             if (threadIdx.x == 0) d.st->cur = par ^ 1;
