@@ -109,34 +109,54 @@ def _straddled(c: np.ndarray, lo: float, hi: float, edges) -> np.ndarray:
     return np.unique(np.concatenate(out)) if out else np.zeros(0, dtype=np.int64)
 
 
+def _label2d(xs: np.ndarray, zs: np.ndarray, boxes: np.ndarray) -> np.ndarray:
+    """Index (1-based, 0 = background) of the last box covering each sample
+    point xs (sorted) x zs, in Fortran order: the label form of _paint2d."""
+    lab = np.zeros((xs.size, zs.size), dtype=np.int32, order="F")
+    for q, b in enumerate(boxes):
+        i0, i1 = _ranges(xs, b[0], b[1])
+        if i1 <= i0:
+            continue
+        k0, k1 = _ranges(zs, b[2], b[3])
+        if k1 > k0:
+            lab[i0:i1, k0:k1] = q + 1
+    return lab
+
+
 def _cell_mean_banded(xc, yc, dx, dy, boxes, nBg, harmonicDir, NSub, off):
     """epsCellMean without wrap, sub-sampling only where a box edge passes
     between a cell's samples.  A cell whose samples all lie inside or all
-    outside every box has NSub^2 equal samples: its mean is formed from the
-    painted value by the same sequence of operations as the full sub-sampled
-    mean, and the cells an edge crosses (whole columns and rows) are computed
-    by that full mean, so the result is bitwise the full computation's."""
+    outside every box has NSub^2 equal samples: its mean depends only on that
+    material and is formed by the same sequence of operations as the full
+    sub-sampled mean (one evaluation per material), and the cells an edge
+    crosses (whole columns and rows) are computed by the full mean, so the
+    result is bitwise the full computation's."""
     lo_x, hi_x = off[0] * dx, off[-1] * dx
     lo_y, hi_y = off[0] * dy, off[-1] * dy
     bx = [e for b in boxes if b[1] > b[0] and b[3] > b[2] for e in (b[0], b[1])]
     by = [e for b in boxes if b[1] > b[0] and b[3] > b[2] for e in (b[2], b[3])]
     cols = _straddled(xc, lo_x, hi_x, bx)
     rows = _straddled(yc, lo_y, hi_y, by)
-    # uniform cells: the painted value at the cells' own samples (any one of them)
-    v = _paint2d(xc + off[0] * dx, yc + off[0] * dy, nBg, boxes, None)
-    if harmonicDir == "none":
-        acc = np.zeros_like(v)
-        for _ in range(NSub * NSub):
-            acc += v
-        out = acc / NSub ** 2
-    else:
-        inv = np.zeros_like(v)
-        for _ in range(NSub):
-            inv += 1.0 / v
-        acc = np.zeros_like(v)
-        for _ in range(NSub):
-            acc += NSub / inv
-        out = acc / NSub
+    # uniform cells: the material at the cells' own samples (any one of them)
+    lab = _label2d(xc + off[0] * dx, yc + off[0] * dy, boxes)
+    vals = np.concatenate([[float(nBg) ** 2], boxes[:, 4] ** 2]) if boxes.size else np.array([float(nBg) ** 2])
+    table = np.empty_like(vals)
+    for m, v in enumerate(vals):
+        v = np.float64(v)
+        if harmonicDir == "none":
+            acc = np.float64(0.0)
+            for _ in range(NSub * NSub):
+                acc = acc + v
+            table[m] = acc / NSub ** 2
+        else:
+            inv = np.float64(0.0)
+            for _ in range(NSub):
+                inv = inv + 1.0 / v
+            acc = np.float64(0.0)
+            for _ in range(NSub):
+                acc = acc + NSub / inv
+            table[m] = acc / NSub
+    out = table[lab]
     if cols.size:
         out[cols, :] = _cell_mean_full(xc[cols], yc, dx, dy, boxes, nBg, harmonicDir, NSub, off, None)
     if rows.size:
