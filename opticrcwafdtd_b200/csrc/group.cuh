@@ -117,6 +117,7 @@ struct Group2D : Group {
             all_cells += j->cells();
             add_streams(j->host_streams, j->nL, j->d_st);
         }
+        sort_frame_tiles(frame.begin(), frame.end());   // members' frames, by CPML specialisation
         cudaStreamSynchronize(st);   // descriptors of the previous build may still be read
         arena.release();
         Arena ar;

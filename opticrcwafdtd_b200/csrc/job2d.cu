@@ -224,6 +224,7 @@ int plan2d(const orf_sim2d* s, const orf_tuning& tuning, Plan2D* plan) {
         for (int m = 0; m < s->n_monz; ++m)
             if (s->monitors_z[m] >= t.ok0 && s->monitors_z[m] < t.ok0 + t.oh) t.flags |= 4;
     }
+    sort_frame_tiles(plan->tiles.begin() + plan->nfast, plan->tiles.end());
     return ORF_OK;
 }
 

@@ -1,5 +1,7 @@
 // job2d.cuh -- device-resident 2D run (orf.fdtd2D).
 #pragma once
+#include <algorithm>
+
 #include "engine.cuh"
 
 namespace orf {
@@ -13,6 +15,16 @@ struct Plan2D {
     std::vector<FastTile2D> tiles;
 };
 int plan2d(const orf_sim2d* s, const orf_tuning& tuning, Plan2D* plan);
+
+// Frame tiles in runs of one CPML specialisation (flags 8 / 16): the
+// persistent frame launch then keeps the CTAs of an SM in the same code
+// (mixed, they miss in the instruction cache); the order changes no value.
+template <class It>
+void sort_frame_tiles(It first, It last) {
+    std::stable_sort(first, last, [](const FastTile2D& a, const FastTile2D& b) {
+        return (a.flags & 24) > (b.flags & 24);
+    });
+}
 
 template <class R>
 struct Job2D : orf_job {

@@ -178,12 +178,14 @@ __device__ __forceinline__ void mbar_init(unsigned long long* b, unsigned cnt) {
 __device__ __forceinline__ void mbar_expect_tx(unsigned long long* b, unsigned bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(sm_addr(b)), "r"(bytes) : "memory");
 }
-__device__ __forceinline__ bool mbar_try_wait(unsigned long long* b, unsigned parity) {
+// try_wait with a suspend-time hint: the polling thread sleeps until the
+// phase completes or about hint_ns pass, instead of re-issuing the poll
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* b, unsigned parity, unsigned hint_ns) {
     unsigned ok;
     asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
         : "=r"(ok)
-        : "r"(sm_addr(b)), "r"(parity)
+        : "r"(sm_addr(b)), "r"(parity), "r"(hint_ns)
         : "memory");
     return ok != 0;
 }
@@ -194,13 +196,14 @@ __device__ __forceinline__ unsigned long long global_ns() {
 }
 // Wait for the phase of parity `parity` of mbarrier b to complete, giving up
 // after kSpinMax polls or limit_ns nanoseconds; true when it completed.
+constexpr unsigned kPollHintNs = 20000;   // longest sleep of one poll
 __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* b, unsigned parity,
                                                   unsigned long long limit_ns) {
-    if (mbar_try_wait(b, parity)) return true;
+    if (mbar_try_wait(b, parity, kPollHintNs)) return true;
     const unsigned long long t0 = global_ns();
     for (long long spins = 1; spins < kSpinMax; ++spins) {
-        if (mbar_try_wait(b, parity)) return true;
-        if ((spins & 63) == 0 && global_ns() - t0 > limit_ns) return false;
+        if (mbar_try_wait(b, parity, kPollHintNs)) return true;
+        if (global_ns() - t0 > limit_ns) return false;
     }
     return false;
 }
