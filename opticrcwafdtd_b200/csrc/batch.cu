@@ -134,10 +134,38 @@ int run_batch(orf_ctx* ctx, int n, const orf_sim2d* sims, orf_out2d* outs, orf_p
     if (rc != ORF_OK) return rc;
     t0 = now_s();
     ctx->stats.loop_ms += 1e3 * (t0 - t1);
-    for (int q = 0; q < n; ++q) {
-        ctx->stats.cell_updates += jobs[q]->pl.last_step * jobs[q]->cells();
-        ORF_TRY(jobs[q]->finish2d(&outs[q]));
+    for (int q = 0; q < n; ++q) ctx->stats.cell_updates += jobs[q]->pl.last_step * jobs[q]->cells();
+    // results of the instances on host threads, each with a stream of its own
+    // (the loop has ended: the instances' sums are final and independent)
+    auto fin = [&](int tid) {
+        cudaSetDevice(ctx->device);
+        cudaStream_t fs = nullptr;
+        if (cudaStreamCreateWithFlags(&fs, cudaStreamNonBlocking) != cudaSuccess) {
+            cudaGetLastError();
+            for (int q = tid; q < n; q += nthreads) {
+                status[q] = ORF_ECUDA;
+                why[q] = "cannot create a stream for the results";
+            }
+            return;
+        }
+        for (int q = tid; q < n; q += nthreads) {
+            status[q] = jobs[q]->finish2d_on(&outs[q], fs);
+            if (status[q] != ORF_OK) why[q] = last_error();
+        }
+        cudaStreamDestroy(fs);
+    };
+    if (nthreads == 1) {
+        fin(0);
+    } else {
+        std::vector<std::thread> pool;
+        for (int t = 0; t < nthreads; ++t) pool.emplace_back(fin, t);
+        for (auto& t : pool) t.join();
     }
+    for (int q = 0; q < n; ++q)
+        if (status[q] != ORF_OK) {
+            set_error("instance %d: %s", q + 1, why[q].c_str());
+            return status[q];
+        }
     groups.clear();
     jobs.clear();
     ctx->stats.finish_ms += 1e3 * (now_s() - t0);

@@ -698,21 +698,28 @@ int64_t Job2D<R>::steps_done() {
 
 template <class R>
 int Job2D<R>::finish2d(orf_out2d* o) {
-    cudaStream_t st = ctx->stream;
+    return finish2d_on(o, ctx->stream);
+}
+
+// Results on stream st (a batch finishes its instances on several host
+// threads, each with a stream of its own, after the time loop has ended)
+template <class R>
+int Job2D<R>::finish2d_on(orf_out2d* o, cudaStream_t st) {
     ORF_CUDA(cudaStreamSynchronize(st));
+    int64_t d2h = 0;
     JobState js;
     ORF_CUDA(cudaMemcpy(&js, d_st, sizeof js, cudaMemcpyDeviceToHost));
     const bool f64 = sizeof(R) == 8;
     ORF_CUDA(launch_flux(f64, d_streams, d_pairs, npairs, nL, d_flux, st));
     std::vector<double> fl((size_t)(nM + nMZ) * nL);
     if (!fl.empty()) ORF_CUDA(cudaMemcpyAsync(fl.data(), d_flux, fl.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
-    ctx->stats.d2h_bytes += (int64_t)(fl.size() * sizeof(double));
+    d2h += (int64_t)(fl.size() * sizeof(double));
     // DFT lines: stream q -> complex [l][e]
     auto fetch = [&](int q, double* dst) -> int {
         if (!dst) return ORF_OK;
         const DftStream& S = host_streams[q];
         const size_t n = (size_t)S.len * nL;
-        ctx->stats.d2h_bytes += (int64_t)(n * sizeof(double2));
+        d2h += (int64_t)(n * sizeof(double2));
         if (f64) {
             ORF_CUDA(cudaMemcpyAsync(dst, S.acc, n * sizeof(double2), cudaMemcpyDeviceToHost, st));
         } else {
@@ -738,6 +745,7 @@ int Job2D<R>::finish2d(orf_out2d* o) {
     o->converged = js.converged;
     o->steps = js.step;
     o->time = js.step * S;
+    add_d2h(ctx, d2h);
     return ORF_OK;
 }
 

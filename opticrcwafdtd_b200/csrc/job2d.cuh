@@ -81,6 +81,7 @@ struct Job2D : orf_job {
     int reset() override;
     int get_fields(double* const* f, int nf) override;
     int finish2d(orf_out2d* o) override;
+    int finish2d_on(orf_out2d* o, cudaStream_t st);
     // enqueue every remaining chunk with direct launches, then synchronize
     int advance_all_direct();
     void state_regions(int b, std::vector<std::pair<void*, size_t>>& out) override;

@@ -19,6 +19,11 @@ void add_h2d(orf_ctx* c, int64_t bytes) {
     c->stats.h2d_bytes += bytes;
 }
 
+void add_d2h(orf_ctx* c, int64_t bytes) {
+    std::lock_guard<std::mutex> g(g_stats_mu);
+    c->stats.d2h_bytes += bytes;
+}
+
 namespace {
 struct DevPool {
     std::mutex mu;

@@ -206,6 +206,7 @@ namespace orf {
 inline WaitCtl wait_ctl(const orf_ctx* c) { return WaitCtl{c->wait_ns, c->stall_plane}; }
 // host-to-device byte counter of a context, safe from several host threads
 void add_h2d(orf_ctx* c, int64_t bytes);
+void add_d2h(orf_ctx* c, int64_t bytes);
 void ctx_retain(orf_ctx* c);
 void ctx_release(orf_ctx* c);
 }  // namespace orf
