@@ -73,7 +73,7 @@ def parse(argv=None):
     ap.add_argument("--serve-rate", type=float, default=0.0, help="fixed arrival rate (jobs/s) instead of --serve-load")
     ap.add_argument("--serve-capacity-jobs", type=int, default=24)
     ap.add_argument("--serve-max-cells", type=float, default=5e7)
-    ap.add_argument("--serve-macro", type=int, default=500)
+    ap.add_argument("--serve-macro", type=int, default=150)
     ap.add_argument("--serve-check-frac", type=float, default=0.25)
     return ap.parse_args(argv)
 
