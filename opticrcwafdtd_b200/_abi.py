@@ -258,13 +258,14 @@ def marshal_sim2d(sim: Any) -> Marshalled:
 
 def alloc_out2d(m: Marshalled) -> tuple[OrfOut2D, dict]:
     nx, nz, nL, nM, nMZ = (m.meta[k] for k in ("nx", "nz", "nL", "nM", "nMZ"))
+    # the DFT lines are written in full by the run's results (no zero fill)
     bufs = {
         "flux": np.zeros((nM, nL), order="F"),
         "fluxZ": np.zeros((nMZ, nL), order="F"),
-        "P": np.zeros((nz, nL, nM), dtype=np.complex128, order="F"),
-        "B": np.zeros((nz, nL, nM), dtype=np.complex128, order="F"),
-        "PZ": np.zeros((nx, nL, nMZ), dtype=np.complex128, order="F"),
-        "AZ": np.zeros((nx, nL, nMZ), dtype=np.complex128, order="F"),
+        "P": np.empty((nz, nL, nM), dtype=np.complex128, order="F"),
+        "B": np.empty((nz, nL, nM), dtype=np.complex128, order="F"),
+        "PZ": np.empty((nx, nL, nMZ), dtype=np.complex128, order="F"),
+        "AZ": np.empty((nx, nL, nMZ), dtype=np.complex128, order="F"),
     }
     o = OrfOut2D()
     o.flux = _ptr(bufs["flux"]) if bufs["flux"].size else None

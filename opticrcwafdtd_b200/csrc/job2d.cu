@@ -391,12 +391,12 @@ int Job2D<R>::create(const orf_sim2d* s) {
 
     // mapped host status ring and cancel flag (not in no-allocation mode)
     if (!ext_base) {
-        ORF_CUDA(cudaHostAlloc((void**)&ring_h, sizeof(ChunkStatus) * kStatusRing, cudaHostAllocMapped));
+        ORF_TRY(host_mapped_alloc(sizeof(ChunkStatus) * kStatusRing, (void**)&ring_h, (void**)&ring_d));
         std::memset(ring_h, 0, sizeof(ChunkStatus) * kStatusRing);
-        ORF_CUDA(cudaHostGetDevicePointer((void**)&ring_d, ring_h, 0));
-        ORF_CUDA(cudaHostAlloc((void**)&cancel_h, sizeof(int), cudaHostAllocMapped));
+        void* ch = nullptr;
+        ORF_TRY(host_mapped_alloc(sizeof(int), &ch, (void**)&cancel_d));
+        cancel_h = static_cast<volatile int*>(ch);
         *cancel_h = 0;
-        ORF_CUDA(cudaHostGetDevicePointer((void**)&cancel_d, (void*)cancel_h, 0));
     }
 
     // ---- upload
@@ -595,8 +595,8 @@ Job2D<R>::~Job2D() {
         cudaStreamSynchronize(ctx->stream);
         arena.release();
     }
-    if (ring_h) cudaFreeHost(ring_h);
-    if (cancel_h) cudaFreeHost((void*)cancel_h);
+    host_mapped_free(ring_h);
+    host_mapped_free((void*)cancel_h);
 }
 
 template <class R>
@@ -705,10 +705,9 @@ int Job2D<R>::finish2d(orf_out2d* o) {
 // threads, each with a stream of its own, after the time loop has ended)
 template <class R>
 int Job2D<R>::finish2d_on(orf_out2d* o, cudaStream_t st) {
-    ORF_CUDA(cudaStreamSynchronize(st));
     int64_t d2h = 0;
-    JobState js;
-    ORF_CUDA(cudaMemcpy(&js, d_st, sizeof js, cudaMemcpyDeviceToHost));
+    JobState js;   // read after the stream's last synchronisation below
+    ORF_CUDA(cudaMemcpyAsync(&js, d_st, sizeof js, cudaMemcpyDeviceToHost, st));
     const bool f64 = sizeof(R) == 8;
     ORF_CUDA(launch_flux(f64, d_streams, d_pairs, npairs, nL, d_flux, st));
     std::vector<double> fl((size_t)(nM + nMZ) * nL);

@@ -349,10 +349,12 @@ int Job3D<R>::create(const orf_sim3d* s) {
     ORF_TRY(ar.alloc());
     arena = ar;
     ORF_CUDA(cudaMemsetAsync(arena.base, 0, arena.total, st));
-    ORF_CUDA(cudaHostAlloc((void**)&ring_h, sizeof(ChunkStatus) * kStatusRing, cudaHostAllocMapped));
-    ORF_CUDA(cudaHostGetDevicePointer((void**)&ring_d, ring_h, 0));
-    ORF_CUDA(cudaHostAlloc((void**)&cancel_h, sizeof(int), cudaHostAllocMapped));
-    ORF_CUDA(cudaHostGetDevicePointer((void**)&cancel_d, (void*)cancel_h, 0));
+    ORF_TRY(host_mapped_alloc(sizeof(ChunkStatus) * kStatusRing, (void**)&ring_h, (void**)&ring_d));
+    std::memset(ring_h, 0, sizeof(ChunkStatus) * kStatusRing);
+    void* ch = nullptr;
+    ORF_TRY(host_mapped_alloc(sizeof(int), &ch, (void**)&cancel_d));
+    cancel_h = static_cast<volatile int*>(ch);
+    *cancel_h = 0;
 
     auto up = [&](void* dst, const void* src, size_t bytes) -> int {
         if (bytes == 0) return ORF_OK;

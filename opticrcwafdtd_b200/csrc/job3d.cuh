@@ -49,8 +49,8 @@ struct Job3D : orf_job {
             cudaStreamSynchronize(ctx->stream);
             arena.release();
         }
-        if (ring_h) cudaFreeHost(ring_h);
-        if (cancel_h) cudaFreeHost((void*)cancel_h);
+        host_mapped_free(ring_h);
+        host_mapped_free((void*)cancel_h);
     }
     size_t N() const { return (size_t)n[0] * n[1] * n[2]; }
     size_t NP() const { return (size_t)pitch * n[1] * n[2]; }

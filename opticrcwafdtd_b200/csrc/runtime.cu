@@ -133,6 +133,78 @@ void dev_trim(int device) {
     if (!evict.empty() && cur != device) cudaSetDevice(cur);
 }
 
+namespace {
+constexpr size_t kHostSlab = size_t(1) << 20;   // pinned bytes per cudaHostAlloc
+constexpr int kHostClasses = 9;                 // slot sizes 256 B .. 64 KiB (powers of two)
+struct HostPool {
+    std::mutex mu;
+    std::vector<void*> idle[kHostClasses];
+    std::unordered_map<void*, int> cls;         // every slot handed out: its size class
+    char* cur = nullptr;                        // unused tail of the newest slab
+    size_t left = 0;
+};
+HostPool& host_pool() {
+    static HostPool* p = new HostPool;   // never destroyed: slots may be released during exit
+    return *p;
+}
+}  // namespace
+
+int host_mapped_alloc(size_t bytes, void** host, void** dev) {
+    *host = *dev = nullptr;
+    int c = 0;
+    while (c < kHostClasses && (size_t(256) << c) < bytes) ++c;
+    if (c == kHostClasses) {
+        set_error("mapped host buffer of %zu bytes above the slot limit", bytes);
+        return ORF_EINVAL;
+    }
+    const size_t sz = size_t(256) << c;
+    HostPool& P = host_pool();
+    void* h = nullptr;
+    {
+        std::lock_guard<std::mutex> g(P.mu);
+        if (!P.idle[c].empty()) {
+            h = P.idle[c].back();
+            P.idle[c].pop_back();
+        } else {
+            if (P.left < sz) {   // a new slab; the old tail stays unused
+                void* s = nullptr;
+                const cudaError_t e = cudaHostAlloc(&s, kHostSlab, cudaHostAllocMapped | cudaHostAllocPortable);
+                if (e != cudaSuccess) {
+                    cudaGetLastError();
+                    set_error("pinned host allocation failed: %s", cudaGetErrorString(e));
+                    return ORF_ECUDA;
+                }
+                P.cur = static_cast<char*>(s);
+                P.left = kHostSlab;
+            }
+            h = P.cur;   // every slot starts on a 256-byte boundary
+            P.cur += sz;
+            P.left -= sz;
+        }
+        P.cls[h] = c;
+    }
+    const cudaError_t e = cudaHostGetDevicePointer(dev, h, 0);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        host_mapped_free(h);
+        *dev = nullptr;
+        set_error("no device address for a mapped host buffer: %s", cudaGetErrorString(e));
+        return ORF_ECUDA;
+    }
+    *host = h;
+    return ORF_OK;
+}
+
+void host_mapped_free(void* host) {
+    if (!host) return;
+    HostPool& P = host_pool();
+    std::lock_guard<std::mutex> g(P.mu);
+    auto it = P.cls.find(host);
+    if (it == P.cls.end()) return;
+    P.idle[it->second].push_back(host);
+    P.cls.erase(it);
+}
+
 void set_error(const char* fmt, ...) {
     char buf[1024];
     va_list ap;

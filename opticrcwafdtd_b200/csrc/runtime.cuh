@@ -122,6 +122,15 @@ int dev_alloc(size_t bytes, void** out);
 void dev_free(void* p);
 void dev_trim(int device);                        // cudaFree the cached blocks of a device
 
+// Small mapped (zero-copy) host buffers -- a job's status ring and cancel
+// flag -- carved from pinned pages that the process keeps: a pair of
+// cudaHostAlloc / cudaFreeHost per job costs far more than the job's own
+// set-up when a batch holds hundreds of instances, and cudaFreeHost waits
+// for the device.  Slots are reused by later jobs, never unpinned; their
+// contents are not cleared.  dev receives the slot's device address.
+int host_mapped_alloc(size_t bytes, void** host, void** dev);
+void host_mapped_free(void* host);
+
 // Bump allocator over one device block: a job's buffers come from one block.
 struct Arena {
     std::vector<std::pair<void**, size_t>> req;
