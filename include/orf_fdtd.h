@@ -427,6 +427,38 @@ ORF_API int32_t orf_eps3d(orf_ctx* ctx, const double* x, const double* y, const 
                           const double* period,
                           int32_t nshape, const orf_eps_shape* shapes, double* ex, double* ey, double* ez);
 
+/* ---------------------------------------------------------------- FDFD --
+ * The 2D TE frequency-domain solver with its adjoint (toolbox/+orf/fdfd2D.m:1-19,
+ * `out = orf.fdfd2D(x, z, epsr, lambda0, J)`, out.solve, out.adjoint):
+ *   (1/s_x) d/dx((1/s_x) dE/dx) + (1/s_z) d/dz((1/s_z) dE/dz) + k0^2 eps E = -J
+ * for E = E_y on the grid's points (those of orf.fdtd2DTE), E = 0 outside,
+ * stretched-coordinate PML s = 1 + i a (depth/L)^3 (e^{-i w t} convention)
+ * of npml cells per side, a = 2 ln(1/R) / (k0 L), L = npml dx.
+ * orf_fdfd2d_factor builds the operator and factors it on the device (block
+ * LU along the longer axis; the shorter axis may hold at most 384 points);
+ * each orf_fdfd2d_solve is then one forward and one backward sweep.
+ * Complex arrays are interleaved (re, im) pairs of nx*nz entries in
+ * column-major order (entry (i, k) at i + nx*k), as MATLAB's interleaved
+ * complex API hands them over. */
+typedef struct orf_fdfd2d {
+    int32_t nx, nz;
+    double dx;                 /* grid spacing, the same on both axes [um] */
+    const double* eps;         /* relative permittivity, complex (nx*nz pairs) */
+    double lambda0;            /* vacuum wavelength [um]; k0 = 2 pi / lambda0 */
+    int32_t npml_x, npml_z;    /* PML cells per side (Npml, default 30 30) */
+    double pml_reflection;     /* PmlReflection (default 1e-8) */
+} orf_fdfd2d;
+typedef struct orf_fdfd orf_fdfd;   /* factored operator, device-resident */
+
+ORF_API int32_t orf_fdfd2d_factor(orf_ctx* ctx, const orf_fdfd2d* problem, orf_fdfd** out);
+/* transpose 0: solves A x = -rhs (the field E for a current J = rhs, out.E /
+ * out.solve(J2)); transpose 1: solves A.' x = rhs (out.adjoint(g): for a
+ * figure of merit c = sum(g .* E), dc/deps = -k0^2 x .* E). */
+ORF_API int32_t orf_fdfd2d_solve(orf_fdfd* f, const double* rhs, double* x, int32_t transpose);
+/* block size (shorter axis), number of blocks, CTAs of the solver's cluster */
+ORF_API int32_t orf_fdfd2d_info(const orf_fdfd* f, int32_t* block, int32_t* nblocks, int32_t* cluster);
+ORF_API void    orf_fdfd2d_release(orf_fdfd* f);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,5 +1,6 @@
 """opticrcwafdtd_b200 -- B200-native Yee FDTD engine for OpticRCWAFDTD's
-orf.fdtd2D / orf.fdtd2DTE / orf.fdtd3D (toolbox/+orf/fdtd2D.m, fdtd3D.m).
+orf.fdtd2D / orf.fdtd2DTE / orf.fdtd3D (toolbox/+orf/fdtd2D.m, fdtd3D.m), and
+its 2D frequency-domain solver orf.fdfd2D (toolbox/+orf/fdfd2D.m).
 
 The time loop runs in liborf_fdtd.so (hand-written sm_100a CUDA behind the C
 ABI in include/orf_fdtd.h).  This package is the host-side mirror of the
@@ -16,3 +17,4 @@ from .coupler import (apodizedGrating, bestFiberCoupling, fiberCoupling, grating
 
 __version__ = "0.1.0"
 from .fdtd import Context, Job, Server, device_count, fdtd2D, fdtd2D_batch, fdtd2DTE, fdtd3D  # noqa: F401,E402
+from .fdfd import FDFD2D, fdfd2D  # noqa: F401,E402

@@ -130,6 +130,12 @@ class OrfServeJobInfo(C.Structure):
                 ("reserved", C.c_int32)]
 
 
+class OrfFdfd2D(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("nz", C.c_int32), ("dx", C.c_double), ("eps", c_double_p),
+                ("lambda0", C.c_double), ("npml_x", C.c_int32), ("npml_z", C.c_int32),
+                ("pml_reflection", C.c_double)]
+
+
 class OrfError(RuntimeError):
     """Error raised for a non-zero orf_status; ``identifier`` mirrors MATLAB's
     error identifiers (e.g. ``'orf:cancelled'``, tests/TestGUISupport.m:39-43)."""

@@ -68,6 +68,10 @@ _SIGS = {
                               C.c_int32, C.c_double, C.c_int32, C.c_int32, P(C.c_double), C.c_int32, C.c_void_p,
                               P(C.c_double), P(C.c_double), P(C.c_double)]),
     "orf_serve_clock": (C.c_double, [C.c_void_p]),
+    "orf_fdfd2d_factor": (C.c_int32, [C.c_void_p, P(_abi.OrfFdfd2D), P(C.c_void_p)]),
+    "orf_fdfd2d_solve": (C.c_int32, [C.c_void_p, P(C.c_double), P(C.c_double), C.c_int32]),
+    "orf_fdfd2d_info": (C.c_int32, [C.c_void_p, P(C.c_int32), P(C.c_int32), P(C.c_int32)]),
+    "orf_fdfd2d_release": (None, [C.c_void_p]),
     "orf_serve_close": (C.c_int32, [C.c_void_p]),
     "orf_check_violations": (C.c_int32, [P(C.c_uint64), C.c_int32]),
 }

@@ -1,0 +1,590 @@
+// fdfd.cu -- orf_fdfd2d_*: the 2D TE frequency-domain solver with its adjoint
+// (toolbox/+orf/fdfd2D.m:1-19) on the device.
+//
+//   (1/s_x) d/dx((1/s_x) dE/dx) + (1/s_z) d/dz((1/s_z) dE/dz) + k0^2 eps E = -J
+//
+// on the FDTD's E_y points, E = 0 outside the grid, stretched-coordinate PML
+// s = 1 + i a (depth / L)^3 (e^{-i w t}), discretised with the 5-point
+// stencil.  Ordered block by block along the longer axis, the matrix is block
+// tridiagonal: blocks of m = min(nx, nz) unknowns (one line across the
+// shorter axis), tridiagonal diagonal blocks, diagonal couplings to the
+// neighbouring lines.  The factorisation is the block LU of that structure,
+//   D_0 = A_00,  D_b = A_bb - B_b D_{b-1}^{-1} C_{b-1},
+// with every D_b inverted by Gauss-Jordan elimination with partial pivoting
+// and the inverses kept on the device; a solve is then a forward and a
+// backward sweep of matrix-vector products with them (m^2 per line), for A
+// and, with the same inverses, for A.' (the adjoint, fdfd2D.m:13-15).
+//
+// The block inversions run on one thread-block cluster of 8 or 16 CTAs: CTA c
+// holds rows [c R, c R + R) of the block in registers (thread j: column j),
+// and each pivot step exchanges the CTAs' pivot candidates, the pivot row and
+// the row it replaces through distributed shared memory, with one cluster
+// barrier per pivot.  The next block's Schur complement is formed from the
+// inverse while it is still in registers.  Cluster barriers are hardware
+// barriers: no CTA spins on memory.
+#include <cooperative_groups.h>
+
+#include <complex>
+
+#include "runtime.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace orf {
+namespace {
+
+constexpr int kFdMaxM = 384;      // largest block (the shorter grid axis)
+constexpr int kSolveThreads = 256;
+
+struct FdfdDev {
+    int m, nb;                 // block size, number of blocks
+    const double2* diag;       // [nb][m]
+    const double2* wm;         // [nb][m]: coupling to p - 1 inside the block
+    const double2* wp;         // [nb][m]: to p + 1
+    const double2* bm;         // [nb][m]: to the same p of block b - 1
+    const double2* bp;         // [nb][m]: to block b + 1
+    double2* inv;              // [nb][m][m]: D_b^{-1}, row-major
+    int* fault;                // a zero pivot (singular block)
+};
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double cabs2(double2 a) { return a.x * a.x + a.y * a.y; }
+
+// Block LU of the whole operator: block b inverted in place, stored to
+// P.inv[b], then turned into D_{b+1} = A - B D_b^{-1} C in registers.
+// Thread j holds column j of the CTA's RM (or fewer) rows; NT threads at most.
+template <int RM, int NT>
+__global__ void __launch_bounds__(NT, 1) k_fdfd_factor(FdfdDev P) {
+    cg::cluster_group cl = cg::this_cluster();
+    const int C = (int)cl.num_blocks();
+    const int c = (int)cl.block_rank();
+    const int m = P.m;
+    const int R = (m + C - 1) / C;
+    const int r0 = c * R;
+    const int nr = max(0, min(m, r0 + R) - r0);
+    const int j = threadIdx.x;
+    const bool col = j < m;
+
+    // per pivot parity: this CTA's candidate pivot row, its row k, and the
+    // candidate's |value|^2 and row index (read by the other CTAs)
+    __shared__ double2 s_cand[2][kFdMaxM];
+    __shared__ double2 s_rowk[2][kFdMaxM];
+    __shared__ double s_cval[2];
+    __shared__ int s_cidx[2];
+    __shared__ double2 s_f[RM];     // column k of the owned rows (after the exchange)
+    __shared__ double2 s_ip;        // 1 / pivot
+    __shared__ int s_best;
+    __shared__ int s_piv[kFdMaxM];
+    __shared__ int s_perm[kFdMaxM];
+    __shared__ double2 s_x[kFdMaxM];
+
+    double2 a[RM];
+#pragma unroll
+    for (int q = 0; q < RM; ++q) a[q] = make_double2(0.0, 0.0);
+    long long g = 0;   // pivot steps so far (buffer parity)
+
+    for (int b = 0; b < P.nb; ++b) {
+        // ---- D_b: the tridiagonal block minus B_b D_{b-1}^{-1} C_{b-1}
+        if (col) {
+            const double2 cpj = b > 0 ? P.bp[(size_t)(b - 1) * m + j] : make_double2(0.0, 0.0);
+#pragma unroll
+            for (int q = 0; q < RM; ++q) {
+                if (q >= nr) break;
+                const int p = r0 + q;
+                const size_t o = (size_t)b * m + p;
+                double2 v = make_double2(0.0, 0.0);
+                if (b > 0) {
+                    const double2 s = cmul(cmul(P.bm[o], a[q]), cpj);
+                    v = make_double2(-s.x, -s.y);
+                }
+                if (j == p) v = cadd(v, P.diag[o]);
+                else if (j == p - 1) v = cadd(v, P.wm[o]);
+                else if (j == p + 1) v = cadd(v, P.wp[o]);
+                a[q] = v;
+            }
+        }
+        // ---- Gauss-Jordan inversion in place, partial pivoting
+        for (int k = 0; k < m; ++k, ++g) {
+            const int par = (int)(g & 1);
+            if (j == k) {   // this CTA's candidate: the largest |a| of column k on rows >= k
+                double best = -1.0;
+                int bi = m;
+#pragma unroll
+                for (int q = 0; q < RM; ++q) {
+                    if (q >= nr) break;
+                    const int r = r0 + q;
+                    const double v = cabs2(a[q]);
+                    if (r >= k && v > best) {
+                        best = v;
+                        bi = r;
+                    }
+                }
+                s_cval[par] = best;
+                s_cidx[par] = bi;
+                s_best = bi;
+            }
+            __syncthreads();
+            const int bl = s_best;
+            if (col) {
+#pragma unroll
+                for (int q = 0; q < RM; ++q) {
+                    if (q >= nr) break;
+                    const int r = r0 + q;
+                    if (r == bl) s_cand[par][j] = a[q];
+                    if (r == k) s_rowk[par][j] = a[q];
+                }
+            }
+            cl.sync();   // candidates and rows of every CTA are published
+            // the pivot row: the largest candidate, the lowest row on a tie
+            // (every thread decides the same)
+            double best = -1.0;
+            int p = m, oc = 0;
+            for (int c2 = 0; c2 < C; ++c2) {
+                const double v = *cl.map_shared_rank(&s_cval[par], c2);
+                const int i = *cl.map_shared_rank(&s_cidx[par], c2);
+                if (i < m && (v > best || (v == best && i < p))) {
+                    best = v;
+                    p = i;
+                    oc = c2;
+                }
+            }
+            double2 prow = make_double2(0.0, 0.0);
+            if (col) {
+                prow = cl.map_shared_rank(&s_cand[par][0], oc)[j];
+                if (p != k && p >= r0 && p < r0 + nr) {   // row p takes the old row k
+                    const double2 rk = cl.map_shared_rank(&s_rowk[par][0], k / R)[j];
+#pragma unroll
+                    for (int q = 0; q < RM; ++q)
+                        if (r0 + q == p) a[q] = rk;
+                }
+            }
+            if (j == k) {
+#pragma unroll
+                for (int q = 0; q < RM; ++q) s_f[q] = a[q];
+                const double dd = cabs2(prow);
+                if (dd == 0.0) {
+                    atomicExch(P.fault, 1);
+                    s_ip = make_double2(0.0, 0.0);
+                } else {
+                    s_ip = make_double2(prow.x / dd, -prow.y / dd);
+                }
+            }
+            if (j == 0) s_piv[k] = p;
+            __syncthreads();
+            const double2 ip = s_ip;
+            const double2 pr = j == k ? ip : cmul(prow, ip);   // the scaled pivot row
+            if (col) {
+#pragma unroll
+                for (int q = 0; q < RM; ++q) {
+                    if (q >= nr) break;
+                    const int r = r0 + q;
+                    if (r == k) {
+                        a[q] = pr;
+                    } else {
+                        const double2 f = s_f[q];
+                        a[q] = j == k ? make_double2(-(f.x * ip.x - f.y * ip.y), -(f.x * ip.y + f.y * ip.x))
+                                      : csub(a[q], cmul(f, pr));
+                    }
+                }
+            }
+        }
+        // ---- undo the row exchanges on the columns of the inverse, last first:
+        // column j of D_b^{-1} is column perm[j] of what the threads hold
+        __syncthreads();
+        if (j == 0) {
+            for (int q = 0; q < m; ++q) s_perm[q] = q;
+            for (int k = m - 1; k >= 0; --k) {
+                const int pk = s_piv[k];
+                if (pk != k) {
+                    const int t = s_perm[k];
+                    s_perm[k] = s_perm[pk];
+                    s_perm[pk] = t;
+                }
+            }
+        }
+        __syncthreads();
+        const int src = col ? s_perm[j] : 0;
+#pragma unroll
+        for (int q = 0; q < RM; ++q) {
+            if (q >= nr) break;
+            if (col) s_x[j] = a[q];
+            __syncthreads();
+            if (col) a[q] = s_x[src];
+            __syncthreads();
+        }
+        if (col) {
+            double2* out = P.inv + (size_t)b * m * m;
+#pragma unroll
+            for (int q = 0; q < RM; ++q) {
+                if (q >= nr) break;
+                out[(size_t)(r0 + q) * m + j] = a[q];
+            }
+        }
+    }
+    cl.sync();   // no CTA leaves while another may still read its shared memory
+}
+
+// Forward and backward sweeps with the stored inverses.
+//   mode 0: A x = -rhs:   w_b = -rhs_b - B_b y_{b-1},  y_b = D_b^{-1} w_b,
+//                         x_b = y_b - D_b^{-1} C_b x_{b+1}
+//   mode 1: A.' x = rhs:  z_b = D_b^{-T} (rhs_b - C_{b-1} z_{b-1}),
+//                         x_{b-1} = z_{b-1} - D_{b-1}^{-T} B_b x_b
+// Vector entries are owned by the CTA that owns the row of the same index;
+// the products gather the whole vector (mode 0) or reduce partial sums over
+// the owned rows (mode 1) through distributed shared memory, one cluster
+// barrier per line.
+__global__ void __launch_bounds__(kSolveThreads, 1) k_fdfd_solve(FdfdDev P, const double2* rhs, double2* x,
+                                                                  double2* Y, int mode) {
+    cg::cluster_group cl = cg::this_cluster();
+    const int C = (int)cl.num_blocks();
+    const int c = (int)cl.block_rank();
+    const int m = P.m, nb = P.nb;
+    const int R = (m + C - 1) / C;
+    const int r0 = c * R;
+    const int nr = max(0, min(m, r0 + R) - r0);
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    constexpr int NW = kSolveThreads / 32;
+    __shared__ double2 s_pub[2][kFdMaxM];   // published own entries (mode 0) / partial sums (mode 1)
+    __shared__ double2 s_full[kFdMaxM];     // mode 0: the gathered vector
+    __shared__ double2 s_u[kFdMaxM];        // mode 1: the owned entries of the multiplied vector
+    long long g = 0;
+    auto warp_sum = [&](double2 v) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+            v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+        }
+        return v;
+    };
+    if (mode == 0) {
+        // dst_b = D_b^{-1} s_full on the owned rows (base_b minus it when base is given)
+        auto gemv_rows = [&](int b, const double2* base, double2* dst) {
+            const double2* Ib = P.inv + (size_t)b * m * m;
+            for (int q = warp; q < nr; q += NW) {
+                const int p = r0 + q;
+                const double2* row = Ib + (size_t)p * m;
+                double2 acc = make_double2(0.0, 0.0);
+                for (int jj = lane; jj < m; jj += 32) acc = cadd(acc, cmul(row[jj], s_full[jj]));
+                acc = warp_sum(acc);
+                if (lane == 0) dst[(size_t)b * m + p] = base ? csub(base[(size_t)b * m + p], acc) : acc;
+            }
+        };
+        for (int b = 0; b < nb; ++b, ++g) {
+            const int par = (int)(g & 1);
+            for (int q = t; q < nr; q += kSolveThreads) {
+                const int p = r0 + q;
+                const size_t o = (size_t)b * m + p;
+                double2 w = make_double2(-rhs[o].x, -rhs[o].y);
+                if (b > 0) w = csub(w, cmul(P.bm[o], Y[o - m]));
+                s_pub[par][p] = w;
+            }
+            cl.sync();
+            for (int jj = t; jj < m; jj += kSolveThreads) s_full[jj] = cl.map_shared_rank(&s_pub[par][0], jj / R)[jj];
+            __syncthreads();
+            gemv_rows(b, nullptr, Y);
+            __syncthreads();
+        }
+        for (int q = t; q < nr; q += kSolveThreads) {
+            const size_t o = (size_t)(nb - 1) * m + r0 + q;
+            x[o] = Y[o];
+        }
+        __syncthreads();
+        for (int b = nb - 2; b >= 0; --b, ++g) {
+            const int par = (int)(g & 1);
+            for (int q = t; q < nr; q += kSolveThreads) {
+                const int p = r0 + q;
+                const size_t o = (size_t)b * m + p;
+                s_pub[par][p] = cmul(P.bp[o], x[o + m]);
+            }
+            cl.sync();
+            for (int jj = t; jj < m; jj += kSolveThreads) s_full[jj] = cl.map_shared_rank(&s_pub[par][0], jj / R)[jj];
+            __syncthreads();
+            gemv_rows(b, Y, x);
+            __syncthreads();
+        }
+    } else {
+        // partial sums of D_b^{-T} u over the owned rows, for every column
+        auto partial = [&](int b, int par) {
+            const double2* Ib = P.inv + (size_t)b * m * m;
+            for (int jj = t; jj < m; jj += kSolveThreads) {
+                double2 acc = make_double2(0.0, 0.0);
+                for (int q = 0; q < nr; ++q) acc = cadd(acc, cmul(Ib[(size_t)(r0 + q) * m + jj], s_u[q]));
+                s_pub[par][jj] = acc;
+            }
+        };
+        auto reduce_own = [&](int par, int q) {
+            double2 s = make_double2(0.0, 0.0);
+            for (int c2 = 0; c2 < C; ++c2) s = cadd(s, cl.map_shared_rank(&s_pub[par][0], c2)[r0 + q]);
+            return s;
+        };
+        for (int b = 0; b < nb; ++b, ++g) {
+            const int par = (int)(g & 1);
+            for (int q = t; q < nr; q += kSolveThreads) {
+                const size_t o = (size_t)b * m + r0 + q;
+                double2 u = rhs[o];
+                if (b > 0) u = csub(u, cmul(P.bp[o - m], Y[o - m]));
+                s_u[q] = u;
+            }
+            __syncthreads();
+            partial(b, par);
+            cl.sync();
+            for (int q = t; q < nr; q += kSolveThreads) Y[(size_t)b * m + r0 + q] = reduce_own(par, q);
+            __syncthreads();
+        }
+        for (int q = t; q < nr; q += kSolveThreads) {
+            const size_t o = (size_t)(nb - 1) * m + r0 + q;
+            x[o] = Y[o];
+        }
+        __syncthreads();
+        for (int b = nb - 1; b >= 1; --b, ++g) {
+            const int par = (int)(g & 1);
+            for (int q = t; q < nr; q += kSolveThreads) {
+                const size_t o = (size_t)b * m + r0 + q;
+                s_u[q] = cmul(P.bm[o], x[o]);
+            }
+            __syncthreads();
+            partial(b - 1, par);
+            cl.sync();
+            for (int q = t; q < nr; q += kSolveThreads) {
+                const size_t o = (size_t)(b - 1) * m + r0 + q;
+                x[o] = csub(Y[o], reduce_own(par, q));
+            }
+            __syncthreads();
+        }
+    }
+    cl.sync();   // no CTA leaves while another may still read its shared memory
+}
+
+// cluster size and rows per CTA for block size m (threads: m rounded up to
+// a warp, at most C * RM)
+int fd_shape(int m, int* C, int* RM) {
+    static const int kC[3] = {8, 8, 16}, kR[3] = {16, 32, 24};
+    for (int q = 0; q < 3; ++q)
+        if (kC[q] * kR[q] >= m) {
+            *C = kC[q];
+            *RM = kR[q];
+            return ORF_OK;
+        }
+    set_error("fdfd2D: the shorter grid axis has %d points, above the %d this solver takes", m, kFdMaxM);
+    return ORF_ETOOLARGE;
+}
+
+template <class K, class... Args>
+cudaError_t launch_cluster(K kern, int C, int threads, cudaStream_t s, Args... args) {
+    if (C > 8) {
+        const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        if (e != cudaSuccess) return e;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)C, 1, 1);
+    cfg.blockDim = dim3((unsigned)threads, 1, 1);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = (unsigned)C;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
+using cplx = std::complex<double>;
+
+// s at the integer points (half = false) or at the half points u = -1/2 ..
+// n-1/2 (half = true) of one axis: s = 1 + i a (depth / L)^3 inside the
+// npml-cell layers, depth = npml - u below the low edge, u - (n-1-npml)
+// above the high edge (the FDTD's CPML convention), a = 2 ln(1/R) / (k0 L)
+std::vector<cplx> fd_stretch(int n, int npml, double d, double k0, double R, bool half) {
+    const int npts = half ? n + 1 : n;
+    std::vector<cplx> s(npts, cplx(1.0, 0.0));
+    if (npml <= 0) return s;
+    const double L = npml * d;
+    const double a = 2.0 * std::log(1.0 / R) / (k0 * L);
+    const double lo = npml, hi = (n - 1) - npml;
+    for (int q = 0; q < npts; ++q) {
+        const double u = half ? q - 0.5 : (double)q;
+        double depth = 0.0;
+        if (u < lo) depth = lo - u;
+        else if (u > hi) depth = u - hi;
+        const double r = depth * d / L;
+        s[q] = cplx(1.0, a * r * r * r);
+    }
+    return s;
+}
+
+}  // namespace
+}  // namespace orf
+
+using namespace orf;
+
+struct orf_fdfd {
+    orf_ctx* ctx = nullptr;
+    int nx = 0, nz = 0, m = 0, nb = 0, C = 8, RM = 16;
+    bool along_x = true;   // blocks are lines of constant x (m = nz)
+    Arena ar;
+    double2 *diag = nullptr, *wm = nullptr, *wp = nullptr, *bm = nullptr, *bp = nullptr;
+    double2 *inv = nullptr, *Y = nullptr, *vin = nullptr, *vout = nullptr;
+    int* fault = nullptr;
+    ~orf_fdfd() {
+        if (ar.base) {
+            cudaStreamSynchronize(ctx->stream);
+            ar.release();
+        }
+        if (ctx) ctx_release(ctx);
+    }
+    FdfdDev dev() const { return FdfdDev{m, nb, diag, wm, wp, bm, bp, inv, fault}; }
+    // (i, k) of the grid <-> entry b * m + p of the block layout
+    size_t at(int i, int k) const { return along_x ? (size_t)i * m + k : (size_t)k * m + i; }
+};
+
+extern "C" int32_t orf_fdfd2d_factor(orf_ctx* ctx, const orf_fdfd2d* pr, orf_fdfd** out) {
+    if (!out) {
+        set_error("out is null");
+        return ORF_EINVAL;
+    }
+    *out = nullptr;
+    if (!ctx || !pr || !pr->eps) {
+        set_error("ctx, problem and eps are required");
+        return ORF_EINVAL;
+    }
+    const int nx = pr->nx, nz = pr->nz;
+    if (nx < 3 || nz < 3 || !(pr->dx > 0) || !(pr->lambda0 > 0)) {
+        set_error("fdfd2D: needs at least 3 x 3 points, dx > 0 and lambda0 > 0");
+        return ORF_EINVAL;
+    }
+    if (pr->npml_x < 0 || pr->npml_z < 0 || 2 * pr->npml_x >= nx || 2 * pr->npml_z >= nz) {
+        set_error("fdfd2D: Npml must leave interior points on both axes");
+        return ORF_EINVAL;
+    }
+    if (!(pr->pml_reflection > 0 && pr->pml_reflection < 1)) {
+        set_error("fdfd2D: PmlReflection must lie in (0, 1)");
+        return ORF_EINVAL;
+    }
+    ORF_ON_DEVICE(ctx->device);
+    auto F = std::make_unique<orf_fdfd>();
+    F->nx = nx;
+    F->nz = nz;
+    F->along_x = nz <= nx;
+    F->m = F->along_x ? nz : nx;
+    F->nb = F->along_x ? nx : nz;
+    ORF_TRY(fd_shape(F->m, &F->C, &F->RM));
+    const int m = F->m, nb = F->nb;
+    const size_t N = (size_t)nx * nz;
+
+    // ---- operator coefficients, rows scaled as in A E = -J
+    const double d = pr->dx, k0 = 2.0 * kPi / pr->lambda0, R = pr->pml_reflection;
+    const auto sxi = fd_stretch(nx, pr->npml_x, d, k0, R, false), sxh = fd_stretch(nx, pr->npml_x, d, k0, R, true);
+    const auto szi = fd_stretch(nz, pr->npml_z, d, k0, R, false), szh = fd_stretch(nz, pr->npml_z, d, k0, R, true);
+    std::vector<double2> hd(N), hwm(N), hwp(N), hbm(N), hbp(N);
+    const double h2 = 1.0 / (d * d);
+    auto d2 = [](cplx v) { return make_double2(v.real(), v.imag()); };
+    for (int k = 0; k < nz; ++k)
+        for (int i = 0; i < nx; ++i) {
+            const cplx cxm = h2 / (sxi[i] * sxh[i]), cxp = h2 / (sxi[i] * sxh[i + 1]);
+            const cplx czm = h2 / (szi[k] * szh[k]), czp = h2 / (szi[k] * szh[k + 1]);
+            const size_t g = (size_t)i + (size_t)nx * k;
+            const cplx eps(pr->eps[2 * g], pr->eps[2 * g + 1]);
+            const cplx dg = -(cxm + cxp + czm + czp) + k0 * k0 * eps;
+            const size_t o = F->at(i, k);
+            hd[o] = d2(dg);
+            hwm[o] = d2(F->along_x ? czm : cxm);
+            hwp[o] = d2(F->along_x ? czp : cxp);
+            hbm[o] = d2(F->along_x ? cxm : czm);
+            hbp[o] = d2(F->along_x ? cxp : czp);
+        }
+
+    F->ctx = ctx;
+    ctx_retain(ctx);
+    Arena& ar = F->ar;
+    ar.add(&F->diag, N);
+    ar.add(&F->wm, N);
+    ar.add(&F->wp, N);
+    ar.add(&F->bm, N);
+    ar.add(&F->bp, N);
+    ar.add(&F->inv, (size_t)nb * m * m);
+    ar.add(&F->Y, N);
+    ar.add(&F->vin, N);
+    ar.add(&F->vout, N);
+    ar.add(&F->fault, 1);
+    ORF_TRY(ar.alloc());
+    cudaStream_t st = ctx->stream;
+    ORF_CUDA(cudaMemcpyAsync(F->diag, hd.data(), N * sizeof(double2), cudaMemcpyHostToDevice, st));
+    ORF_CUDA(cudaMemcpyAsync(F->wm, hwm.data(), N * sizeof(double2), cudaMemcpyHostToDevice, st));
+    ORF_CUDA(cudaMemcpyAsync(F->wp, hwp.data(), N * sizeof(double2), cudaMemcpyHostToDevice, st));
+    ORF_CUDA(cudaMemcpyAsync(F->bm, hbm.data(), N * sizeof(double2), cudaMemcpyHostToDevice, st));
+    ORF_CUDA(cudaMemcpyAsync(F->bp, hbp.data(), N * sizeof(double2), cudaMemcpyHostToDevice, st));
+    ORF_CUDA(cudaMemsetAsync(F->fault, 0, sizeof(int), st));
+    add_h2d(ctx, (int64_t)(5 * N * sizeof(double2)));
+    const int threads = (m + 31) / 32 * 32;
+    const FdfdDev P = F->dev();
+    cudaError_t e;
+    switch (F->RM) {
+        case 16: e = launch_cluster(k_fdfd_factor<16, 128>, F->C, threads, st, P); break;
+        case 32: e = launch_cluster(k_fdfd_factor<32, 256>, F->C, threads, st, P); break;
+        default: e = launch_cluster(k_fdfd_factor<24, 384>, F->C, threads, st, P); break;
+    }
+    ORF_CUDA(e);
+    int fault = 0;
+    ORF_CUDA(cudaMemcpyAsync(&fault, F->fault, sizeof(int), cudaMemcpyDeviceToHost, st));
+    ORF_CUDA(cudaStreamSynchronize(st));
+    if (fault) {
+        set_error("fdfd2D: the operator is singular (a zero pivot in the block elimination)");
+        return ORF_EINVAL;
+    }
+    *out = F.release();
+    return ORF_OK;
+}
+
+extern "C" int32_t orf_fdfd2d_solve(orf_fdfd* F, const double* rhs, double* x, int32_t transpose) {
+    if (!F || !rhs || !x) {
+        set_error("fdfd handle, rhs and x are required");
+        return ORF_EINVAL;
+    }
+    ORF_ON_DEVICE(F->ctx->device);
+    const size_t N = (size_t)F->nx * F->nz;
+    std::vector<double2> h(N);
+    for (int k = 0; k < F->nz; ++k)
+        for (int i = 0; i < F->nx; ++i) {
+            const size_t g = (size_t)i + (size_t)F->nx * k;
+            h[F->at(i, k)] = make_double2(rhs[2 * g], rhs[2 * g + 1]);
+        }
+    cudaStream_t st = F->ctx->stream;
+    ORF_CUDA(cudaMemcpyAsync(F->vin, h.data(), N * sizeof(double2), cudaMemcpyHostToDevice, st));
+    add_h2d(F->ctx, (int64_t)(N * sizeof(double2)));
+    ORF_CUDA(launch_cluster(k_fdfd_solve, F->C, kSolveThreads, st, F->dev(), (const double2*)F->vin, F->vout, F->Y,
+                            transpose ? 1 : 0));
+    ORF_CUDA(cudaMemcpyAsync(h.data(), F->vout, N * sizeof(double2), cudaMemcpyDeviceToHost, st));
+    ORF_CUDA(cudaStreamSynchronize(st));
+    add_d2h(F->ctx, (int64_t)(N * sizeof(double2)));
+    for (int k = 0; k < F->nz; ++k)
+        for (int i = 0; i < F->nx; ++i) {
+            const size_t g = (size_t)i + (size_t)F->nx * k;
+            const double2 v = h[F->at(i, k)];
+            x[2 * g] = v.x;
+            x[2 * g + 1] = v.y;
+        }
+    return ORF_OK;
+}
+
+extern "C" void orf_fdfd2d_release(orf_fdfd* F) {
+    if (!F) return;
+    DeviceScope ds(F->ctx->device);
+    delete F;
+}
+
+extern "C" int32_t orf_fdfd2d_info(const orf_fdfd* F, int32_t* block, int32_t* nblocks, int32_t* cluster) {
+    if (!F) {
+        set_error("fdfd handle is null");
+        return ORF_EINVAL;
+    }
+    if (block) *block = F->m;
+    if (nblocks) *nblocks = F->nb;
+    if (cluster) *cluster = F->C;
+    return ORF_OK;
+}

@@ -277,3 +277,23 @@ def serve_stream(n_jobs: int = 32, seed: int = 5, rate: float = 1.0, cells=(2e5,
             sim = _coupler_instance(nx, nz, period, ff, etch, st, precision, n_lambda)
             jobs.append(dict(t=t, dims=2, cells=nx * nz, steps=st, sim=sim))
     return jobs
+
+
+def fdfd_straight_guide(d: float = 0.02, lam: float = 1.55):
+    """The FDFD straight-guide problem of tests/TestInverseDesign.m:12-24: an
+    SOI slab (Si substrate below z = -2, 2 um BOX n = 1.444, 220 nm Si
+    n = 3.476, air above) on x in [0, 10], z in [-2.6, 1.8] um (cell
+    centres), fed at x = 2 um by its TE0 mode, solved over the window
+    -1.5 < z < z_end - 30 d.  Returns (x, z, epsr, lam, J, mode, win)."""
+    from .geometry import epsFromBoxes
+    x = np.round(np.arange(0, 10 + d / 2, d), 12)
+    z = np.arange(-2.6, 1.8 + d / 2, d) + d / 2
+    epsr = epsFromBoxes(x, z, 1.0, np.array([[-np.inf, np.inf, -np.inf, -2, 3.476],
+                                             [-np.inf, np.inf, -2, 0, 1.444],
+                                             [-np.inf, np.inf, 0, 0.22, 3.476]]))
+    win = (z > -1.5) & (z < z[-1] - 30 * d)
+    i0 = int(round(2 / d))
+    m = slabModes(z[win], np.sqrt(epsr[i0, win]), lam, "TE")
+    J = np.zeros((x.size, z.size))
+    J[i0, win] = np.real(m["field"][:, 0])
+    return x, z, epsr, lam, J, m, win
