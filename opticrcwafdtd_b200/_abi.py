@@ -262,23 +262,45 @@ def marshal_sim2d(sim: Any) -> Marshalled:
                                 "nM": mons.size, "nMZ": monz.size, "lambdas": lam})
 
 
-def alloc_out2d(m: Marshalled) -> tuple[OrfOut2D, dict]:
+def _out2d_shapes(m: Marshalled) -> dict:
     nx, nz, nL, nM, nMZ = (m.meta[k] for k in ("nx", "nz", "nL", "nM", "nMZ"))
-    # the DFT lines are written in full by the run's results (no zero fill)
-    bufs = {
-        "flux": np.zeros((nM, nL), order="F"),
-        "fluxZ": np.zeros((nMZ, nL), order="F"),
-        "P": np.empty((nz, nL, nM), dtype=np.complex128, order="F"),
-        "B": np.empty((nz, nL, nM), dtype=np.complex128, order="F"),
-        "PZ": np.empty((nx, nL, nMZ), dtype=np.complex128, order="F"),
-        "AZ": np.empty((nx, nL, nMZ), dtype=np.complex128, order="F"),
-    }
+    return {"P": (nz, nL, nM), "B": (nz, nL, nM), "PZ": (nx, nL, nMZ), "AZ": (nx, nL, nMZ)}
+
+
+def alloc_out2d(m: Marshalled, slab: np.ndarray | None = None) -> tuple[OrfOut2D, dict]:
+    """Output buffers of one 2D run.  The DFT lines are written in full by
+    the run's results (no zero fill); slab (a flat complex128 array, see
+    alloc_out2d_many) holds them when given."""
+    nL, nM, nMZ = (m.meta[k] for k in ("nL", "nM", "nMZ"))
+    bufs = {"flux": np.zeros((nM, nL), order="F"), "fluxZ": np.zeros((nMZ, nL), order="F")}
+    off = 0
+    for k, shp in _out2d_shapes(m).items():
+        n = int(np.prod(shp))
+        if slab is None:
+            bufs[k] = np.empty(shp, dtype=np.complex128, order="F")
+        else:
+            bufs[k] = slab[off:off + n].reshape(shp, order="F")
+            off += n
     o = OrfOut2D()
     o.flux = _ptr(bufs["flux"]) if bufs["flux"].size else None
     o.flux_z = _ptr(bufs["fluxZ"]) if bufs["fluxZ"].size else None
     for k in ("P", "B", "PZ", "AZ"):
         setattr(o, k, _ptr(bufs[k]) if bufs[k].size else None)
     return o, bufs
+
+
+def alloc_out2d_many(ms: list) -> list:
+    """Output buffers of a batch: the DFT lines of every instance carved from
+    one allocation (a batch of couplers returns most of a gigabyte; its
+    pages are first written by the host threads finishing the batch, in
+    parallel)."""
+    sizes = [sum(int(np.prod(s)) for s in _out2d_shapes(m).values()) for m in ms]
+    slab = np.empty(sum(sizes), dtype=np.complex128)
+    outs, off = [], 0
+    for m, n in zip(ms, sizes):
+        outs.append(alloc_out2d(m, slab[off:off + n]))
+        off += n
+    return outs
 
 
 def finish_out2d(m: Marshalled, o: OrfOut2D, bufs: dict) -> dict:

@@ -713,20 +713,30 @@ int Job2D<R>::finish2d_on(orf_out2d* o, cudaStream_t st) {
     std::vector<double> fl((size_t)(nM + nMZ) * nL);
     if (!fl.empty()) ORF_CUDA(cudaMemcpyAsync(fl.data(), d_flux, fl.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
     d2h += (int64_t)(fl.size() * sizeof(double));
-    // DFT lines: stream q -> complex [l][e]
+    // DFT lines: stream q -> complex [l][e], through a pinned staging buffer
+    // (in no-allocation mode straight into the caller's buffers)
+    void* stage = nullptr;
+    if (!ext_base) ORF_TRY(pinned_stage_acquire(&stage));
+    struct StageGuard {
+        void* p;
+        ~StageGuard() { pinned_stage_release(p); }
+    } stage_guard{stage};
     auto fetch = [&](int q, double* dst) -> int {
         if (!dst) return ORF_OK;
         const DftStream& S = host_streams[q];
         const size_t n = (size_t)S.len * nL;
         d2h += (int64_t)(n * sizeof(double2));
-        if (f64) {
-            ORF_CUDA(cudaMemcpyAsync(dst, S.acc, n * sizeof(double2), cudaMemcpyDeviceToHost, st));
-        } else {
+        const void* src = S.acc;
+        if (!f64) {   // FP32 sums with their compensation -> complex doubles
             ORF_CUDA(launch_acc_to_complex(false, S.acc, n, d_stage, st));
-            ORF_CUDA(cudaMemcpyAsync(dst, d_stage, n * sizeof(double2), cudaMemcpyDeviceToHost, st));
-            ORF_CUDA(cudaStreamSynchronize(st));   // staging buffer is reused
+            src = d_stage;
         }
-        return ORF_OK;
+        if (!stage) {
+            ORF_CUDA(cudaMemcpyAsync(dst, src, n * sizeof(double2), cudaMemcpyDeviceToHost, st));
+            ORF_CUDA(cudaStreamSynchronize(st));   // the device staging buffer is reused
+            return ORF_OK;
+        }
+        return copy_d2h_staged(dst, src, n * sizeof(double2), stage, st);
     };
     for (int m = 0; m < nM; ++m) {
         ORF_TRY(fetch(2 * m, o->P ? o->P + (size_t)2 * nz * nL * m : nullptr));

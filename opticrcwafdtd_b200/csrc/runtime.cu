@@ -1,4 +1,5 @@
 // runtime.cu -- errors, shared physics definitions, context, chunk engine.
+#include <algorithm>
 #include <atomic>
 #include <map>
 #include <mutex>
@@ -203,6 +204,57 @@ void host_mapped_free(void* host) {
     if (it == P.cls.end()) return;
     P.idle[it->second].push_back(host);
     P.cls.erase(it);
+}
+
+namespace {
+struct StagePool {
+    std::mutex mu;
+    std::vector<void*> idle;
+};
+StagePool& stage_pool() {
+    static StagePool* p = new StagePool;   // never destroyed: buffers may be released during exit
+    return *p;
+}
+}  // namespace
+
+int pinned_stage_acquire(void** buf) {
+    *buf = nullptr;
+    StagePool& P = stage_pool();
+    {
+        std::lock_guard<std::mutex> g(P.mu);
+        if (!P.idle.empty()) {
+            *buf = P.idle.back();
+            P.idle.pop_back();
+            return ORF_OK;
+        }
+    }
+    const cudaError_t e = cudaHostAlloc(buf, kStageBytes, cudaHostAllocPortable);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *buf = nullptr;
+        set_error("pinned staging buffer: %s", cudaGetErrorString(e));
+        return ORF_ECUDA;
+    }
+    return ORF_OK;
+}
+
+void pinned_stage_release(void* buf) {
+    if (!buf) return;
+    StagePool& P = stage_pool();
+    std::lock_guard<std::mutex> g(P.mu);
+    P.idle.push_back(buf);
+}
+
+int copy_d2h_staged(void* dst, const void* src, size_t bytes, void* stage, cudaStream_t st) {
+    char* d = static_cast<char*>(dst);
+    const char* s = static_cast<const char*>(src);
+    for (size_t off = 0; off < bytes; off += kStageBytes) {
+        const size_t n = std::min(kStageBytes, bytes - off);
+        ORF_CUDA(cudaMemcpyAsync(stage, s + off, n, cudaMemcpyDeviceToHost, st));
+        ORF_CUDA(cudaStreamSynchronize(st));
+        std::memcpy(d + off, stage, n);
+    }
+    return ORF_OK;
 }
 
 void set_error(const char* fmt, ...) {

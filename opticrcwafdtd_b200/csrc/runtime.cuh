@@ -131,6 +131,18 @@ void dev_trim(int device);                        // cudaFree the cached blocks 
 int host_mapped_alloc(size_t bytes, void** host, void** dev);
 void host_mapped_free(void* host);
 
+// Pinned host staging buffers for device-to-host result copies, kept by the
+// process and reused: a copy into pinned memory runs at the link's speed,
+// and the host thread then moves it into the caller's (pageable) buffer, so
+// the several host threads finishing a batch copy in parallel.  Each buffer
+// holds kStageBytes; a thread takes one for the duration of its results.
+constexpr size_t kStageBytes = size_t(4) << 20;
+int pinned_stage_acquire(void** buf);
+void pinned_stage_release(void* buf);
+// Device-to-host copy of `bytes` from `src` into the pageable `dst` through
+// the staging buffer `stage`, on stream st (synchronises st).
+int copy_d2h_staged(void* dst, const void* src, size_t bytes, void* stage, cudaStream_t st);
+
 // Bump allocator over one device block: a job's buffers come from one block.
 struct Arena {
     std::vector<std::pair<void**, size_t>> req;

@@ -171,7 +171,7 @@ def fdtd2D_batch(sims, ctx: Context | None = None, progress=None, autotune: bool
     if not ms:
         return []
     arr = (_abi.OrfSim2D * len(ms))(*[m.struct for m in ms])
-    outs = [_abi.alloc_out2d(m) for m in ms]
+    outs = _abi.alloc_out2d_many(ms)
     oarr = (_abi.OrfOut2D * len(ms))(*[o for o, _ in outs])
     own = ctx is None
     if own:
