@@ -11,7 +11,7 @@ result's error against an FP64 run of the same job (error_vs_fp64); the FP64
 form itself is held to the FP64 oracle at this grid size by the GPU tests.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload pixel2d|coupler|pillar3d|coupler_batch|serve] [--no-forms]
+                    [--workload pixel2d|coupler|pillar3d|coupler_batch|serve|fdfd] [--no-forms]
 
 At N = 1 the headline line also carries one sub-record per other form of
 the engine, each with its own timing, clocks and roofline:
@@ -21,6 +21,8 @@ the engine, each with its own timing, clocks and roofline:
   c4_coupler_batch  256 uneven FP32 grating couplers, 10000 steps, one batched call
   c5_served         a Poisson stream of 100 mixed 2D / 3D FP32 jobs at 80 % of the
                     measured capacity through the serving loop (p50 / p99 latency)
+  fdfd2d            the 2D TE frequency-domain solver on a 501 x 221 SOI slab:
+                    factorisation, solve and adjoint solve times, error vs the oracle
 --workload runs one of them alone as its own line.
 
 Under torchrun every rank runs its own replica of the job on its GPU (a
@@ -64,7 +66,7 @@ def parse(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="headline only, without the sub-records")
-    ap.add_argument("--workload", default="pixel2d", choices=["pixel2d", "coupler", "pillar3d", "coupler_batch", "serve"],
+    ap.add_argument("--workload", default="pixel2d", choices=["pixel2d", "coupler", "pillar3d", "coupler_batch", "serve", "fdfd"],
                     help="pixel2d is the headline; the others measure one form alone")
     ap.add_argument("--batch", type=int, default=256)
     ap.add_argument("--size3d", default="600,600,300", help="pillar3d grid NX,NY,NZ (smaller for profiling)")
@@ -669,8 +671,72 @@ def bench_serve(args, rank, world, local, dist):
             "phase_s": phase, "clocks": clk.summary()}
 
 
+def bench_fdfd(args, rank, world, local, dist):
+    """The 2D TE frequency-domain solver (orf.fdfd2D, toolbox/+orf/fdfd2D.m)
+    on the reference's straight-guide problem: SOI slab, 501 x 221 points at
+    20 nm, 30-cell PML, TE0 source; one factorisation, one solve, one adjoint
+    solve, against the FDFD oracle (scipy sparse LU, one host thread)."""
+    import numpy as np
+    import torch
+    import opticrcwafdtd_b200 as orf
+    from opticrcwafdtd_b200 import workloads
+    x, z, epsr, lam, J, m, win = workloads.fdfd_straight_guide()
+    ctx = orf.Context(local)
+    g = np.conj(J)
+    for _ in range(max(1, args.warmup)):
+        orf.fdfd2D(x, z, epsr, lam, J, ctx=ctx).close()
+    reps = max(1, args.steps)
+    tf = ts = ta = 0.0
+    with ClockSampler(local) as clk:
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            o = orf.fdfd2D(x, z, epsr, lam, J, ctx=ctx)   # factorisation + the first solve
+            t1 = time.perf_counter()
+            o.solve(J)
+            t2 = time.perf_counter()
+            lam_ = o.adjoint(g)
+            t3 = time.perf_counter()
+            tf += (t1 - t0) - (t2 - t1)
+            ts += t2 - t1
+            ta += t3 - t2
+            E = o.E
+            info = o.info()
+            o.close()
+    torch.cuda.synchronize()
+    tf, ts, ta = 1e3 * tf / reps, 1e3 * ts / reps, 1e3 * ta / reps
+    mb, nb = info["block"], info["blocks"]
+    sweep_bytes = 2 * nb * mb * mb * 16          # the two sweeps read every block inverse once
+    peak, src = measured_peaks()
+    line = {"metric": "fdfd2D factor + solve", "value": tf + ts, "unit": "ms", "n_gpus": 1, "steps": reps,
+            "warmup": max(1, args.warmup), "ms_per_step": tf + ts + ta, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic (SOI slab, TE0 mode source)",
+            "config": {"workload": "FDFD 2D TE SOI slab 501x221 dx=20nm, 30-cell PML, one factorisation, "
+                                   "one solve, one adjoint solve", "block": mb, "blocks": nb,
+                       "cluster_ctas": info["cluster"]},
+            "factor_ms": tf, "solve_ms": ts, "adjoint_ms": ta,
+            "factor_gflops": 8.0 * nb * mb ** 3 / (tf / 1e3) / 1e9,
+            "solve_roofline": {"bound": "hbm", "achieved": sweep_bytes / (ts / 1e3) / 1e9, "peak": peak,
+                               "unit": "GB/s", "frac": sweep_bytes / (ts / 1e3) / 1e9 / peak, "peak_source": src,
+                               "note": "block inverses read by the two sweeps; host copies of J and E included"},
+            "clocks": clk.summary()}
+    if not args.no_cpu_baseline:
+        from oracle.fdfd import fdfd2D as ofdfd
+        t0 = time.perf_counter()
+        r = ofdfd(x, z, epsr, lam, J)
+        t1 = time.perf_counter()
+        ra = r.adjoint(g)
+        t2 = time.perf_counter()
+        rel = lambda a, b: float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
+        line["cpu_baseline"] = {"value": 1e3 * (t1 - t0), "unit": "ms", "cores": 1, "kind": "port",
+                                "sample": "the same factorisation + solve (scipy sparse LU, SuperLU)",
+                                "adjoint_ms": 1e3 * (t2 - t1)}
+        line["error_vs_oracle"] = {"E_rel_l2": rel(E, r.E), "adjoint_rel_l2": rel(lam_, ra)}
+    ctx.close()
+    return line
+
+
 WORKLOADS = {"pixel2d": bench_pixel2d, "coupler": bench_pixel2d, "pillar3d": bench_pillar3d,
-             "coupler_batch": bench_coupler_batch, "serve": bench_serve}
+             "coupler_batch": bench_coupler_batch, "serve": bench_serve, "fdfd": bench_fdfd}
 
 
 def run_forms(args, local):
@@ -686,6 +752,7 @@ def run_forms(args, local):
         ("c4_coupler_batch", "coupler_batch", dict(time_steps=10000, steps=3, warmup=3, precision="single",
                                                    batch=256)),
         ("c5_served", "serve", dict()),
+        ("fdfd2d", "fdfd", dict(steps=3, warmup=1)),
     ]
     out = {}
     for key, wl, kw in subs:
