@@ -114,11 +114,14 @@ int encode_fn(EncodeTiledFn* out) {
 }
 
 template <class R>
-int Job3D<R>::encode_tmap3(CUtensorMap* m, CUtensorMapDataType t, const void* base, size_t esz, int bx, int by) {
+int Job3D<R>::encode_tmap3(CUtensorMap* m, CUtensorMapDataType t, const void* base, size_t esz, int bx, int by,
+                           int rows_pitch, int nplanes) {
     EncodeTiledFn fn;
     ORF_TRY(encode_fn(&fn));
-    const cuuint64_t dims[3] = {(cuuint64_t)n[0], (cuuint64_t)n[1], (cuuint64_t)n[2]};
-    const cuuint64_t strides[2] = {(cuuint64_t)pitch * esz, (cuuint64_t)pitch * n[1] * esz};
+    const int rp = rows_pitch > 0 ? rows_pitch : pitch;
+    const int np = nplanes > 0 ? nplanes : n[2];
+    const cuuint64_t dims[3] = {(cuuint64_t)n[0], (cuuint64_t)n[1], (cuuint64_t)np};
+    const cuuint64_t strides[2] = {(cuuint64_t)rp * esz, (cuuint64_t)rp * n[1] * esz};
     const cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
     const cuuint32_t estr[3] = {1, 1, 1};
     const CUresult r = fn(m, t, 3, const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -436,6 +439,24 @@ int Job3D<R>::create(const orf_sim3d* s) {
                 ORF_TRY(encode_tmap3(&maps[6 + 3 * b + c], ft, h.H[b][c], sizeof(R), kTile3X + 8, kTile3Y + 1));
             }
         for (int c = 0; c < 3; ++c) ORF_TRY(encode_tmap3(&maps[12 + c], it, d_ix[c], idxw, kTile3X, kTile3Y));
+        // FP32 CPML tiles: the z-axis psi of the H update (psiH[b][c][2]) and
+        // of the E update (psiE[b][c][2]), c = 0, 1, planes of nx x ny in
+        // slab order, box 40 x 10 like E; rows of nx values must be a
+        // multiple of 16 bytes
+        h.tma_psi = 0;
+        bool zpsi = sizeof(R) == 4 && h.nslabH[2] > 0 && h.nslabI[2] > 0 && (n[0] * sizeof(R)) % 16 == 0;
+        for (int b = 0; b < 2; ++b)
+            for (int c = 0; c < 2; ++c) zpsi = zpsi && h.psiH[b][c][2] && h.psiE[b][c][2];
+        if (zpsi) {
+            for (int b = 0; b < 2; ++b)
+                for (int c = 0; c < 2; ++c) {
+                    ORF_TRY(encode_tmap3(&maps[15 + 2 * b + c], ft, h.psiH[b][c][2], sizeof(R), kTile3X + 8,
+                                         kTile3Y + 2, n[0], h.nslabH[2]));
+                    ORF_TRY(encode_tmap3(&maps[19 + 2 * b + c], ft, h.psiE[b][c][2], sizeof(R), kTile3X + 8,
+                                         kTile3Y + 2, n[0], h.nslabI[2]));
+                }
+            h.tma_psi = 1;
+        }
         ORF_TRY(up(d_tmap, maps.data(), maps.size() * sizeof(CUtensorMap)));
         h.tmap = d_tmap;
     }

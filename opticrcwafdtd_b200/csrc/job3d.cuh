@@ -58,8 +58,11 @@ struct Job3D : orf_job {
     int64_t step_budget() const override { return nmax; }
 
     int create(const orf_sim3d* s);
-    static constexpr int kTmaps3 = 15;   // E[2][3], H[2][3], index[3]
-    int encode_tmap3(CUtensorMap* m, CUtensorMapDataType t, const void* base, size_t esz, int bx, int by);
+    static constexpr int kTmaps3 = 23;   // E[2][3], H[2][3], index[3], z psi H[2][2], z psi E[2][2]
+    // rows_pitch / nplanes: row length and plane count of the array (the
+    // field pitch and nz unless given)
+    int encode_tmap3(CUtensorMap* m, CUtensorMapDataType t, const void* base, size_t esz, int bx, int by,
+                     int rows_pitch = 0, int nplanes = 0);
     int init_state();
     int advance(int64_t nsteps, orf_progress_fn progress, void* user) override;
     int64_t steps_done() override;

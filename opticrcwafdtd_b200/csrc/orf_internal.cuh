@@ -186,8 +186,11 @@ struct Inst3D {
     JobState* st;
     // TMA tensor maps (CUtensorMap, 128 B each) in device memory, or null:
     // [0..5] E[b][c] boxes 40 x 10 x 1, [6..11] H[b][c] boxes 40 x 9 x 1,
-    // [12..14] index[c] boxes 32 x 8 x 1 (b = buffer, c = component)
+    // [12..14] index[c] boxes 32 x 8 x 1 (b = buffer, c = component);
+    // when tma_psi: [15..18] psiH[b][c][2], [19..22] psiE[b][c][2] (c = 0, 1),
+    // boxes 40 x 10 x 1 over nx x ny x slab planes
     const void* tmap;
+    int tma_psi;
 };
 
 struct Tile3D {

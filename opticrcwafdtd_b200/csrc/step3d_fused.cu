@@ -26,6 +26,8 @@
 // and written once per step: 12 values plus 3 index bytes per cell, the
 // algorithmic minimum.  The arithmetic of every update is that of the split
 // H-then-E formulation, operation for operation.
+#include <type_traits>
+
 #include "orf_internal.cuh"
 
 namespace orf {
@@ -162,13 +164,18 @@ __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_grou
 template <int N>
 __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-template <class R, class IT>
-constexpr size_t slot_bytes() {   // 3 E blocks, 3 H blocks, 3 index blocks
-    return 3 * (size_t)EB<R> * sizeof(R) + 3 * (size_t)HB<R> * sizeof(R) + 3 * (size_t)NT * sizeof(IT);
+// FP32 CPML kernels carry the four z-axis psi planes of a cell's H and E
+// updates in the ring too (ZR); FP64 ones load them from global memory
+template <class R, bool PML>
+constexpr bool kZRing = PML && sizeof(R) == 4;
+template <class R, class IT, bool ZR>
+constexpr size_t slot_bytes() {   // 3 E blocks, 3 H blocks, 3 index blocks (+ 4 psi blocks)
+    return 3 * (size_t)EB<R> * sizeof(R) + 3 * (size_t)HB<R> * sizeof(R) + 3 * (size_t)NT * sizeof(IT) +
+           (ZR ? 4 * (size_t)EB<R> * sizeof(R) : 0);
 }
-template <class R, class IT>
+template <class R, class IT, bool ZR>
 constexpr size_t smem_bytes() {   // the ring, then the new-H plane, + 128 for alignment
-    return NS<R> * slot_bytes<R, IT>() + 3 * (size_t)EB<R> * sizeof(R) + 128;
+    return NS<R> * slot_bytes<R, IT, ZR>() + 3 * (size_t)EB<R> * sizeof(R) + 128;
 }
 
 __device__ __forceinline__ unsigned sm_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -269,13 +276,18 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
     // (the launch requests 128 spare bytes)
     unsigned char* dsm = dsm_raw + ((128u - (sm_addr(dsm_raw) & 127u)) & 127u);
     constexpr int EBr = EB<R>, HBr = HB<R>;
-    constexpr size_t SB = slot_bytes<R, IT>();
+    constexpr bool ZR = kZRing<R, PML>;
+    constexpr size_t SB = slot_bytes<R, IT, ZR>();
     // slot s: E component q at sEq(s, q), H at sHq(s, q), index at sIq(s, q);
     // region cell (r, c) (x = i0-1+c, y = j0-1+r) at r * SX + c + CX
     auto sEq = [&](int s2, int q) { return reinterpret_cast<R*>(dsm + s2 * SB) + q * EBr; };
     auto sHq = [&](int s2, int q) { return reinterpret_cast<R*>(dsm + s2 * SB) + 3 * EBr + q * HBr; };
     auto sIq = [&](int s2, int q) {
         return reinterpret_cast<IT*>(dsm + s2 * SB + 3 * (EBr + HBr) * sizeof(R)) + q * NT;
+    };
+    // ZR: z psi block q of slot s (0, 1: psiH of Hx, Hy; 2, 3: psiE of Ex, Ey), the E layout
+    auto sZq = [&](int s2, int q) {
+        return reinterpret_cast<R*>(dsm + s2 * SB + 3 * (EBr + HBr) * sizeof(R) + 3 * NT * sizeof(IT)) + q * EBr;
     };
     constexpr int ns = NS<R>;
     R* sHn = reinterpret_cast<R*>(dsm + ns * SB);      // [3][EB]
@@ -328,6 +340,10 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
     // memory, the entry every cell of a plane reads
     __shared__ R szp[PML ? 2 : 1][PML ? 3 * (kSeg3 + 2) : 1];
     const int np2 = PML ? sx.np[2] : 0;
+    // FP32 CPML tiles with a z slab on the TMA path take the z-axis psi of
+    // their cells through the ring as well (slab planes of the psi arrays)
+    const bool zring = ZR && use_tma && I->tma_psi != 0 && np2 > 0;
+    const unsigned tx_bytes = kTx + (zring ? 4u * (unsigned)(SX * RY * sizeof(R)) : 0u);
     if constexpr (PML) {
         const int cnt = k1 - k0 + 2;
         if (np2 > 0) {
@@ -374,7 +390,7 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
                 const int zc = pok ? pw : -1;   // z = -1: the whole box reads as zero
                 // order the block's earlier generic reads of this slot before the async writes
                 asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-                mbar_expect_tx(&sbar[s2], kTx);
+                mbar_expect_tx(&sbar[s2], tx_bytes);
                 s_issued = p;
                 // failure-detection test hook (off unless set on the host):
                 // the slot is armed but its copies are never issued
@@ -383,6 +399,14 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
                     tma_load3(sEq(s2, q), tm + 128 * (3 * par + q), i0 - 4, j0 - 1, zc, &sbar[s2]);
                     tma_load3(sHq(s2, q), tm + 128 * (6 + 3 * par + q), i0 - 4, j0 - 1, zc, &sbar[s2]);
                     tma_load3(sIq(s2, q), tm + 128 * (12 + q), i0, j0, zc, &sbar[s2]);
+                }
+                if (zring) {   // slab plane of the psi arrays, or z = -1 (zeros) off the slab
+                    const int zh = pok ? slab(true, pw, nz, np2) : -1;
+                    const int ze = pok ? slab(false, pw, nz, np2) : -1;
+                    for (int c = 0; c < 2; ++c) {
+                        tma_load3(sZq(s2, c), tm + 128 * (15 + 2 * par + c), i0 - 4, j0 - 1, zh, &sbar[s2]);
+                        tma_load3(sZq(s2, 2 + c), tm + 128 * (19 + 2 * par + c), i0 - 4, j0 - 1, ze, &sbar[s2]);
+                    }
                 }
             }
             return;
@@ -510,7 +534,8 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
     // of the plane's iteration, so the loads overlap the barriers and the H
     // phase instead of stalling the update (psi of buffer par is read-only)
     // (FP32: in FP64 the values held ahead would spill at three CTAs per SM)
-    const bool zpre = PML && sizeof(R) == 4 && np2 > 0;
+    const bool zpre = PML && sizeof(R) == 4 && np2 > 0 && !zring;
+    const bool zgiven = zpre || zring;   // the z-axis psi reach cpml6 from outside
     R zHo0 = R(0), zHo1 = R(0), zHh0 = R(0), zHh1 = R(0), zEo0 = R(0), zEo1 = R(0);
     auto load_zH = [&](int p) {
         const int sl = slab(true, p, nz, np2);
@@ -533,17 +558,12 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
         zEo0 = __ldg(sx.pin[0][0][2] + o);
         zEo1 = __ldg(sx.pin[0][1][2] + o);
     };
-    if (zpre) load_zH(k0);
-    for (int k = k0; k < k1; ++k) {
-        const int it = k - k0;
-        const int s0 = it % ns, s1 = (it + 1) % ns, sn = (it + ns - 1) % ns;
-        if (it == 0) wait_plane(k, s0);
-        wait_plane(k + 1, s1);   // planes k and k+1 have landed (later ones may be in flight)
-        __syncthreads();         // ... for every thread; everyone is done with plane k-1
-        if (s_abort) break;      // a wait ran out: the whole CTA leaves the march here
-        if (k + ns - 1 <= k1) load_plane(k + ns - 1, sn);   // into the slot of plane k-1
-        cp_commit();
-        if (zpre) load_zE(k);
+    // One plane of the march after its loads: H of plane k, then E.  SP: the
+    // plane or the tile carries a TF/SF plane or a DFT monitor; in interior
+    // tiles the other planes run a form without that code (same operations,
+    // same bits).
+    auto march_plane = [&](int k, int it, int s0, int s1, auto sp) {
+        constexpr bool SP = decltype(sp)::value;
         const R* E0x = sEq(s0, 0);
         const R* E0y = sEq(s0, 1);
         const R* E0z = sEq(s0, 2);
@@ -562,7 +582,8 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
                 hy = H0y[e];
                 hz = H0z[e];
                 h_cell<PML>(I, sx, false, hi, hj, k, E0x[e], E0y[e], E0z[e], E1x[e], E1y[e], E0z[e + 1], E0y[e + 1],
-                            E0z[e + SX], E0x[e + SX], hx, hy, hz, gE, haloSrcH || k == kSrcH, zpre, zHh0, zHh1);
+                            E0z[e + SX], E0x[e + SX], hx, hy, hz, gE, SP && (haloSrcH || k == kSrcH), zgiven,
+                            zring ? sZq(s0, 0)[e] : zHh0, zring ? sZq(s0, 1)[e] : zHh1);
             }
             sHn[e] = hx;
             sHn[EBr + e] = hy;
@@ -580,7 +601,8 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
                 hyk = H0y[e];
                 hzk = H0z[e];
                 h_cell<PML>(I, sx, true, i, j, k, exo, eyo, ezo, E1x[e], E1y[e], E0z[e + 1], E0y[e + 1], E0z[e + SX],
-                            E0x[e + SX], hxk, hyk, hzk, gE, ownSrcH || k == kSrcH, zpre, zHo0, zHo1);
+                            E0x[e + SX], hxk, hyk, hzk, gE, SP && (ownSrcH || k == kSrcH), zgiven,
+                            zring ? sZq(s0, 0)[e] : zHo0, zring ? sZq(s0, 1)[e] : zHo1);
                 const size_t o = (size_t)k * plane + (size_t)j * pitch + i;
                 Hout[0][o] = hxk;
                 Hout[1][o] = hyk;
@@ -602,12 +624,13 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
             // Ey += cy ((Hx - Hx(k-1)) - (Hz - Hz(i-1)))
             // Ez += cz ((Hy - Hy(i-1)) - (Hx - Hx(j-1)))
             R dd[6] = {hzk - hz_j, hyk - hym, hxk - hxm, hzk - hz_i, hyk - hy_i, hxk - hx_j};
-            if (PML) cpml6(sx, 0, true, i, j, k, dd, zpre, zEo0, zEo1);
+            if (PML)
+                cpml6(sx, 0, true, i, j, k, dd, zgiven, zring ? sZq(s0, 2)[e] : zEo0, zring ? sZq(s0, 3)[e] : zEo1);
             R ex = exo + coef<R, IT>(slut, I->lutc, v0) * (dd[0] - dd[1]);
             R ey = eyo + coef<R, IT>(slut, I->lutc, v1) * (dd[2] - dd[3]);
             R ez = ezo + coef<R, IT>(slut, I->lutc, v2) * (dd[4] - dd[5]);
             // TF/SF: the source plane is total field
-            if (ownSrcE || k == kSrcE) {
+            if (SP && (ownSrcE || k == kSrcE)) {
                 const int sb = (sa + 1) % 3, sc = (sa + 2) % 3;
                 const size_t pq = (size_t)sel3(sb, i, j, k) + (size_t)I->na * sel3(sc, i, j, k);
                 const R ua = __ldg(I->sEa + pq) * gH, ub = __ldg(I->sEb + pq) * gH;
@@ -620,8 +643,8 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
             Eout[1][o] = ey;
             Eout[2][o] = ez;
             // DFT samples: E on the plane, H averaged over the planes m-1, m of its normal
-            unsigned hit = mcol;
-            if ((zpl >> it) & 1ull) {
+            unsigned hit = SP ? mcol : 0u;
+            if (SP && ((zpl >> it) & 1ull)) {
                 for (unsigned b = mz; b; b &= b - 1) {
                     const int m = __ffs(b) - 1;
                     if (k == I->mon_index[m]) hit |= 1u << m;
@@ -664,6 +687,27 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
         }
         // the next iteration's first barrier separates these reads of the
         // new-H plane and slot s0 from their reuse
+    };
+    // the tile has x / y normal source or monitor columns (every plane is special)
+    const bool colSpecial = __syncthreads_or(ownSrcH || ownSrcE || haloSrcH || mcol != 0u) != 0;
+    if (zpre) load_zH(k0);
+    for (int k = k0; k < k1; ++k) {
+        const int it = k - k0;
+        const int s0 = it % ns, s1 = (it + 1) % ns, sn = (it + ns - 1) % ns;
+        if (it == 0) wait_plane(k, s0);
+        wait_plane(k + 1, s1);   // planes k and k+1 have landed (later ones may be in flight)
+        __syncthreads();         // ... for every thread; everyone is done with plane k-1
+        if (s_abort) break;      // a wait ran out: the whole CTA leaves the march here
+        if (k + ns - 1 <= k1) load_plane(k + ns - 1, sn);   // into the slot of plane k-1
+        cp_commit();
+        if (zpre) load_zE(k);
+        if constexpr (PML) {   // one form: the CPML loop is large enough without a second copy
+            march_plane(k, it, s0, s1, std::true_type{});
+        } else {
+            const bool special = colSpecial || k == kSrcH || k == kSrcE || ((zpl >> it) & 1ull) != 0;
+            if (special) march_plane(k, it, s0, s1, std::true_type{});
+            else march_plane(k, it, s0, s1, std::false_type{});
+        }
     }
     asm volatile("cp.async.wait_all;\n" ::: "memory");   // no cp.async copy outlives the CTA
     // Every TMA plane armed, k0 .. k1, was waited for inside the march unless
@@ -689,7 +733,7 @@ k_step3d(const Inst3D<R>* __restrict__ insts, const Tile3D* __restrict__ tiles, 
 template <class R, class IT, bool PML>
 cudaError_t launch_one(const void* insts, const Tile3D* tiles, int ntiles, int par, int off, int we, WaitCtl wc,
                        cudaStream_t s) {
-    constexpr size_t smem = smem_bytes<R, IT>();
+    constexpr size_t smem = smem_bytes<R, IT, kZRing<R, PML>>();
     static int done[64] = {0};
     int dev = 0;
     cudaGetDevice(&dev);
