@@ -15,11 +15,13 @@
 // backward sweep of matrix-vector products with them (m^2 per line), for A
 // and, with the same inverses, for A.' (the adjoint, fdfd2D.m:13-15).
 //
-// The block inversions run on one thread-block cluster of 8 or 16 CTAs: CTA c
-// holds rows [c R, c R + R) of the block in registers (thread j: column j),
-// and each pivot step exchanges the CTAs' pivot candidates, the pivot row and
-// the row it replaces through distributed shared memory, with one cluster
-// barrier per pivot.  The next block's Schur complement is formed from the
+// The block inversions run on one thread-block cluster of 8 CTAs (16, a
+// non-portable cluster size, for blocks above 128 points): CTA c
+// holds rows [c R, c R + R) of the block in registers (thread j: column j).
+// At each pivot step every CTA stores its pivot candidate and candidate row
+// (and the owner of row k that row) into the shared memory of every CTA of
+// the cluster; after one cluster barrier each CTA picks the pivot and
+// eliminates from local copies, with no remote read on the critical path.  The next block's Schur complement is formed from the
 // inverse while it is still in registers.  Cluster barriers are hardware
 // barriers: no CTA spins on memory.
 #include <cooperative_groups.h>
@@ -47,6 +49,16 @@ struct FdfdDev {
     int* fault;                // a zero pivot (singular block)
 };
 
+struct FdCand {   // a CTA's pivot candidate: |value|^2 and row (m: none)
+    double v;
+    int i, pad;
+};
+
+// dynamic shared memory of the factor kernel for block size m on C CTAs
+inline size_t fd_factor_smem(int m, int C) {
+    return (size_t)2 * C * m * sizeof(double2) + (size_t)2 * m * sizeof(double2) + (size_t)2 * C * sizeof(FdCand);
+}
+
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
     return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
@@ -69,14 +81,15 @@ __global__ void __launch_bounds__(NT, 1) k_fdfd_factor(FdfdDev P) {
     const int j = threadIdx.x;
     const bool col = j < m;
 
-    // per pivot parity: this CTA's candidate pivot row, its row k, and the
-    // candidate's |value|^2 and row index (read by the other CTAs)
-    __shared__ double2 s_cand[2][kFdMaxM];
-    __shared__ double2 s_rowk[2][kFdMaxM];
-    __shared__ double s_cval[2];
-    __shared__ int s_cidx[2];
-    __shared__ double2 s_f[RM];     // column k of the owned rows (after the exchange)
-    __shared__ double2 s_ip;        // 1 / pivot
+    // Exchange buffers, per pivot parity, written by the other CTAs of the
+    // cluster (remote stores before the pivot's cluster barrier) and read
+    // locally after it: every CTA's candidate pivot row and its |value|^2 and
+    // row index, and row k.
+    extern __shared__ double2 s_dyn[];
+    double2* s_cand = s_dyn;                   // [2][C][m]
+    double2* s_rowk = s_cand + 2 * C * m;      // [2][m]
+    FdCand* s_cv = reinterpret_cast<FdCand*>(s_rowk + 2 * m);   // [2][C]
+    __shared__ double2 s_colk[2][RM];   // column k of the owned rows, before the exchange
     __shared__ int s_best;
     __shared__ int s_piv[kFdMaxM];
     __shared__ int s_perm[kFdMaxM];
@@ -115,7 +128,8 @@ __global__ void __launch_bounds__(NT, 1) k_fdfd_factor(FdfdDev P) {
                 int bi = m;
 #pragma unroll
                 for (int q = 0; q < RM; ++q) {
-                    if (q >= nr) break;
+                    s_colk[par][q] = a[q];
+                    if (q >= nr) continue;
                     const int r = r0 + q;
                     const double v = cabs2(a[q]);
                     if (r >= k && v > best) {
@@ -123,61 +137,52 @@ __global__ void __launch_bounds__(NT, 1) k_fdfd_factor(FdfdDev P) {
                         bi = r;
                     }
                 }
-                s_cval[par] = best;
-                s_cidx[par] = bi;
                 s_best = bi;
+                const FdCand cd{best, bi, 0};
+                for (int c2 = 0; c2 < C; ++c2) *cl.map_shared_rank(&s_cv[par * C + c], c2) = cd;
             }
             __syncthreads();
             const int bl = s_best;
-            if (col) {
+            if (col) {   // push the candidate row, and row k, into every CTA of the cluster
+                double2 vb = make_double2(0.0, 0.0), vk = make_double2(0.0, 0.0);
 #pragma unroll
                 for (int q = 0; q < RM; ++q) {
-                    if (q >= nr) break;
-                    const int r = r0 + q;
-                    if (r == bl) s_cand[par][j] = a[q];
-                    if (r == k) s_rowk[par][j] = a[q];
+                    if (r0 + q == bl) vb = a[q];
+                    if (r0 + q == k) vk = a[q];
+                }
+                const bool ownk = k >= r0 && k < r0 + nr;
+                for (int c2 = 0; c2 < C; ++c2) {
+                    if (bl < m) cl.map_shared_rank(s_cand, c2)[(size_t)(par * C + c) * m + j] = vb;
+                    if (ownk) cl.map_shared_rank(s_rowk, c2)[(size_t)par * m + j] = vk;
                 }
             }
-            cl.sync();   // candidates and rows of every CTA are published
+            cl.sync();   // every CTA's candidate, candidate row and row k are here
             // the pivot row: the largest candidate, the lowest row on a tie
             // (every thread decides the same)
             double best = -1.0;
             int p = m, oc = 0;
             for (int c2 = 0; c2 < C; ++c2) {
-                const double v = *cl.map_shared_rank(&s_cval[par], c2);
-                const int i = *cl.map_shared_rank(&s_cidx[par], c2);
-                if (i < m && (v > best || (v == best && i < p))) {
-                    best = v;
-                    p = i;
+                const FdCand cd = s_cv[par * C + c2];
+                if (cd.i < m && (cd.v > best || (cd.v == best && cd.i < p))) {
+                    best = cd.v;
+                    p = cd.i;
                     oc = c2;
                 }
             }
-            double2 prow = make_double2(0.0, 0.0);
-            if (col) {
-                prow = cl.map_shared_rank(&s_cand[par][0], oc)[j];
-                if (p != k && p >= r0 && p < r0 + nr) {   // row p takes the old row k
-                    const double2 rk = cl.map_shared_rank(&s_rowk[par][0], k / R)[j];
-#pragma unroll
-                    for (int q = 0; q < RM; ++q)
-                        if (r0 + q == p) a[q] = rk;
-                }
+            const double2* prow_all = s_cand + (size_t)(par * C + oc) * m;
+            const double2* rowk = s_rowk + (size_t)par * m;
+            const double2 pk = prow_all[k];
+            const double dd = cabs2(pk);
+            const double2 ip = dd == 0.0 ? make_double2(0.0, 0.0) : make_double2(pk.x / dd, -pk.y / dd);
+            if (j == 0) {
+                s_piv[k] = p;
+                if (dd == 0.0) atomicExch(P.fault, 1);
             }
-            if (j == k) {
-#pragma unroll
-                for (int q = 0; q < RM; ++q) s_f[q] = a[q];
-                const double dd = cabs2(prow);
-                if (dd == 0.0) {
-                    atomicExch(P.fault, 1);
-                    s_ip = make_double2(0.0, 0.0);
-                } else {
-                    s_ip = make_double2(prow.x / dd, -prow.y / dd);
-                }
-            }
-            if (j == 0) s_piv[k] = p;
-            __syncthreads();
-            const double2 ip = s_ip;
-            const double2 pr = j == k ? ip : cmul(prow, ip);   // the scaled pivot row
             if (col) {
+                const double2 prow = prow_all[j];
+                const double2 pr = j == k ? ip : cmul(prow, ip);   // the scaled pivot row
+                const bool swap = p != k && p >= r0 && p < r0 + nr;   // row p takes the old row k
+                const double2 rkj = rowk[j], rkk = rowk[k];
 #pragma unroll
                 for (int q = 0; q < RM; ++q) {
                     if (q >= nr) break;
@@ -185,9 +190,11 @@ __global__ void __launch_bounds__(NT, 1) k_fdfd_factor(FdfdDev P) {
                     if (r == k) {
                         a[q] = pr;
                     } else {
-                        const double2 f = s_f[q];
+                        const bool sw = swap && r == p;
+                        const double2 f = sw ? rkk : s_colk[par][q];
+                        const double2 cur = sw ? rkj : a[q];
                         a[q] = j == k ? make_double2(-(f.x * ip.x - f.y * ip.y), -(f.x * ip.y + f.y * ip.x))
-                                      : csub(a[q], cmul(f, pr));
+                                      : csub(cur, cmul(f, pr));
                     }
                 }
             }
@@ -362,7 +369,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1) k_fdfd_solve(FdfdDev P, cons
 // cluster size and rows per CTA for block size m (threads: m rounded up to
 // a warp, at most C * RM)
 int fd_shape(int m, int* C, int* RM) {
-    static const int kC[3] = {8, 8, 16}, kR[3] = {16, 32, 24};
+    static const int kC[3] = {8, 16, 16}, kR[3] = {16, 16, 24};
     for (int q = 0; q < 3; ++q)
         if (kC[q] * kR[q] >= m) {
             *C = kC[q];
@@ -374,15 +381,19 @@ int fd_shape(int m, int* C, int* RM) {
 }
 
 template <class K, class... Args>
-cudaError_t launch_cluster(K kern, int C, int threads, cudaStream_t s, Args... args) {
+cudaError_t launch_cluster(K kern, int C, int threads, size_t smem, cudaStream_t s, Args... args) {
     if (C > 8) {
         const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        if (e != cudaSuccess) return e;
+    }
+    if (smem > 48 * 1024) {
+        const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)C, 1, 1);
     cfg.blockDim = dim3((unsigned)threads, 1, 1);
-    cfg.dynamicSmemBytes = 0;
+    cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeClusterDimension;
@@ -524,11 +535,10 @@ extern "C" int32_t orf_fdfd2d_factor(orf_ctx* ctx, const orf_fdfd2d* pr, orf_fdf
     const int threads = (m + 31) / 32 * 32;
     const FdfdDev P = F->dev();
     cudaError_t e;
-    switch (F->RM) {
-        case 16: e = launch_cluster(k_fdfd_factor<16, 128>, F->C, threads, st, P); break;
-        case 32: e = launch_cluster(k_fdfd_factor<32, 256>, F->C, threads, st, P); break;
-        default: e = launch_cluster(k_fdfd_factor<24, 384>, F->C, threads, st, P); break;
-    }
+    const size_t fsm = fd_factor_smem(m, F->C);
+    if (F->RM == 16 && threads <= 128) e = launch_cluster(k_fdfd_factor<16, 128>, F->C, threads, fsm, st, P);
+    else if (F->RM == 16) e = launch_cluster(k_fdfd_factor<16, 256>, F->C, threads, fsm, st, P);
+    else e = launch_cluster(k_fdfd_factor<24, 384>, F->C, threads, fsm, st, P);
     ORF_CUDA(e);
     int fault = 0;
     ORF_CUDA(cudaMemcpyAsync(&fault, F->fault, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -557,7 +567,7 @@ extern "C" int32_t orf_fdfd2d_solve(orf_fdfd* F, const double* rhs, double* x, i
     cudaStream_t st = F->ctx->stream;
     ORF_CUDA(cudaMemcpyAsync(F->vin, h.data(), N * sizeof(double2), cudaMemcpyHostToDevice, st));
     add_h2d(F->ctx, (int64_t)(N * sizeof(double2)));
-    ORF_CUDA(launch_cluster(k_fdfd_solve, F->C, kSolveThreads, st, F->dev(), (const double2*)F->vin, F->vout, F->Y,
+    ORF_CUDA(launch_cluster(k_fdfd_solve, F->C, kSolveThreads, 0, st, F->dev(), (const double2*)F->vin, F->vout, F->Y,
                             transpose ? 1 : 0));
     ORF_CUDA(cudaMemcpyAsync(h.data(), F->vout, N * sizeof(double2), cudaMemcpyDeviceToHost, st));
     ORF_CUDA(cudaStreamSynchronize(st));
