@@ -17,11 +17,14 @@
 //
 // The block inversions run on one thread-block cluster of 8 CTAs (16, a
 // non-portable cluster size, for blocks above 128 points): CTA c
-// holds rows [c R, c R + R) of the block in registers (thread j: column j).
-// At each pivot step every CTA stores its pivot candidate and candidate row
-// (and the owner of row k that row) into the shared memory of every CTA of
-// the cluster; after one cluster barrier each CTA picks the pivot and
-// eliminates from local copies, with no remote read on the critical path.  The next block's Schur complement is formed from the
+// holds rows [c R, c R + R) of the block in registers (one column per
+// thread, the rows split over up to four thread groups).
+// At each pivot step every CTA stores its pivot candidate into the shared
+// memory of every CTA of the cluster; after a cluster barrier all pick the
+// same pivot, its owner stores the pivot row into every CTA (and the owner
+// of row k that row into the pivot row's owner), and after a second barrier
+// each CTA eliminates from local copies: no remote read, one row broadcast
+// per pivot.  The next block's Schur complement is formed from the
 // inverse while it is still in registers.  Cluster barriers are hardware
 // barriers: no CTA spins on memory.
 #include <cooperative_groups.h>
@@ -36,6 +39,7 @@ namespace orf {
 namespace {
 
 constexpr int kFdMaxM = 384;      // largest block (the shorter grid axis)
+constexpr int kFdMaxC = 16;       // largest cluster
 constexpr int kSolveThreads = 256;
 
 struct FdfdDev {
@@ -54,11 +58,6 @@ struct FdCand {   // a CTA's pivot candidate: |value|^2 and row (m: none)
     int i, pad;
 };
 
-// dynamic shared memory of the factor kernel for block size m on C CTAs
-inline size_t fd_factor_smem(int m, int C) {
-    return (size_t)2 * C * m * sizeof(double2) + (size_t)2 * m * sizeof(double2) + (size_t)2 * C * sizeof(FdCand);
-}
-
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
     return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
@@ -68,36 +67,48 @@ __device__ __forceinline__ double cabs2(double2 a) { return a.x * a.x + a.y * a.
 
 // Block LU of the whole operator: block b inverted in place, stored to
 // P.inv[b], then turned into D_{b+1} = A - B D_b^{-1} C in registers.
-// Thread j holds column j of the CTA's RM (or fewer) rows; NT threads at most.
-template <int RM, int NT>
+// Thread (j, h) = (t % mp, t / mp) holds column j of the CTA's rows
+// h*RS .. h*RS + RS - 1 (TPC groups of RS rows; mp = m rounded up to a warp),
+// so that a pivot step's row work is spread over TPC times as many warps.
+template <int RS, int TPC, int NT>
 __global__ void __launch_bounds__(NT, 1) k_fdfd_factor(FdfdDev P) {
+    constexpr int RM = RS * TPC;   // rows per CTA at most
     cg::cluster_group cl = cg::this_cluster();
     const int C = (int)cl.num_blocks();
     const int c = (int)cl.block_rank();
     const int m = P.m;
+    const int mp = (m + 31) / 32 * 32;
     const int R = (m + C - 1) / C;
     const int r0 = c * R;
     const int nr = max(0, min(m, r0 + R) - r0);
-    const int j = threadIdx.x;
+    const int t = threadIdx.x;
+    const int j = t % mp, h = t / mp;
+    const int q0 = h * RS;            // first of this thread's rows, local to the CTA
+    const int r1 = r0 + q0;           // ... as a row of the block
+    const int nq = max(0, min(RS, nr - q0));   // this thread's rows
     const bool col = j < m;
 
     // Exchange buffers, per pivot parity, written by the other CTAs of the
-    // cluster (remote stores before the pivot's cluster barrier) and read
-    // locally after it: every CTA's candidate pivot row and its |value|^2 and
-    // row index, and row k.
-    extern __shared__ double2 s_dyn[];
-    double2* s_cand = s_dyn;                   // [2][C][m]
-    double2* s_rowk = s_cand + 2 * C * m;      // [2][m]
-    FdCand* s_cv = reinterpret_cast<FdCand*>(s_rowk + 2 * m);   // [2][C]
+    // cluster (remote stores before a cluster barrier) and read locally after
+    // it: every CTA's pivot candidate (|value|^2, row), the pivot row, and
+    // row k (sent to the pivot row's owner only).
+    __shared__ FdCand s_cv[2][kFdMaxC];
+    // s_prow[2] and s_rowk[2] in the pivot steps; the column exchange of a
+    // finished block (up to 4 row groups) reuses them: no CTA writes them
+    // again before the next block's first candidate barrier, which this CTA
+    // reaches only after its exchange
+    __shared__ double2 s_ex[4][kFdMaxM];
+    double2 (*s_prow)[kFdMaxM] = s_ex;
+    double2 (*s_rowk)[kFdMaxM] = s_ex + 2;
     __shared__ double2 s_colk[2][RM];   // column k of the owned rows, before the exchange
-    __shared__ int s_best;
+    __shared__ FdCand s_hc[2][TPC];     // the row groups' candidates
     __shared__ int s_piv[kFdMaxM];
     __shared__ int s_perm[kFdMaxM];
-    __shared__ double2 s_x[kFdMaxM];
+    static_assert(TPC <= 4, "the column exchange uses s_ex");
 
-    double2 a[RM];
+    double2 a[RS];
 #pragma unroll
-    for (int q = 0; q < RM; ++q) a[q] = make_double2(0.0, 0.0);
+    for (int u = 0; u < RS; ++u) a[u] = make_double2(0.0, 0.0);
     long long g = 0;   // pivot steps so far (buffer parity)
 
     for (int b = 0; b < P.nb; ++b) {
@@ -105,96 +116,125 @@ __global__ void __launch_bounds__(NT, 1) k_fdfd_factor(FdfdDev P) {
         if (col) {
             const double2 cpj = b > 0 ? P.bp[(size_t)(b - 1) * m + j] : make_double2(0.0, 0.0);
 #pragma unroll
-            for (int q = 0; q < RM; ++q) {
-                if (q >= nr) break;
-                const int p = r0 + q;
+            for (int u = 0; u < RS; ++u) {
+                if (u >= nq) break;
+                const int p = r1 + u;
                 const size_t o = (size_t)b * m + p;
                 double2 v = make_double2(0.0, 0.0);
                 if (b > 0) {
-                    const double2 s = cmul(cmul(P.bm[o], a[q]), cpj);
+                    const double2 s = cmul(cmul(P.bm[o], a[u]), cpj);
                     v = make_double2(-s.x, -s.y);
                 }
                 if (j == p) v = cadd(v, P.diag[o]);
                 else if (j == p - 1) v = cadd(v, P.wm[o]);
                 else if (j == p + 1) v = cadd(v, P.wp[o]);
-                a[q] = v;
+                a[u] = v;
             }
         }
         // ---- Gauss-Jordan inversion in place, partial pivoting
         for (int k = 0; k < m; ++k, ++g) {
             const int par = (int)(g & 1);
-            if (j == k) {   // this CTA's candidate: the largest |a| of column k on rows >= k
+            if (j == k) {   // the group's candidate: the largest |a| of column k on its rows >= k
                 double best = -1.0;
                 int bi = m;
 #pragma unroll
-                for (int q = 0; q < RM; ++q) {
-                    s_colk[par][q] = a[q];
-                    if (q >= nr) continue;
-                    const int r = r0 + q;
-                    const double v = cabs2(a[q]);
+                for (int u = 0; u < RS; ++u) {
+                    if (q0 + u < RM) s_colk[par][q0 + u] = a[u];
+                    if (u >= nq) continue;
+                    const int r = r1 + u;
+                    const double v = cabs2(a[u]);
                     if (r >= k && v > best) {
                         best = v;
                         bi = r;
                     }
                 }
-                s_best = bi;
-                const FdCand cd{best, bi, 0};
-                for (int c2 = 0; c2 < C; ++c2) *cl.map_shared_rank(&s_cv[par * C + c], c2) = cd;
+                s_hc[par][h] = FdCand{best, bi, 0};
             }
             __syncthreads();
-            const int bl = s_best;
-            if (col) {   // push the candidate row, and row k, into every CTA of the cluster
-                double2 vb = make_double2(0.0, 0.0), vk = make_double2(0.0, 0.0);
+            // the CTA's candidate (the same in every thread)
+            double cbest = -1.0;
+            int bl = m;
 #pragma unroll
-                for (int q = 0; q < RM; ++q) {
-                    if (r0 + q == bl) vb = a[q];
-                    if (r0 + q == k) vk = a[q];
-                }
-                const bool ownk = k >= r0 && k < r0 + nr;
-                for (int c2 = 0; c2 < C; ++c2) {
-                    if (bl < m) cl.map_shared_rank(s_cand, c2)[(size_t)(par * C + c) * m + j] = vb;
-                    if (ownk) cl.map_shared_rank(s_rowk, c2)[(size_t)par * m + j] = vk;
+            for (int hh = 0; hh < TPC; ++hh) {
+                const FdCand cd = s_hc[par][hh];
+                if (cd.i < m && (cd.v > cbest || (cd.v == cbest && cd.i < bl))) {
+                    cbest = cd.v;
+                    bl = cd.i;
                 }
             }
-            cl.sync();   // every CTA's candidate, candidate row and row k are here
-            // the pivot row: the largest candidate, the lowest row on a tie
-            // (every thread decides the same)
-            double best = -1.0;
-            int p = m, oc = 0;
-            for (int c2 = 0; c2 < C; ++c2) {
-                const FdCand cd = s_cv[par * C + c2];
-                if (cd.i < m && (cd.v > best || (cd.v == best && cd.i < p))) {
-                    best = cd.v;
-                    p = cd.i;
-                    oc = c2;
+            if (t == 0) {   // the CTA's candidate into every CTA
+                const FdCand cd{cbest, bl, 0};
+                for (int c2 = 0; c2 < C; ++c2) *cl.map_shared_rank(&s_cv[par][c], c2) = cd;
+            }
+            cl.sync();   // every CTA's candidate is here
+            // the pivot row: the largest candidate, the lowest row on a tie;
+            // lane c2 of every warp reads CTA c2's candidate and the warp
+            // reduces (every warp decides the same)
+            int p;
+            {
+                const int lane = t & 31;
+                double best = -1.0;
+                int bi = m;
+                if (lane < C) {
+                    const FdCand cd = s_cv[par][lane];
+                    if (cd.i < m) {
+                        best = cd.v;
+                        bi = cd.i;
+                    }
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+                    const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                    if (ob > best || (ob == best && oi < bi)) {
+                        best = ob;
+                        bi = oi;
+                    }
+                }
+                p = bi;
+            }
+            if (col) {   // the pivot row into every CTA, row k into the pivot row's owner
+                const bool hasp = p >= r1 && p < r1 + nq, hask = p != k && k >= r1 && k < r1 + nq;
+                if (hasp || hask) {
+                    double2 vp = make_double2(0.0, 0.0), vk = make_double2(0.0, 0.0);
+#pragma unroll
+                    for (int u = 0; u < RS; ++u) {
+                        if (r1 + u == p) vp = a[u];
+                        if (r1 + u == k) vk = a[u];
+                    }
+                    if (hasp)
+                        for (int c2 = 0; c2 < C; ++c2) cl.map_shared_rank(&s_prow[par][0], c2)[j] = vp;
+                    if (hask) cl.map_shared_rank(&s_rowk[par][0], p / R)[j] = vk;
                 }
             }
-            const double2* prow_all = s_cand + (size_t)(par * C + oc) * m;
-            const double2* rowk = s_rowk + (size_t)par * m;
+            cl.sync();   // the pivot row (and, at its owner, row k) is here
+            const double2* prow_all = &s_prow[par][0];
+            const double2* rowk = &s_rowk[par][0];
             const double2 pk = prow_all[k];
             const double dd = cabs2(pk);
-            const double2 ip = dd == 0.0 ? make_double2(0.0, 0.0) : make_double2(pk.x / dd, -pk.y / dd);
-            if (j == 0) {
+            const double inv_dd = dd == 0.0 ? 0.0 : 1.0 / dd;
+            const double2 ip = make_double2(pk.x * inv_dd, -pk.y * inv_dd);
+            if (t == 0) {
                 s_piv[k] = p;
                 if (dd == 0.0) atomicExch(P.fault, 1);
             }
-            if (col) {
+            if (col && nq > 0) {
                 const double2 prow = prow_all[j];
                 const double2 pr = j == k ? ip : cmul(prow, ip);   // the scaled pivot row
-                const bool swap = p != k && p >= r0 && p < r0 + nr;   // row p takes the old row k
+                const bool swap = p != k && p >= r1 && p < r1 + nq;   // row p takes the old row k
                 const double2 rkj = rowk[j], rkk = rowk[k];
 #pragma unroll
-                for (int q = 0; q < RM; ++q) {
-                    if (q >= nr) break;
-                    const int r = r0 + q;
+                for (int u = 0; u < RS; ++u) {
+                    if (u >= nq) break;
+                    const int r = r1 + u;
                     if (r == k) {
-                        a[q] = pr;
+                        a[u] = pr;
                     } else {
+                        // column k of the inverse: -f / pivot (pr = 1 / pivot there)
                         const bool sw = swap && r == p;
-                        const double2 f = sw ? rkk : s_colk[par][q];
-                        const double2 cur = sw ? rkj : a[q];
-                        a[q] = j == k ? make_double2(-(f.x * ip.x - f.y * ip.y), -(f.x * ip.y + f.y * ip.x))
-                                      : csub(cur, cmul(f, pr));
+                        const double2 f = sw ? rkk : s_colk[par][q0 + u];
+                        const double2 cur = j == k ? make_double2(0.0, 0.0) : (sw ? rkj : a[u]);
+                        a[u] = csub(cur, cmul(f, pr));
                     }
                 }
             }
@@ -202,33 +242,32 @@ __global__ void __launch_bounds__(NT, 1) k_fdfd_factor(FdfdDev P) {
         // ---- undo the row exchanges on the columns of the inverse, last first:
         // column j of D_b^{-1} is column perm[j] of what the threads hold
         __syncthreads();
-        if (j == 0) {
+        if (t == 0) {
             for (int q = 0; q < m; ++q) s_perm[q] = q;
             for (int k = m - 1; k >= 0; --k) {
                 const int pk = s_piv[k];
                 if (pk != k) {
-                    const int t = s_perm[k];
+                    const int tmp = s_perm[k];
                     s_perm[k] = s_perm[pk];
-                    s_perm[pk] = t;
+                    s_perm[pk] = tmp;
                 }
             }
         }
         __syncthreads();
         const int src = col ? s_perm[j] : 0;
 #pragma unroll
-        for (int q = 0; q < RM; ++q) {
-            if (q >= nr) break;
-            if (col) s_x[j] = a[q];
+        for (int u = 0; u < RS; ++u) {
+            if (col) s_ex[h][j] = a[u];
             __syncthreads();
-            if (col) a[q] = s_x[src];
+            if (col) a[u] = s_ex[h][src];
             __syncthreads();
         }
         if (col) {
             double2* out = P.inv + (size_t)b * m * m;
 #pragma unroll
-            for (int q = 0; q < RM; ++q) {
-                if (q >= nr) break;
-                out[(size_t)(r0 + q) * m + j] = a[q];
+            for (int u = 0; u < RS; ++u) {
+                if (u >= nq) break;
+                out[(size_t)(r1 + u) * m + j] = a[u];
             }
         }
     }
@@ -366,8 +405,10 @@ __global__ void __launch_bounds__(kSolveThreads, 1) k_fdfd_solve(FdfdDev P, cons
     cl.sync();   // no CTA leaves while another may still read its shared memory
 }
 
-// cluster size and rows per CTA for block size m (threads: m rounded up to
-// a warp, at most C * RM)
+// Factor kernel shape for block size m: CTAs of the cluster, rows per CTA
+// at most (RM), thread groups per column (TPC); threads TPC x m rounded up
+// to a warp.  m <= 128: 8 CTAs, 4 groups of 4 rows; m <= 256: 16 CTAs, 4
+// groups of 4 rows; m <= 384: 16 CTAs, one group of 24 rows.
 int fd_shape(int m, int* C, int* RM) {
     static const int kC[3] = {8, 16, 16}, kR[3] = {16, 16, 24};
     for (int q = 0; q < 3; ++q)
@@ -532,13 +573,13 @@ extern "C" int32_t orf_fdfd2d_factor(orf_ctx* ctx, const orf_fdfd2d* pr, orf_fdf
     ORF_CUDA(cudaMemcpyAsync(F->bp, hbp.data(), N * sizeof(double2), cudaMemcpyHostToDevice, st));
     ORF_CUDA(cudaMemsetAsync(F->fault, 0, sizeof(int), st));
     add_h2d(ctx, (int64_t)(5 * N * sizeof(double2)));
-    const int threads = (m + 31) / 32 * 32;
+    const int mp = (m + 31) / 32 * 32;
     const FdfdDev P = F->dev();
     cudaError_t e;
-    const size_t fsm = fd_factor_smem(m, F->C);
-    if (F->RM == 16 && threads <= 128) e = launch_cluster(k_fdfd_factor<16, 128>, F->C, threads, fsm, st, P);
-    else if (F->RM == 16) e = launch_cluster(k_fdfd_factor<16, 256>, F->C, threads, fsm, st, P);
-    else e = launch_cluster(k_fdfd_factor<24, 384>, F->C, threads, fsm, st, P);
+    const size_t fsm = 0;
+    if (F->RM == 16 && mp <= 128) e = launch_cluster(k_fdfd_factor<4, 4, 512>, F->C, 4 * mp, fsm, st, P);
+    else if (F->RM == 16) e = launch_cluster(k_fdfd_factor<4, 4, 1024>, F->C, 4 * mp, fsm, st, P);
+    else e = launch_cluster(k_fdfd_factor<24, 1, 384>, F->C, mp, fsm, st, P);
     ORF_CUDA(e);
     int fault = 0;
     ORF_CUDA(cudaMemcpyAsync(&fault, F->fault, sizeof(int), cudaMemcpyDeviceToHost, st));
