@@ -51,6 +51,8 @@ struct FdfdDev {
     const double2* bp;         // [nb][m]: to block b + 1
     double2* inv;              // [nb][m][m]: D_b^{-1}, row-major
     int* fault;                // a zero pivot (singular block)
+    double2* xpan;             // [m][kPanel]: the blocked factorisation's panel, every row
+    double2* xrow;             // [kPanel][m]: its pivot rows
 };
 
 struct FdCand {   // a CTA's pivot candidate: |value|^2 and row (m: none)
@@ -274,6 +276,264 @@ __global__ void __launch_bounds__(NT, 1) k_fdfd_factor(FdfdDev P) {
     cl.sync();   // no CTA leaves while another may still read its shared memory
 }
 
+// Blocked form of the same elimination for blocks of up to 256 points:
+// pivots chosen and applied kPanel columns at a time.  Every CTA reads the
+// panel columns of all rows (each CTA writes its rows' entries to a global
+// scratch panel, cluster barrier, every CTA reads it back from L2: the
+// fan-out goes through L2, not through one SM's port), runs the panel's
+// pivot steps on that copy with block barriers only (pivot rows by partial
+// pivoting among the rows not yet used, the lowest row on a tie: every CTA
+// decides the same), reads the panel's pivot rows the same way (second
+// cluster barrier), and applies the rank-kPanel update
+//   pivot rows:  A[K, N] <- P^-1 A[K, N],   others: A[r, N] -= A[r, K0] P^-1 A[K, N]
+// to its own rows (P: the panel block of the pivot rows, N: the columns
+// outside the panel); the panel columns take the replica's values.  Rows
+// are not exchanged: the inverse is the result with its rows taken in pivot
+// order and its columns in the inverse order, and is stored to P.inv row by
+// row in its true place, then read back for the next block.
+constexpr int kPanel = 8;
+constexpr int kPanelMaxM = 256;
+
+inline size_t fd_panel_smem(int m) {   // s_pan[m][W], s_pn[m][W], s_rk[W][m], s_u[W][m], s_rows[2][m][W]
+    return (size_t)6 * m * kPanel * sizeof(double2);
+}
+
+template <int RS, int TPC, int NT>
+__global__ void __launch_bounds__(NT, 1) k_fdfd_factor_panel(FdfdDev P) {
+    cg::cluster_group cl = cg::this_cluster();
+    const int C = (int)cl.num_blocks();
+    const int c = (int)cl.block_rank();
+    const int m = P.m;
+    const int mp = (m + 31) / 32 * 32;
+    const int R = (m + C - 1) / C;
+    const int r0 = c * R;
+    const int nr = max(0, min(m, r0 + R) - r0);
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int nt = (int)blockDim.x, nwarps = nt / 32;   // TPC x mp threads (at most NT)
+    const int j = t % mp, h = t / mp;
+    const int q0 = h * RS;
+    const int r1 = r0 + q0;
+    const int nq = max(0, min(RS, nr - q0));
+    const bool col = j < m;
+    constexpr int W = kPanel;
+
+    extern __shared__ double2 s_dyn[];
+    double2* s_pan = s_dyn;                          // [m][W]: the panel, every row (old values)
+    double2* s_pn = s_pan + (size_t)m * W;           // [m][W]: the panel after its pivot steps
+    double2* s_rk = s_pn + (size_t)m * W;            // [W][m]: the panel's pivot rows (old values)
+    double2* s_u = s_rk + (size_t)W * m;             // [W][m]: P^-1 times them
+    double2* s_rows = s_u + (size_t)W * m;           // [2][m][W]: the copy's rows, per pivot step
+    __shared__ FdCand s_wc[2][NT / 32];              // per warp candidates, per pivot step
+    __shared__ int s_K[W];                           // pivot rows of the panel
+    __shared__ signed char s_kidx[kPanelMaxM];       // index of a row in s_K, or -1
+    __shared__ int s_piv[kPanelMaxM];
+    __shared__ int s_ipiv[kPanelMaxM];
+
+    double2 a[RS];
+#pragma unroll
+    for (int u = 0; u < RS; ++u) a[u] = make_double2(0.0, 0.0);
+
+    for (int b = 0; b < P.nb; ++b) {
+        // ---- D_b: the tridiagonal block minus B_b D_{b-1}^{-1} C_{b-1}
+        if (col) {
+            const double2 cpj = b > 0 ? P.bp[(size_t)(b - 1) * m + j] : make_double2(0.0, 0.0);
+#pragma unroll
+            for (int u = 0; u < RS; ++u) {
+                if (u >= nq) break;
+                const int p = r1 + u;
+                const size_t o = (size_t)b * m + p;
+                double2 v = make_double2(0.0, 0.0);
+                if (b > 0) {
+                    const double2 s = cmul(cmul(P.bm[o], a[u]), cpj);
+                    v = make_double2(-s.x, -s.y);
+                }
+                if (j == p) v = cadd(v, P.diag[o]);
+                else if (j == p - 1) v = cadd(v, P.wm[o]);
+                else if (j == p + 1) v = cadd(v, P.wp[o]);
+                a[u] = v;
+            }
+        }
+        bool myused = false;   // row t (thread t < m) is the pivot row of an earlier column
+        for (int k0 = 0; k0 < m; k0 += W) {
+            const int we = min(W, m - k0);
+            double2* pan = s_pan;
+            // ---- the panel entries of the own rows to the scratch panel; every
+            // CTA reads the whole panel back (L2, bypassing L1: the scratch is
+            // rewritten every panel).  The scratch is written again only after
+            // the next cluster barrier, which every reader reaches after its read.
+            if (col && j >= k0 && j < k0 + we) {
+#pragma unroll
+                for (int u = 0; u < RS; ++u)
+                    if (u < nq) P.xpan[(size_t)(r1 + u) * W + (j - k0)] = a[u];
+            }
+            __threadfence();
+            cl.sync();   // the whole panel is in memory
+            // ---- the panel's pivot steps on the copy: thread r holds row r
+            double2 pr[W];
+            if (t < m) {
+#pragma unroll
+                for (int l = 0; l < W; ++l) {
+                    pr[l] = l < we ? __ldcg(P.xpan + (size_t)t * W + l) : make_double2(0.0, 0.0);
+                    pan[(size_t)t * W + l] = pr[l];
+                }
+            }
+            // one block barrier per pivot step: every row thread publishes its
+            // row and every warp its candidate (buffers alternate by step), then
+            // every warp reduces the candidates itself and reads the pivot row
+            for (int aa = 0; aa < we; ++aa) {
+                const int sp2 = aa & 1;
+                double2* rows = s_rows + (size_t)sp2 * m * W;
+                double best = -1.0;
+                int bi = m;
+                if (t < m) {
+                    double2 v = pr[0];
+#pragma unroll
+                    for (int l = 0; l < W; ++l) {
+                        rows[(size_t)t * W + l] = pr[l];
+                        if (l == aa) v = pr[l];
+                    }
+                    if (!myused) {
+                        best = cabs2(v);
+                        bi = t;
+                    }
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+                    const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                    if (ob > best || (ob == best && oi < bi)) {
+                        best = ob;
+                        bi = oi;
+                    }
+                }
+                if (lane == 0) s_wc[sp2][warp] = FdCand{best, bi, 0};
+                __syncthreads();
+                best = -1.0;
+                bi = m;
+                if (lane < nwarps) {
+                    const FdCand cd = s_wc[sp2][lane];
+                    best = cd.v;
+                    bi = cd.i;
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+                    const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                    if (ob > best || (ob == best && oi < bi)) {
+                        best = ob;
+                        bi = oi;
+                    }
+                }
+                const bool bad = bi >= m || best == 0.0;
+                const int p = bi >= m ? 0 : bi;
+                if (t == 0) {
+                    if (bad) atomicExch(P.fault, 1);
+                    s_piv[k0 + aa] = p;
+                    s_K[aa] = p;
+                }
+                if (t == p) myused = true;
+                const double2* prw = rows + (size_t)p * W;
+                const double2 pk = prw[aa];
+                const double dd = cabs2(pk);
+                const double inv_dd = dd == 0.0 ? 0.0 : 1.0 / dd;
+                const double2 ip = make_double2(pk.x * inv_dd, -pk.y * inv_dd);
+                if (t < m) {
+                    double2 f = pr[0];
+#pragma unroll
+                    for (int l = 1; l < W; ++l)
+                        if (l == aa) f = pr[l];
+#pragma unroll
+                    for (int l = 0; l < W; ++l) {
+                        const double2 sp = l == aa ? ip : cmul(prw[l], ip);   // the scaled pivot row
+                        if (t == p) pr[l] = sp;
+                        else pr[l] = csub(l == aa ? make_double2(0.0, 0.0) : pr[l], cmul(f, sp));
+                    }
+                }
+            }
+            __syncthreads();   // s_K, s_piv
+            if (t < m) {
+#pragma unroll
+                for (int l = 0; l < W; ++l) s_pn[(size_t)t * W + l] = pr[l];
+                s_kidx[t] = -1;
+            }
+            __syncthreads();
+            if (t < we) s_kidx[s_K[t]] = (signed char)t;
+            // ---- the panel's pivot rows (old values, every column) through the
+            // scratch rows, read back by every CTA
+            if (col) {
+#pragma unroll
+                for (int u = 0; u < RS; ++u) {
+                    if (u >= nq) break;
+                    const int r = r1 + u;
+                    for (int i = 0; i < we; ++i)
+                        if (s_K[i] == r) P.xrow[(size_t)i * m + j] = a[u];
+                }
+            }
+            __threadfence();
+            cl.sync();   // the pivot rows are in memory
+            for (int e = t; e < we * m; e += nt) s_rk[e] = __ldcg(P.xrow + e);
+            __syncthreads();
+            // ---- U = P^-1 (pivot rows): row i of U by the threads of group i % TPC
+            if (col) {
+                for (int i = h; i < we; i += TPC) {
+                    double2 acc = make_double2(0.0, 0.0);
+                    const double2* pinv = s_pn + (size_t)s_K[i] * W;
+                    for (int l = 0; l < we; ++l) acc = cadd(acc, cmul(pinv[l], s_rk[(size_t)l * m + j]));
+                    s_u[(size_t)i * m + j] = acc;
+                }
+            }
+            __syncthreads();
+            // ---- the rank-we update of the own rows
+            if (col) {
+                const bool inpan = j >= k0 && j < k0 + we;
+#pragma unroll
+                for (int u = 0; u < RS; ++u) {
+                    if (u >= nq) break;
+                    const int r = r1 + u;
+                    if (inpan) {
+                        a[u] = s_pn[(size_t)r * W + (j - k0)];
+                    } else if (s_kidx[r] >= 0) {
+                        a[u] = s_u[(size_t)s_kidx[r] * m + j];
+                    } else {
+                        double2 v = a[u];
+                        for (int l = 0; l < we; ++l) v = csub(v, cmul(pan[(size_t)r * W + l], s_u[(size_t)l * m + j]));
+                        a[u] = v;
+                    }
+                }
+            }
+            __syncthreads();   // s_kidx, s_u and s_pn are rewritten by the next panel
+        }
+        // ---- the inverse: row ipiv[r] is row r of what the threads hold,
+        // with column j taken from column ipiv[j]
+        if (t < m) s_ipiv[s_piv[t]] = t;
+        __syncthreads();
+        double2* s_ex = s_u;   // [TPC][m] (TPC <= kPanel)
+        const int src = col ? s_ipiv[j] : 0;
+#pragma unroll
+        for (int u = 0; u < RS; ++u) {
+            if (col) s_ex[(size_t)h * m + j] = a[u];
+            __syncthreads();
+            if (col) a[u] = s_ex[(size_t)h * m + src];
+            __syncthreads();
+        }
+        double2* out = P.inv + (size_t)b * m * m;
+        if (col) {
+#pragma unroll
+            for (int u = 0; u < RS; ++u)
+                if (u < nq) out[(size_t)s_ipiv[r1 + u] * m + j] = a[u];
+        }
+        __threadfence();
+        cl.sync();   // every CTA's rows of the inverse are in memory
+        if (col) {
+#pragma unroll
+            for (int u = 0; u < RS; ++u)
+                if (u < nq) a[u] = out[(size_t)(r1 + u) * m + j];
+        }
+        __syncthreads();
+    }
+    cl.sync();   // no CTA leaves while another may still read its shared memory
+}
+
 // Forward and backward sweeps with the stored inverses.
 //   mode 0: A x = -rhs:   w_b = -rhs_b - B_b y_{b-1},  y_b = D_b^{-1} w_b,
 //                         x_b = y_b - D_b^{-1} C_b x_{b+1}
@@ -481,7 +741,7 @@ struct orf_fdfd {
     bool along_x = true;   // blocks are lines of constant x (m = nz)
     Arena ar;
     double2 *diag = nullptr, *wm = nullptr, *wp = nullptr, *bm = nullptr, *bp = nullptr;
-    double2 *inv = nullptr, *Y = nullptr, *vin = nullptr, *vout = nullptr;
+    double2 *inv = nullptr, *Y = nullptr, *vin = nullptr, *vout = nullptr, *xpan = nullptr, *xrow = nullptr;
     int* fault = nullptr;
     ~orf_fdfd() {
         if (ar.base) {
@@ -490,7 +750,7 @@ struct orf_fdfd {
         }
         if (ctx) ctx_release(ctx);
     }
-    FdfdDev dev() const { return FdfdDev{m, nb, diag, wm, wp, bm, bp, inv, fault}; }
+    FdfdDev dev() const { return FdfdDev{m, nb, diag, wm, wp, bm, bp, inv, fault, xpan, xrow}; }
     // (i, k) of the grid <-> entry b * m + p of the block layout
     size_t at(int i, int k) const { return along_x ? (size_t)i * m + k : (size_t)k * m + i; }
 };
@@ -564,6 +824,8 @@ extern "C" int32_t orf_fdfd2d_factor(orf_ctx* ctx, const orf_fdfd2d* pr, orf_fdf
     ar.add(&F->vin, N);
     ar.add(&F->vout, N);
     ar.add(&F->fault, 1);
+    ar.add(&F->xpan, (size_t)m * 8);
+    ar.add(&F->xrow, (size_t)8 * m);
     ORF_TRY(ar.alloc());
     cudaStream_t st = ctx->stream;
     ORF_CUDA(cudaMemcpyAsync(F->diag, hd.data(), N * sizeof(double2), cudaMemcpyHostToDevice, st));
@@ -577,8 +839,9 @@ extern "C" int32_t orf_fdfd2d_factor(orf_ctx* ctx, const orf_fdfd2d* pr, orf_fdf
     const FdfdDev P = F->dev();
     cudaError_t e;
     const size_t fsm = 0;
-    if (F->RM == 16 && mp <= 128) e = launch_cluster(k_fdfd_factor<4, 4, 512>, F->C, 4 * mp, fsm, st, P);
-    else if (F->RM == 16) e = launch_cluster(k_fdfd_factor<4, 4, 1024>, F->C, 4 * mp, fsm, st, P);
+    const size_t psm = fd_panel_smem(m);
+    if (F->RM == 16 && mp <= 128) e = launch_cluster(k_fdfd_factor_panel<4, 4, 512>, F->C, 4 * mp, psm, st, P);
+    else if (F->RM == 16) e = launch_cluster(k_fdfd_factor_panel<8, 2, 512>, F->C, 2 * mp, psm, st, P);
     else e = launch_cluster(k_fdfd_factor<24, 1, 384>, F->C, mp, fsm, st, P);
     ORF_CUDA(e);
     int fault = 0;
