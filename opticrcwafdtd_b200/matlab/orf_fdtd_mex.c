@@ -10,6 +10,16 @@
  *   c   = orf_fdtd_mex('marshal3d', sim)  the orf_sim3d likewise (for checking defaults)
  *   v   = orf_fdtd_mex('version')         orf_abi_version()
  *
+ *   id  = orf_fdtd_mex('fdfd2D_factor', x, z, epsr, lambda0, Npml, PmlReflection)
+ *   E   = orf_fdtd_mex('fdfd2D_solve', id, rhs, transpose)
+ *         orf_fdtd_mex('fdfd2D_release', id)
+ *         the frequency-domain solver of orf.fdfd2D (toolbox/+orf/fdfd2D.m:1-19):
+ *         the factors stay on the device under a small integer id (at most
+ *         64 at once) until released; transpose 0 returns E with A E = -rhs,
+ *         1 returns lam with A.' lam = rhs.  epsr and rhs are nx x nz,
+ *         real or complex; E is complex nx x nz.  +orf/fdfd2D.m builds the
+ *         reference's result struct on these (out.solve, out.adjoint, fluxes).
+ *
  * Inputs: every sim field of fdtd2D.m:9-23 / fdtd2DTE.m:7-25 / fdtd3D.m:11-24
  * with the reference's defaults (pol "TE", periodicZ false, npml 0,
  * source.neff 1, source.bw 0.2, maxTime 1e4, shutoff 1e-10, courant
@@ -527,6 +537,122 @@ static void show3d(mxArray* plhs[], const mxArray* s) {
     plhs[0] = o;
 }
 
+/* -------------------------------------------------------------- FDFD ----- */
+#define MAXFDFD 64
+static orf_fdfd* g_fdfd[MAXFDFD];   /* factored operators by id - 1 */
+static int32_t g_fdfd_n[MAXFDFD][2];
+
+/* uniform increasing vector of at least three points */
+static void vgrid(const mxArray* a, const char* name, int32_t* n, double* d) {
+    if (!mxIsDouble(a) || mxIsComplex(a) || mxGetNumberOfElements(a) < 3)
+        bad("%s must be a real vector of at least three points", name);
+    const double* v = mxGetDoubles(a);
+    const size_t m = mxGetNumberOfElements(a);
+    const double h = v[1] - v[0];
+    double dev = 0.0;
+    for (size_t i = 1; i < m; ++i) dev = fmax(dev, fabs((v[i] - v[i - 1]) - h));
+    if (!(h > 0) || dev > 1e-9 * fmax(1.0, fabs(h)) * (double)m) bad("%s must be uniform and increasing", name);
+    *n = (int32_t)m;
+    *d = h;
+}
+
+/* an nx x nz double array as interleaved complex: the array's own storage
+ * when complex, else a complex copy in *tmp (destroyed by the caller) */
+static const double* cplx_arg(const mxArray* a, size_t n, const char* what, mxArray** tmp) {
+    *tmp = NULL;
+    if (!mxIsDouble(a) || mxGetNumberOfElements(a) != n) bad("%s must be a double array of nx x nz elements", what);
+    if (mxIsComplex(a)) return (const double*)mxGetComplexDoubles(a);
+    *tmp = mxCreateDoubleMatrix((mwSize)n, 1, mxCOMPLEX);
+    mxComplexDouble* c = mxGetComplexDoubles(*tmp);
+    const double* r = mxGetDoubles(a);
+    for (size_t q = 0; q < n; ++q) {
+        c[q].real = r[q];
+        c[q].imag = 0.0;
+    }
+    return (const double*)c;
+}
+
+static double real_scalar(const mxArray* a, const char* what) {
+    if (!mxIsDouble(a) || mxIsComplex(a) || mxGetNumberOfElements(a) != 1) bad("%s must be a real scalar", what);
+    return mxGetScalar(a);
+}
+
+static int fdfd_id(const mxArray* a) {
+    const double v = real_scalar(a, "the fdfd2D id");
+    const int id = (int)v;
+    if ((double)id != v || id < 1 || id > MAXFDFD || !g_fdfd[id - 1]) bad("no factored operator has this id%s", "");
+    return id - 1;
+}
+
+static void fdfd_factor(mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
+    if (nrhs != 7)
+        mexErrMsgIdAndTxt("orf:invalidInput",
+                          "usage: id = orf_fdtd_mex('fdfd2D_factor', x, z, epsr, lambda0, Npml, PmlReflection)");
+    int32_t nx, nz;
+    double dx, dz;
+    vgrid(prhs[1], "x", &nx, &dx);
+    vgrid(prhs[2], "z", &nz, &dz);
+    if (fabs(dx - dz) > 1e-9 * dx) bad("x and z must have the same spacing%s", "");
+    const double lambda0 = real_scalar(prhs[4], "lambda0");
+    const mxArray* np = prhs[5];
+    const size_t nn = mxGetNumberOfElements(np);
+    if (!mxIsDouble(np) || mxIsComplex(np) || (nn != 1 && nn != 2)) bad("Npml must be one or two cell counts%s", "");
+    const double* npv = mxGetDoubles(np);
+    const double R = real_scalar(prhs[6], "PmlReflection");
+    int slot = -1;
+    for (int q = 0; q < MAXFDFD && slot < 0; ++q)
+        if (!g_fdfd[q]) slot = q;
+    if (slot < 0) bad("%s", "64 factored operators are held already: release some");
+    mxArray* tmp = NULL;
+    const double* eps = cplx_arg(prhs[3], (size_t)nx * nz, "epsr", &tmp);
+    orf_fdfd2d pr;
+    pr.nx = nx;
+    pr.nz = nz;
+    pr.dx = dx;
+    pr.eps = eps;
+    pr.lambda0 = lambda0;
+    pr.npml_x = (int32_t)npv[0];
+    pr.npml_z = (int32_t)npv[nn - 1];
+    pr.pml_reflection = R;
+    orf_ctx* ctx = NULL;
+    int32_t st = orf_ctx_create(0, NULL, &ctx);
+    orf_fdfd* f = NULL;
+    if (st == ORF_OK) {
+        st = orf_fdfd2d_factor(ctx, &pr, &f);
+        orf_ctx_destroy(ctx);   /* the factors keep their context alive */
+    }
+    if (tmp) mxDestroyArray(tmp);
+    if (st != ORF_OK) fail(st);
+    g_fdfd[slot] = f;
+    g_fdfd_n[slot][0] = nx;
+    g_fdfd_n[slot][1] = nz;
+    plhs[0] = mxCreateDoubleScalar((double)(slot + 1));
+}
+
+static void fdfd_solve(mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
+    if (nrhs != 4) mexErrMsgIdAndTxt("orf:invalidInput", "usage: E = orf_fdtd_mex('fdfd2D_solve', id, rhs, transpose)");
+    const int q = fdfd_id(prhs[1]);
+    const int32_t nx = g_fdfd_n[q][0], nz = g_fdfd_n[q][1];
+    const double tr = real_scalar(prhs[3], "transpose");
+    mxArray* tmp = NULL;
+    const double* rhs = cplx_arg(prhs[2], (size_t)nx * nz, "the right-hand side", &tmp);
+    mxArray* out = mxCreateDoubleMatrix((mwSize)nx, (mwSize)nz, mxCOMPLEX);
+    const int32_t st = orf_fdfd2d_solve(g_fdfd[q], rhs, (double*)mxGetComplexDoubles(out), tr != 0.0);
+    if (tmp) mxDestroyArray(tmp);
+    if (st != ORF_OK) {
+        mxDestroyArray(out);
+        fail(st);
+    }
+    plhs[0] = out;
+}
+
+static void fdfd_release(int nrhs, const mxArray* prhs[]) {
+    if (nrhs != 2) mexErrMsgIdAndTxt("orf:invalidInput", "usage: orf_fdtd_mex('fdfd2D_release', id)");
+    const int q = fdfd_id(prhs[1]);
+    orf_fdfd2d_release(g_fdfd[q]);
+    g_fdfd[q] = NULL;
+}
+
 /* ------------------------------------------------------------- entry ----- */
 void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
     char cmd[32];
@@ -534,6 +660,18 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
         mexErrMsgIdAndTxt("orf:invalidInput", "usage: out = orf_fdtd_mex(command, sim)");
     if (!strcmp(cmd, "version")) {
         plhs[0] = mxCreateDoubleScalar((double)orf_abi_version());
+        return;
+    }
+    if (!strcmp(cmd, "fdfd2D_factor")) {
+        fdfd_factor(plhs, nrhs, prhs);
+        return;
+    }
+    if (!strcmp(cmd, "fdfd2D_solve")) {
+        fdfd_solve(plhs, nrhs, prhs);
+        return;
+    }
+    if (!strcmp(cmd, "fdfd2D_release")) {
+        fdfd_release(nrhs, prhs);
         return;
     }
     if (nrhs != 2 || !mxIsStruct(prhs[1]) || mxGetNumberOfElements(prhs[1]) != 1)

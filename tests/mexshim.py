@@ -117,6 +117,16 @@ class Gateway:
         a = a.reshape(dims, order="F")
         return a.item() if a.size == 1 and dims == (1, 1) else a
 
+    def call_args(self, cmd: str, *args):
+        """out = orf_fdtd_mex(cmd, args...); raises MexError; returns the
+        output (None when the command returns nothing)."""
+        mx = [self.to_mx(cmd)] + [self.to_mx(a) for a in args]
+        prhs = (C.c_void_p * len(mx))(*mx)
+        plhs = (C.c_void_p * 1)()
+        if self.L.shim_call(1, plhs, len(mx), prhs):
+            raise MexError(self.L.shim_error_id().decode(), self.L.shim_error_msg().decode())
+        return self.from_mx(plhs[0]) if plhs[0] else None
+
     def call(self, cmd: str, sim=None):
         """out = orf_fdtd_mex(cmd, sim); raises MexError with MATLAB's
         identifier; returns (out, warning identifier or None)."""

@@ -243,3 +243,60 @@ def test_gateway_run3d_equals_python_binding(gw):
         for k in ("Ea", "Eb", "Ha", "Hb"):
             assert np.array_equal(np.reshape(mo[k], mr[k].shape), mr[k]), k
     assert out["steps"] == ref["steps"]
+
+
+# ------------------------------------------------- the FDFD commands ------
+def _fdfd_args(nx=40, nz=30, seed=3):
+    from tests import fdfd_cases
+    x, z, eps, lam, J, g, npml = fdfd_cases.random_problem(nx, nz, seed)
+    return x, z, eps, lam, J, g, npml
+
+
+@pytest.mark.parametrize("edit,frag", [
+    (lambda a: a.__setitem__(0, np.array([0.0, 0.1, 0.3, 0.4])), "uniform"),
+    (lambda a: a.__setitem__(1, a[1] * 2.0), "same spacing"),
+    (lambda a: a.__setitem__(2, a[2][:, :-1]), "nx x nz"),
+    (lambda a: a.__setitem__(4, np.array([1.0, 2.0, 3.0])), "Npml"),
+])
+def test_fdfd_factor_rejects_malformed_input(gw, edit, frag):
+    x, z, eps, lam, J, g, npml = _fdfd_args()
+    a = [x, z, eps, lam, np.asarray(npml, dtype=float), 1e-8]
+    edit(a)
+    with pytest.raises(mexshim.MexError) as ei:
+        gw.call_args("fdfd2D_factor", *a)
+    assert ei.value.identifier == "orf:invalidInput" and frag in ei.value.message
+
+
+def test_fdfd_commands_reject_usage_and_unknown_ids(gw):
+    with pytest.raises(mexshim.MexError) as ei:
+        gw.call_args("fdfd2D_factor", np.arange(5.0))
+    assert ei.value.identifier == "orf:invalidInput"
+    for args in [("fdfd2D_solve", 7.0, np.zeros((3, 3)), 0.0), ("fdfd2D_release", 65.0), ("fdfd2D_release", 1.5)]:
+        with pytest.raises(mexshim.MexError) as ei:
+            gw.call_args(*args)
+        assert ei.value.identifier == "orf:invalidInput"
+
+
+def test_fdfd_factor_without_a_device_raises_no_device(gw):
+    if orf.device_count() > 0:
+        pytest.skip("a GPU is present")
+    x, z, eps, lam, J, g, npml = _fdfd_args()
+    with pytest.raises(mexshim.MexError) as ei:
+        gw.call_args("fdfd2D_factor", x, z, eps, lam, np.asarray(npml, dtype=float), 1e-8)
+    assert ei.value.identifier == "orf:noDevice"
+
+
+@pytest.mark.gpu
+def test_gateway_fdfd_equals_python_binding(gw):
+    x, z, eps, lam, J, g, npml = _fdfd_args(60, 44, 5)
+    fid = gw.call_args("fdfd2D_factor", x, z, eps, lam, np.asarray(npml, dtype=float), 1e-8)
+    E = gw.call_args("fdfd2D_solve", fid, np.real(J), 0.0)      # a real current is accepted
+    lam_ = gw.call_args("fdfd2D_solve", fid, g.ravel(order="F"), 1.0)
+    o = orf.fdfd2D(x, z, eps, lam, np.real(J), Npml=npml)
+    assert np.array_equal(np.reshape(E, o.E.shape), o.E)
+    assert np.array_equal(np.reshape(lam_, o.E.shape), o.adjoint(g))
+    o.close()
+    assert gw.call_args("fdfd2D_release", fid) is None
+    with pytest.raises(mexshim.MexError) as ei:
+        gw.call_args("fdfd2D_solve", fid, np.real(J), 0.0)
+    assert ei.value.identifier == "orf:invalidInput"
