@@ -63,30 +63,6 @@ int validate2d(const orf_sim2d* s) {
     return ORF_OK;
 }
 
-// Distinct values -> dense index (insertion order), exact.
-struct Lut {
-    std::unordered_map<uint64_t, int> map;
-    std::vector<double> vals;
-    uint64_t last_key = ~uint64_t(0);   // neighbouring cells mostly share a material
-    int last_id = -1;
-    int get(double v) {
-        uint64_t key;
-        std::memcpy(&key, &v, 8);
-        if (key == last_key) return last_id;
-        auto it = map.find(key);
-        int id;
-        if (it != map.end()) {
-            id = it->second;
-        } else {
-            id = (int)vals.size();
-            map.emplace(key, id);
-            vals.push_back(v);
-        }
-        last_key = key;
-        last_id = id;
-        return id;
-    }
-};
 
 // Host-only plan of a run's 2D tiles: the interior kernel variant and fused
 // depth, the interior rectangle and the frame strips, and every tile's loaded
@@ -251,32 +227,29 @@ int Job2D<R>::create(const orf_sim2d* s) {
     const size_t cellsP = (size_t)pitch * nz;
 
     // ---- material index + coefficient table
-    Lut lut;
-    std::vector<uint16_t> ix0(cellsP, 0), ix1(te ? 0 : cellsP, 0);
-    lut.get(te ? s->eps[0] : s->eps_x[0]);
-    // one plane at a time, row by row, so the table's last-value shortcut hits
-    auto index_plane = [&](const double* e, int w, int h, std::vector<uint16_t>& ix) -> int {
-        for (int k = 0; k < h; ++k)
-            for (int i = 0; i < w; ++i) {
-                const int v = lut.get(e[i + (size_t)w * k]);
-                if (v > 65535) {
-                    set_error("more than 65536 distinct permittivity values");
-                    return ORF_ETOOLARGE;
-                }
-                ix[(size_t)k * pitch + i] = (uint16_t)v;
-            }
-        return ORF_OK;
+    // one plane at a time, row by row (index_values: several host threads
+    // for large grids, the indices of one sequential scan)
+    std::vector<uint32_t> ix0(cellsP, 0), ix1(te ? 0 : cellsP, 0);
+    std::vector<IndexRow> irows;
+    auto add_plane = [&](const double* e, int w, int h, std::vector<uint32_t>& ix) {
+        for (int k = 0; k < h; ++k) irows.push_back({e + (size_t)w * k, ix.data() + (size_t)k * pitch, w});
     };
     if (te) {
-        ORF_TRY(index_plane(s->eps, nx, nz, ix0));
+        add_plane(s->eps, nx, nz, ix0);
     } else {
-        ORF_TRY(index_plane(s->eps_x, nx, nzA, ix0));
-        ORF_TRY(index_plane(s->eps_z, nxB, nz, ix1));
+        add_plane(s->eps_x, nx, nzA, ix0);
+        add_plane(s->eps_z, nxB, nz, ix1);
     }
-    nlut = (int)lut.vals.size();
+    std::vector<double> lvals;
+    index_values(irows, lvals);
+    if (lvals.size() > 65536) {
+        set_error("more than 65536 distinct permittivity values");
+        return ORF_ETOOLARGE;
+    }
+    nlut = (int)lvals.size();
     idx16 = nlut > 256;
     std::vector<R> hlutc(nlut);
-    for (int v = 0; v < nlut; ++v) hlutc[v] = R(Cc / lut.vals[v]);
+    for (int v = 0; v < nlut; ++v) hlutc[v] = R(Cc / lvals[v]);
 
     // ---- CPML profiles
     const double alpha_max = kPmlAlphaMaxPerK0 * 2.0 * kPi / s->src_lambda0;
@@ -403,12 +376,13 @@ int Job2D<R>::create(const orf_sim2d* s) {
     std::vector<unsigned char> ib0(cellsP * isz), ib1(te ? 0 : cellsP * isz);
     // the device index: the 16-bit table index as is, or narrowed to bytes
     // (plain loops, one per plane, so the compiler vectorises them)
-    auto narrow = [&](const std::vector<uint16_t>& src, std::vector<unsigned char>& dst) {
+    auto narrow = [&](const std::vector<uint32_t>& src, std::vector<unsigned char>& dst) {
+        const uint32_t* v = src.data();
         if (idx16) {
-            std::memcpy(dst.data(), src.data(), cellsP * 2);
+            uint16_t* d = reinterpret_cast<uint16_t*>(dst.data());
+            for (size_t q = 0; q < cellsP; ++q) d[q] = (uint16_t)v[q];
         } else {
             unsigned char* d = dst.data();
-            const uint16_t* v = src.data();
             for (size_t q = 0; q < cellsP; ++q) d[q] = (unsigned char)v[q];
         }
     };
@@ -426,7 +400,7 @@ int Job2D<R>::create(const orf_sim2d* s) {
     ORF_TRY(up(d_ix0, ib0.data(), ib0.size()));
     if (!te) ORF_TRY(up(d_ix1, ib1.data(), ib1.size()));
     ORF_TRY(up(d_lutc, hlutc.data(), hlutc.size() * sizeof(R)));
-    ORF_TRY(up(d_lute, lut.vals.data(), lut.vals.size() * sizeof(double)));
+    ORF_TRY(up(d_lute, lvals.data(), lvals.size() * sizeof(double)));
     auto pxR = toR(px), pxhR = toR(pxh), pzR = toR(pz), pzhR = toR(pzh);
     ORF_TRY(up(d_px, pxR.data(), pxR.size() * sizeof(R)));
     ORF_TRY(up(d_pxh, pxhR.data(), pxhR.size() * sizeof(R)));

@@ -62,33 +62,6 @@ int validate3d(const orf_sim3d* s) {
     return ORF_OK;
 }
 
-namespace {
-
-struct Lut3 {
-    std::unordered_map<uint64_t, uint32_t> map;
-    std::vector<double> vals;
-    uint64_t last_key = ~0ull;
-    uint32_t last_id = 0;
-    uint32_t get(double v) {
-        uint64_t key;
-        std::memcpy(&key, &v, 8);
-        if (key == last_key) return last_id;
-        auto it = map.find(key);
-        uint32_t id;
-        if (it != map.end()) {
-            id = it->second;
-        } else {
-            id = (uint32_t)vals.size();
-            map.emplace(key, id);
-            vals.push_back(v);
-        }
-        last_key = key;
-        last_id = id;
-        return id;
-    }
-};
-
-}  // namespace
 
 // cuTensorMapEncodeTiled from the driver, looked up once through the runtime
 // (no link-time dependency on libcuda)
@@ -193,22 +166,25 @@ int Job3D<R>::create(const orf_sim3d* s) {
     cudaStream_t st = ctx->stream;
 
     // ---- material indices (exact table of distinct eps values)
-    Lut3 lut;
+    // component by component, row by row (index_values: several host
+    // threads for large grids, the indices of one sequential scan)
     const double* eps[3] = {s->eps_x, s->eps_y, s->eps_z};
     std::vector<uint32_t> ix[3];
+    std::vector<IndexRow> irows;
+    irows.reserve((size_t)3 * n[1] * n[2]);
     for (int c = 0; c < 3; ++c) {
         ix[c].assign(NP(), 0);
         for (int k = 0; k < n[2]; ++k)
-            for (int j = 0; j < n[1]; ++j) {
-                const double* src = eps[c] + (size_t)n[0] * ((size_t)j + (size_t)n[1] * k);
-                uint32_t* dst = ix[c].data() + ((size_t)k * n[1] + j) * pitch;
-                for (int i = 0; i < n[0]; ++i) dst[i] = lut.get(src[i]);
-            }
+            for (int j = 0; j < n[1]; ++j)
+                irows.push_back({eps[c] + (size_t)n[0] * ((size_t)j + (size_t)n[1] * k),
+                                 ix[c].data() + ((size_t)k * n[1] + j) * pitch, n[0]});
     }
-    const size_t nlut = lut.vals.size();
+    std::vector<double> lvals;
+    index_values(irows, lvals);
+    const size_t nlut = lvals.size();
     idxw = nlut <= 256 ? 1 : (nlut <= 65536 ? 2 : 4);
     std::vector<R> hlutc(nlut);
-    for (size_t v = 0; v < nlut; ++v) hlutc[v] = R(Cc / lut.vals[v]);
+    for (size_t v = 0; v < nlut; ++v) hlutc[v] = R(Cc / lvals[v]);
 
     // ---- CPML per axis
     const double alpha_max = kPmlAlphaMaxPerK0 * 2.0 * kPi / s->src_lambda0;
@@ -379,7 +355,7 @@ int Job3D<R>::create(const orf_sim3d* s) {
         std::vector<uint32_t>().swap(ix[c]);
     }
     ORF_TRY(up(d_lutc, hlutc.data(), nlut * sizeof(R)));
-    ORF_TRY(up(d_lute, lut.vals.data(), nlut * sizeof(double)));
+    ORF_TRY(up(d_lute, lvals.data(), nlut * sizeof(double)));
     for (int q = 0; q < 3; ++q) {
         std::vector<R> a(pI[q].begin(), pI[q].end()), b(pH[q].begin(), pH[q].end());
         ORF_TRY(up(d_pI[q], a.data(), a.size() * sizeof(R)));

@@ -257,6 +257,89 @@ int copy_d2h_staged(void* dst, const void* src, size_t bytes, void* stage, cudaS
     return ORF_OK;
 }
 
+namespace {
+// one table: distinct values in first-occurrence order, with the last value
+// remembered (neighbouring cells mostly share a material)
+struct ValueTable {
+    std::unordered_map<uint64_t, uint32_t> map;
+    std::vector<double> vals;
+    uint64_t last_key = ~uint64_t(0);
+    uint32_t last_id = 0;
+    uint32_t get(double v) {
+        uint64_t key;
+        std::memcpy(&key, &v, 8);
+        if (key == last_key) return last_id;
+        auto it = map.find(key);
+        uint32_t id;
+        if (it != map.end()) {
+            id = it->second;
+        } else {
+            id = (uint32_t)vals.size();
+            map.emplace(key, id);
+            vals.push_back(v);
+        }
+        last_key = key;
+        last_id = id;
+        return id;
+    }
+};
+}  // namespace
+
+void index_values(const std::vector<IndexRow>& rows, std::vector<double>& vals) {
+    size_t total = 0;
+    for (const auto& r : rows) total += (size_t)r.n;
+    const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+    const int T = total >= (size_t(1) << 20) ? std::min(16, hw) : 1;
+    // rows [cut[t], cut[t+1]) to thread t, about equal cells each
+    std::vector<size_t> cut(T + 1, rows.size());
+    cut[0] = 0;
+    {
+        size_t acc = 0;
+        int t = 1;
+        for (size_t q = 0; q < rows.size() && t < T; ++q) {
+            acc += (size_t)rows[q].n;
+            while (t < T && acc * T >= total * (size_t)t) cut[t++] = q + 1;
+        }
+    }
+    std::vector<ValueTable> loc(T);
+    auto scan = [&](int t) {
+        for (size_t q = cut[t]; q < cut[t + 1]; ++q) {
+            const IndexRow& r = rows[q];
+            for (int i = 0; i < r.n; ++i) r.dst[i] = loc[t].get(r.src[i]);
+        }
+    };
+    if (T == 1) {
+        scan(0);
+        vals = std::move(loc[0].vals);
+        return;
+    }
+    {
+        std::vector<std::thread> pool;
+        for (int t = 0; t < T; ++t) pool.emplace_back(scan, t);
+        for (auto& th : pool) th.join();
+    }
+    // the tables in row order: the global first occurrences
+    ValueTable glob;
+    std::vector<std::vector<uint32_t>> remap(T);
+    for (int t = 0; t < T; ++t) {
+        remap[t].resize(loc[t].vals.size());
+        for (size_t l = 0; l < loc[t].vals.size(); ++l) remap[t][l] = glob.get(loc[t].vals[l]);
+    }
+    auto apply = [&](int t) {
+        const uint32_t* m = remap[t].data();
+        for (size_t q = cut[t]; q < cut[t + 1]; ++q) {
+            const IndexRow& r = rows[q];
+            for (int i = 0; i < r.n; ++i) r.dst[i] = m[r.dst[i]];
+        }
+    };
+    {
+        std::vector<std::thread> pool;
+        for (int t = 0; t < T; ++t) pool.emplace_back(apply, t);
+        for (auto& th : pool) th.join();
+    }
+    vals = std::move(glob.vals);
+}
+
 void set_error(const char* fmt, ...) {
     char buf[1024];
     va_list ap;

@@ -143,6 +143,18 @@ void pinned_stage_release(void* buf);
 // the staging buffer `stage`, on stream st (synchronises st).
 int copy_d2h_staged(void* dst, const void* src, size_t bytes, void* stage, cudaStream_t st);
 
+// Exact dense index of the distinct values of a list of rows, in the order
+// of their first occurrence when the rows are scanned in order: dst[i] of a
+// row is the index of src[i] in vals.  Inputs of a million values or more
+// are scanned by up to 16 host threads (a table per thread, merged in row
+// order, so the indices are those of one sequential scan).
+struct IndexRow {
+    const double* src;
+    uint32_t* dst;
+    int n;
+};
+void index_values(const std::vector<IndexRow>& rows, std::vector<double>& vals);
+
 // Bump allocator over one device block: a job's buffers come from one block.
 struct Arena {
     std::vector<std::pair<void**, size_t>> req;
