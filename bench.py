@@ -372,6 +372,8 @@ def bench_pixel2d(args, rank, world, local, dist):
         te = _max_over_ranks(dist, te)
         e2e = {"value": cells * nsteps * args.steps * world / te / 1e6, "unit": UNIT,
                "h2d_bytes_per_step": es["h2d_bytes"] // args.steps, "d2h_bytes_per_step": es["d2h_bytes"] // args.steps,
+               "ms_per_step": 1e3 * te / args.steps,
+               "host_phase_ms": {k: es[k + "_ms"] / args.steps for k in ("setup", "loop", "finish")},
                "note": "orf.fdtd2D(sim): host eps arrays -> material index + tables -> device, "
                        "time loop, DFT lines + fluxes back to host"}
         ectx.close()

@@ -148,13 +148,22 @@ int32_t orf_fdtd2d_run_ctx(orf_ctx* ctx, const orf_sim2d* sim, orf_out2d* out, o
                            void* user) {
     if (!ctx || !sim || !out) { set_error("NULL argument"); return ORF_EINVAL; }
     ORF_ON_DEVICE(ctx->device);
+    // host phases into the context's counters: set-up (tables, device
+    // block, uploads), the time loop, results and release
     const double t0 = now_s();
     orf_job* job = nullptr;
     ORF_TRY(make_job2d(ctx, sim, &job));
     std::unique_ptr<orf_job> guard(job);
+    const double t1 = now_s();
     ORF_TRY(job->advance(job->step_budget(), progress, user));
+    const double t2 = now_s();
     ORF_TRY(job->finish2d(out));
-    out->wall_time = now_s() - t0;
+    guard.reset();
+    const double t3 = now_s();
+    ctx->stats.setup_ms += 1e3 * (t1 - t0);
+    ctx->stats.loop_ms += 1e3 * (t2 - t1);
+    ctx->stats.finish_ms += 1e3 * (t3 - t2);
+    out->wall_time = t3 - t0;
     return ORF_OK;
 }
 
@@ -245,13 +254,22 @@ int32_t orf_fdtd3d_run_ctx(orf_ctx* ctx, const orf_sim3d* sim, orf_out3d* out, o
                            void* user) {
     if (!ctx || !sim || !out) { set_error("NULL argument"); return ORF_EINVAL; }
     ORF_ON_DEVICE(ctx->device);
+    // host phases into the context's counters: set-up (tables, device
+    // block, uploads), the time loop, results and release
     const double t0 = now_s();
     orf_job* job = nullptr;
     ORF_TRY(make_job3d(ctx, sim, &job));
     std::unique_ptr<orf_job> guard(job);
+    const double t1 = now_s();
     ORF_TRY(job->advance(job->step_budget(), progress, user));
+    const double t2 = now_s();
     ORF_TRY(job->finish3d(out));
-    out->wall_time = now_s() - t0;
+    guard.reset();
+    const double t3 = now_s();
+    ctx->stats.setup_ms += 1e3 * (t1 - t0);
+    ctx->stats.loop_ms += 1e3 * (t2 - t1);
+    ctx->stats.finish_ms += 1e3 * (t3 - t2);
+    out->wall_time = t3 - t0;
     return ORF_OK;
 }
 
