@@ -380,20 +380,19 @@ __global__ void __launch_bounds__(NT, 1) k_fdfd_factor_panel(FdfdDev P) {
             // one block barrier per pivot step: every row thread publishes its
             // row and every warp its candidate (buffers alternate by step), then
             // every warp reduces the candidates itself and reads the pivot row
-            for (int aa = 0; aa < we; ++aa) {
+            // (unrolled: a row's entries are registers indexed by the step)
+#pragma unroll
+            for (int aa = 0; aa < W; ++aa) {
+                if (aa >= we) break;
                 const int sp2 = aa & 1;
                 double2* rows = s_rows + (size_t)sp2 * m * W;
                 double best = -1.0;
                 int bi = m;
                 if (t < m) {
-                    double2 v = pr[0];
 #pragma unroll
-                    for (int l = 0; l < W; ++l) {
-                        rows[(size_t)t * W + l] = pr[l];
-                        if (l == aa) v = pr[l];
-                    }
+                    for (int l = 0; l < W; ++l) rows[(size_t)t * W + l] = pr[l];
                     if (!myused) {
-                        best = cabs2(v);
+                        best = cabs2(pr[aa]);
                         bi = t;
                     }
                 }
@@ -438,10 +437,7 @@ __global__ void __launch_bounds__(NT, 1) k_fdfd_factor_panel(FdfdDev P) {
                 const double inv_dd = dd == 0.0 ? 0.0 : 1.0 / dd;
                 const double2 ip = make_double2(pk.x * inv_dd, -pk.y * inv_dd);
                 if (t < m) {
-                    double2 f = pr[0];
-#pragma unroll
-                    for (int l = 1; l < W; ++l)
-                        if (l == aa) f = pr[l];
+                    const double2 f = pr[aa];
 #pragma unroll
                     for (int l = 0; l < W; ++l) {
                         const double2 sp = l == aa ? ip : cmul(prw[l], ip);   // the scaled pivot row

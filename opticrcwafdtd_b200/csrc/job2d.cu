@@ -229,7 +229,11 @@ int Job2D<R>::create(const orf_sim2d* s) {
     // ---- material index + coefficient table
     // one plane at a time, row by row (index_values: several host threads
     // for large grids, the indices of one sequential scan)
-    std::vector<uint32_t> ix0(cellsP, 0), ix1(te ? 0 : cellsP, 0);
+    // (host scratch of the calling thread, kept between jobs: large grids
+    // then touch no new pages; entries outside the planes are never read)
+    thread_local std::vector<uint32_t> ix0, ix1;
+    ix0.resize(std::max(ix0.size(), cellsP));
+    if (!te) ix1.resize(std::max(ix1.size(), cellsP));
     std::vector<IndexRow> irows;
     auto add_plane = [&](const double* e, int w, int h, std::vector<uint32_t>& ix) {
         for (int k = 0; k < h; ++k) irows.push_back({e + (size_t)w * k, ix.data() + (size_t)k * pitch, w});
@@ -373,21 +377,36 @@ int Job2D<R>::create(const orf_sim2d* s) {
     }
 
     // ---- upload
-    std::vector<unsigned char> ib0(cellsP * isz), ib1(te ? 0 : cellsP * isz);
-    // the device index: the 16-bit table index as is, or narrowed to bytes
-    // (plain loops, one per plane, so the compiler vectorises them)
-    auto narrow = [&](const std::vector<uint32_t>& src, std::vector<unsigned char>& dst) {
+    thread_local std::vector<unsigned char> ib0, ib1;
+    ib0.resize(cellsP * isz);
+    ib1.resize(te ? 0 : cellsP * isz);
+    // the device index: 16-bit or 8-bit table indices of a plane of w x h
+    // cells in rows of `pitch`, zero outside the plane (rows split over
+    // host threads)
+    auto narrow = [&](const std::vector<uint32_t>& src, int w, int hh, std::vector<unsigned char>& dst) {
         const uint32_t* v = src.data();
-        if (idx16) {
-            uint16_t* d = reinterpret_cast<uint16_t*>(dst.data());
-            for (size_t q = 0; q < cellsP; ++q) d[q] = (uint16_t)v[q];
-        } else {
-            unsigned char* d = dst.data();
-            for (size_t q = 0; q < cellsP; ++q) d[q] = (unsigned char)v[q];
-        }
+        parallel_rows_n(nz, (size_t)pitch, [&](int k0, int k1) {
+            for (int k = k0; k < k1; ++k) {
+                const size_t o = (size_t)k * pitch;
+                const int ww = k < hh ? w : 0;
+                if (idx16) {
+                    uint16_t* d = reinterpret_cast<uint16_t*>(dst.data()) + o;
+                    for (int i = 0; i < ww; ++i) d[i] = (uint16_t)v[o + i];
+                    for (int i = ww; i < pitch; ++i) d[i] = 0;
+                } else {
+                    unsigned char* d = dst.data() + o;
+                    for (int i = 0; i < ww; ++i) d[i] = (unsigned char)v[o + i];
+                    for (int i = ww; i < pitch; ++i) d[i] = 0;
+                }
+            }
+        });
     };
-    narrow(ix0, ib0);
-    if (!te) narrow(ix1, ib1);
+    if (te) {
+        narrow(ix0, nx, nz, ib0);
+    } else {
+        narrow(ix0, nx, nzA, ib0);
+        narrow(ix1, nxB, nz, ib1);
+    }
     // (bytes counted here and added to the context's counter once, under a
     // lock: a batch creates its instances on several host threads)
     int64_t h2d = 0;

@@ -340,6 +340,21 @@ void index_values(const std::vector<IndexRow>& rows, std::vector<double>& vals) 
     vals = std::move(glob.vals);
 }
 
+void parallel_rows_n(int n, size_t cells_per_row, const std::function<void(int, int)>& fn) {
+    const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+    const int T = (size_t)n * cells_per_row >= (size_t(1) << 20) ? std::min({16, hw, n}) : 1;
+    if (T <= 1) {
+        if (n > 0) fn(0, n);
+        return;
+    }
+    std::vector<std::thread> pool;
+    for (int t = 0; t < T; ++t) {
+        const int a = (int)((int64_t)n * t / T), b = (int)((int64_t)n * (t + 1) / T);
+        pool.emplace_back([&fn, a, b] { fn(a, b); });
+    }
+    for (auto& th : pool) th.join();
+}
+
 void set_error(const char* fmt, ...) {
     char buf[1024];
     va_list ap;

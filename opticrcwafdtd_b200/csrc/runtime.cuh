@@ -8,6 +8,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <atomic>
 #include <memory>
 #include <string>
@@ -154,6 +155,10 @@ struct IndexRow {
     int n;
 };
 void index_values(const std::vector<IndexRow>& rows, std::vector<double>& vals);
+
+// fn(r0, r1) over rows [0, n) split into contiguous ranges, on up to 16
+// host threads when the n rows of cells_per_row cells hold a million or more
+void parallel_rows_n(int n, size_t cells_per_row, const std::function<void(int, int)>& fn);
 
 // Bump allocator over one device block: a job's buffers come from one block.
 struct Arena {
