@@ -66,10 +66,12 @@ def parse(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="headline only, without the sub-records")
-    ap.add_argument("--workload", default="pixel2d", choices=["pixel2d", "coupler", "pillar3d", "coupler_batch", "serve", "fdfd"],
+    ap.add_argument("--workload", default="pixel2d", choices=["pixel2d", "coupler", "pillar3d", "pillar3d_slabs", "coupler_batch", "serve",
+                                                       "fdfd"],
                     help="pixel2d is the headline; the others measure one form alone")
     ap.add_argument("--batch", type=int, default=256)
     ap.add_argument("--size3d", default="600,600,300", help="pillar3d grid NX,NY,NZ (smaller for profiling)")
+    ap.add_argument("--slabs", type=int, default=2, help="pillar3d_slabs: z slabs of the grid")
     ap.add_argument("--serve-jobs", type=int, default=100)
     ap.add_argument("--serve-load", type=float, default=0.8, help="arrival rate as a fraction of the measured capacity")
     ap.add_argument("--serve-rate", type=float, default=0.0, help="fixed arrival rate (jobs/s) instead of --serve-load")
@@ -477,6 +479,73 @@ def bench_pillar3d(args, rank, world, local, dist):
     return line
 
 
+def bench_pillar3d_slabs(args, rank, world, local, dist):
+    """The 3D pillar lattice computed as z slabs on one GPU (slab3d.SlabRun:
+    one slab job per slab, ghost planes swapped by device copies after every
+    step), timed beside the same run on one grid; the DFT planes of both
+    compared bit for bit."""
+    import numpy as np
+    import torch
+    from opticrcwafdtd_b200 import Context, Job, SlabRun, workloads
+    nsteps = args.time_steps or 300
+    nx3, ny3, nz3 = (int(v) for v in args.size3d.split(","))
+    sim = workloads.pillar_lattice_sim(nx=nx3, ny=ny3, nz=nz3, steps=nsteps, precision=args.precision, device=True)
+    cells = nx3 * ny3 * nz3
+    run = SlabRun(sim, args.slabs, local)
+    stream = torch.cuda.current_stream()
+    ctx = Context(local, stream=stream.cuda_stream)
+    job = Job(sim, ctx, dims=3)
+
+    def timed(fn, sync_stream):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(sync_stream)
+        for _ in range(args.steps):
+            fn()
+        ev1.record(sync_stream)
+        torch.cuda.synchronize()
+        return ev0.elapsed_time(ev1)
+
+    def slab_run():
+        run.reset()
+        run.run()
+
+    def one_grid():
+        job.reset()
+        job.advance(nsteps)
+
+    with ClockSampler(local) as clk:
+        ms_slab = timed(slab_run, run.stream)
+        ms_one = timed(one_grid, stream)
+    out_s = run.finish()
+    out_1 = job.finish()
+    same = all(np.array_equal(a[k], b[k]) for a, b in zip(out_s["mon"], out_1["mon"]) for k in ("Ea", "Eb", "Ha", "Hb"))
+    v_slab = cells * nsteps * args.steps / (ms_slab / 1e3) / 1e6
+    v_one = cells * nsteps * args.steps / (ms_one / 1e3) / 1e6
+    bpc = BYTES_3D[args.precision]
+    line = {"metric": METRIC, "value": v_slab, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_slab / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if args.precision == "single" else "f64",
+            "data": "synthetic (seeded TiO2 pillar radii U[60,180] nm)",
+            "config": {"workload": f"3D pillar lattice {nx3}x{ny3}x{nz3} as {args.slabs} z slabs on one GPU "
+                                   f"(ghost planes swapped after every step), {nsteps} time steps",
+                       "cells": cells, "slabs": [[q.z0, q.z1] for q in run.slabs], "parallelism": "z slabs x1 GPU",
+                       "l2": "inputs larger than L2"},
+            "whole_step_roofline": _whole_frac(v_slab * 1e6, bpc),
+            "one_grid_value": v_one, "slab_over_one_grid": v_slab / v_one,
+            "monitors_bitwise_equal_one_grid": bool(same),
+            # per inner cut: Ex Ey Ez planes up, Ex Ey planes down (pitch x ny each)
+            "swap_bytes_per_step": 5 * ((nx3 + 31) // 32 * 32) * ny3 * (4 if args.precision == "single" else 8)
+                                   * (len(run.slabs) - 1),
+            "clocks": clk.summary()}
+    run.close()
+    job.close()
+    ctx.close()
+    return line
+
+
 def bench_coupler_batch(args, rank, world, local, dist):
     """256 uneven 2D TE grating couplers advanced together (orf_batch2d_run)."""
     import numpy as np
@@ -738,6 +807,7 @@ def bench_fdfd(args, rank, world, local, dist):
 
 
 WORKLOADS = {"pixel2d": bench_pixel2d, "coupler": bench_pixel2d, "pillar3d": bench_pillar3d,
+             "pillar3d_slabs": bench_pillar3d_slabs,
              "coupler_batch": bench_coupler_batch, "serve": bench_serve, "fdfd": bench_fdfd}
 
 
@@ -751,6 +821,8 @@ def run_forms(args, local):
                                             size3d="600,600,300")),
         ("c3_pillar_fp64", "pillar3d", dict(time_steps=1000, steps=3, warmup=3, precision="double",
                                             size3d="600,600,300")),
+        ("c3_pillar_fp32_2slabs", "pillar3d_slabs", dict(time_steps=300, steps=3, warmup=3, precision="single",
+                                                        size3d="600,600,300", slabs=2)),
         ("c4_coupler_batch", "coupler_batch", dict(time_steps=10000, steps=3, warmup=3, precision="single",
                                                    batch=256)),
         ("c5_served", "serve", dict()),

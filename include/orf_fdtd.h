@@ -298,6 +298,32 @@ ORF_API int32_t orf_job3d_finish(orf_job* job, orf_out3d* out);
  * (nx-1)*nz doubles; 3D fills the six components (nx*ny*nz each, order
  * Ex Ey Ez Hx Hy Hz).  For parity tests. */
 ORF_API int32_t orf_job_get_fields(orf_job* job, double* const* fields, int32_t nfields);
+
+/* No counterpart in the reference (fdtd3D.m:1-29 runs one grid).  One z slab
+ * of a 3D grid too large for one GPU: `slab` describes planes [z_offset,
+ * z_offset + slab->nz) of a grid of nz_global planes -- their eps, the
+ * source and monitors in local indices, npml of the whole grid.  Its CPML
+ * profile in z is the whole grid's at those planes (none at an end that
+ * borders another slab), so the slab's cells update bit for bit as in the
+ * whole grid once its edge planes hold the neighbours' values: an inner end
+ * carries one ghost plane, written by the caller after every step from the
+ * neighbouring slab (below: Ex Ey Ez Hx Hy of its last own plane; above: Ex
+ * Ey of its first own plane).  Needs a non-periodic z axis, shutoff = 0
+ * (fixed step count) and inner ends outside the grid's CPML (ORF_EINVAL).
+ * Fields are [nz][ny][pitch] per component, pitch = nx rounded up to 32. */
+ORF_API int32_t orf_job3d_create_slab(orf_ctx* ctx, const orf_sim3d* slab, int32_t z_offset,
+                                      int32_t nz_global, orf_job** job);
+/* Enqueues exactly nsteps more steps of a 3D job on its context's stream
+ * (the DFT fold and check after the 50th step of each chunk and after the
+ * run's last step) and returns without waiting; after s steps from the start
+ * the state is in buffer s % 2.  Does not mix with an unfinished chunk of
+ * orf_job_advance (ORF_EINVAL). */
+ORF_API int32_t orf_job3d_step(orf_job* job, int64_t nsteps);
+/* Device address and size of plane k of field `field` (0..5: Ex Ey Ez Hx Hy
+ * Hz) in field buffer `buffer` (0 or 1) of a 3D job: ny * pitch elements of
+ * the run's precision, contiguous.  For halo exchanges between slabs. */
+ORF_API int32_t orf_job3d_plane(orf_job* job, int32_t buffer, int32_t field, int32_t k, void** dev,
+                                size_t* bytes);
 ORF_API int32_t orf_job_destroy(orf_job* job);
 
 /* Checkpoint / resume (no counterpart in the reference).  The state of a job

@@ -18,3 +18,4 @@ from .coupler import (apodizedGrating, bestFiberCoupling, fiberCoupling, grating
 __version__ = "0.1.0"
 from .fdtd import Context, Job, Server, device_count, fdtd2D, fdtd2D_batch, fdtd2DTE, fdtd3D  # noqa: F401,E402
 from .fdfd import FDFD2D, fdfd2D  # noqa: F401,E402
+from .slab3d import SlabRun, fdtd3D_distributed, fdtd3D_slabs  # noqa: F401,E402

@@ -36,6 +36,10 @@ _SIGS = {
     "orf_fdtd2d_run_noalloc": (C.c_int32, [P(_abi.OrfSim2D), P(_abi.OrfOut2D), C.c_void_p]),
     "orf_job2d_create": (C.c_int32, [C.c_void_p, P(_abi.OrfSim2D), P(C.c_void_p)]),
     "orf_job3d_create": (C.c_int32, [C.c_void_p, P(_abi.OrfSim3D), P(C.c_void_p)]),
+    "orf_job3d_create_slab": (C.c_int32, [C.c_void_p, P(_abi.OrfSim3D), C.c_int32, C.c_int32, P(C.c_void_p)]),
+    "orf_job3d_step": (C.c_int32, [C.c_void_p, C.c_int64]),
+    "orf_job3d_plane": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, P(C.c_void_p),
+                                    P(C.c_size_t)]),
     "orf_job_advance": (C.c_int32, [C.c_void_p, C.c_int64]),
     "orf_job_sync": (C.c_int32, [C.c_void_p]),
     "orf_job_reset": (C.c_int32, [C.c_void_p]),

@@ -192,6 +192,30 @@ int32_t orf_job3d_create(orf_ctx* ctx, const orf_sim3d* sim, orf_job** job) {
     return st;
 }
 
+int32_t orf_job3d_create_slab(orf_ctx* ctx, const orf_sim3d* slab, int32_t z_offset, int32_t nz_global,
+                              orf_job** job) {
+    if (!ctx || !job || !slab) return ORF_EINVAL;
+    ORF_ON_DEVICE(ctx->device);
+    const int st = make_job3d_slab(ctx, slab, z_offset, nz_global, job);
+    if (st == ORF_OK) ctx_retain(ctx);
+    return st;
+}
+
+int32_t orf_job3d_step(orf_job* job, int64_t nsteps) {
+    if (!job) return ORF_EINVAL;
+    if (job->dims != 3) {
+        set_error("orf_job3d_step takes a 3D job");
+        return ORF_EINVAL;
+    }
+    ORF_ON_DEVICE(job->ctx->device);
+    return job->step_async(nsteps);
+}
+
+int32_t orf_job3d_plane(orf_job* job, int32_t buffer, int32_t field, int32_t k, void** dev, size_t* bytes) {
+    if (!job || job->dims != 3) return ORF_EINVAL;
+    return job->plane_ptr(buffer, field, k, dev, bytes);
+}
+
 int32_t orf_job_advance(orf_job* job, int64_t nsteps) {
     if (!job || nsteps < 0) return ORF_EINVAL;
     ORF_ON_DEVICE(job->ctx->device);

@@ -17,7 +17,7 @@
 
 namespace orf {
 
-int validate3d(const orf_sim3d* s) {
+int validate3d(const orf_sim3d* s, bool slab) {
     if (!s) { set_error("sim is NULL"); return ORF_EINVAL; }
     const int n[3] = {s->nx, s->ny, s->nz};
     for (int q = 0; q < 3; ++q)
@@ -45,7 +45,10 @@ int validate3d(const orf_sim3d* s) {
     if (a < 0 || a > 2) { set_error("source.axis must be 1, 2 or 3"); return ORF_EINVAL; }
     const int np = s->periodic[a] ? 0 : s->npml[a];
     if (s->src_index < 0 || s->src_index >= n[a]) { set_error("source.index outside the grid"); return ORF_EINVAL; }
-    if (s->src_index < np || s->src_index >= n[a] - np) { set_error("source.index lies inside the CPML"); return ORF_EINVAL; }
+    if (!(slab && a == 2) && (s->src_index < np || s->src_index >= n[a] - np)) {
+        set_error("source.index lies inside the CPML");
+        return ORF_EINVAL;
+    }
     if (!s->src_Ea || !s->src_Eb || !s->src_Ha || !s->src_Hb) { set_error("source profiles Ea, Eb, Ha, Hb are required"); return ORF_EINVAL; }
     if (!(s->src_lambda0 > 0) || !(s->src_bw > 0)) { set_error("source.lambda0 and source.bw must be positive"); return ORF_EINVAL; }
     if (s->n_mon < 0 || s->n_mon > kMaxMon) { set_error("at most %d monitors", kMaxMon); return ORF_EINVAL; }
@@ -62,6 +65,17 @@ int validate3d(const orf_sim3d* s) {
     return ORF_OK;
 }
 
+
+namespace {
+// psi plane of position u of an n-point axis with an np-position layer at
+// both ends (half: the positions u + 1/2), -1 outside: the step kernel's map
+int slab_index(bool half, int u, int n, int np) {
+    if (np <= 0) return -1;
+    if (u < np) return u;
+    const int hi = half ? n - 1 - np : n - np;
+    return u >= hi ? np + (u - hi) : -1;
+}
+}  // namespace
 
 // cuTensorMapEncodeTiled from the driver, looked up once through the runtime
 // (no link-time dependency on libcuda)
@@ -113,7 +127,7 @@ int Job3D<R>::encode_tmap3(CUtensorMap* m, CUtensorMapDataType t, const void* ba
 // segments of at most kSeg3 planes never mix planes near a z slab with planes
 // away from it, so only the planes that need CPML code run it.  Needs no
 // device; orf_plan3d exposes it for checks of the tiling.
-void plan3d(const orf_sim3d* s, std::vector<Tile3D>& tiles, std::vector<Tile3D>& tiles_pml) {
+void plan3d(const orf_sim3d* s, std::vector<Tile3D>& tiles, std::vector<Tile3D>& tiles_pml, bool zlo, bool zhi) {
     const int n[3] = {s->nx, s->ny, s->nz};
     bool per[3];
     for (int q = 0; q < 3; ++q) per[q] = s->periodic[q] != 0;
@@ -122,7 +136,8 @@ void plan3d(const orf_sim3d* s, std::vector<Tile3D>& tiles, std::vector<Tile3D>&
     auto near_pml = [&](int q, int lo, int hi) {   // cells [lo, hi) along axis q
         const int np = per[q] ? 0 : s->npml[q];
         if (np <= 0) return false;
-        return lo < np + 1 || hi > n[q] - np - 2;
+        const bool at_lo = q != 2 || zlo, at_hi = q != 2 || zhi;
+        return (at_lo && lo < np + 1) || (at_hi && hi > n[q] - np - 2);
     };
     std::vector<std::pair<int, int>> segs;
     for (int k0 = 0; k0 < n[2];) {
@@ -151,7 +166,7 @@ void plan3d(const orf_sim3d* s, std::vector<Tile3D>& tiles, std::vector<Tile3D>&
 
 template <class R>
 int Job3D<R>::create(const orf_sim3d* s) {
-    ORF_TRY(validate3d(s));
+    ORF_TRY(validate3d(s, slab));
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev != ctx->device) ORF_CUDA(cudaSetDevice(ctx->device));
@@ -193,6 +208,43 @@ int Job3D<R>::create(const orf_sim3d* s) {
     int nsI[3], nsH[3];
     for (int q = 0; q < 3; ++q) {
         const int np = per[q] ? 0 : s->npml[q];
+        if (slab && q == 2) {
+            // the global grid's z profile at the slab's planes: identity at an
+            // end that borders another slab.  psi keeps the layout of a
+            // symmetric np-plane layer at both local ends (the kernel's slab
+            // map); at an inner end it stays zero, and b = 1, a = 0 leave each
+            // difference unchanged bit for bit.
+            std::vector<double> gI, gH;
+            pml_profile(nz_glob, nz_glob, np, 0.0, d, S, alpha_max, gI, nullptr);
+            pml_profile(nz_glob, nz_glob, np, 0.5, d, S, alpha_max, gH, nullptr);
+            pI[q].assign(gI.begin() + 3 * (size_t)z_off, gI.begin() + 3 * ((size_t)z_off + n[q]));
+            pH[q].assign(gH.begin() + 3 * (size_t)z_off, gH.begin() + 3 * ((size_t)z_off + n[q]));
+            slI[q].assign(n[q], -1);
+            slH[q].assign(n[q], -1);
+            const bool inner_lo = z_off > 0, inner_hi = z_off + n[q] < nz_glob;
+            for (int u = 0; u < n[q]; ++u) {
+                const int si = slab_index(false, u, n[q], np), sh = slab_index(true, u, n[q], np);
+                slI[q][u] = si;
+                slH[q][u] = sh;
+                const bool ai = pI[q][3 * u + 1] != 0.0 || pI[q][3 * u] != 1.0 || pI[q][3 * u + 2] != 1.0;
+                const bool ah = pH[q][3 * u + 1] != 0.0 || pH[q][3 * u] != 1.0 || pH[q][3 * u + 2] != 1.0;
+                // the layer positions of an end that borders another slab
+                // carry no absorption; every absorbing position has psi
+                const bool lo_i = si >= 0 && u < np, lo_h = sh >= 0 && u < np;
+                const bool bad = (ai && si < 0) || (ah && sh < 0) ||
+                                 (inner_lo && ((ai && lo_i) || (ah && lo_h))) ||
+                                 (inner_hi && ((ai && si >= 0 && !lo_i) || (ah && sh >= 0 && !lo_h)));
+                if (bad) {
+                    set_error("z slab [%d, %d) of %d planes: an end that borders another slab lies within %d "
+                              "planes of the grid's %d-plane CPML",
+                              z_off, z_off + n[q], nz_glob, np + 1, np);
+                    return ORF_EINVAL;
+                }
+            }
+            nsI[q] = np > 0 ? 2 * np : 0;
+            nsH[q] = np > 0 ? 2 * np + 1 : 0;
+            continue;
+        }
         pml_profile(n[q], n[q], np, 0.0, d, S, alpha_max, pI[q], &nsI[q]);
         pml_profile(n[q], n[q], np, 0.5, d, S, alpha_max, pH[q], &nsH[q]);
         slI[q].assign(n[q], -1);
@@ -263,7 +315,9 @@ int Job3D<R>::create(const orf_sim3d* s) {
     npairs = (int)pairs.size();
 
     // ---- tiles (plan3d)
-    plan3d(s, tiles, tiles_pml);
+    // a z slab's ends that border other slabs carry no CPML: their planes are
+    // interior tiles (the psi planes of the layout there stay unused)
+    plan3d(s, tiles, tiles_pml, !slab || z_off == 0, !slab || z_off + n[2] == nz_glob);
     zc = kSeg3;
 
     // ---- device arena
@@ -517,6 +571,8 @@ int Job3D<R>::init_state() {
     if (ring_h) std::memset(ring_h, 0, sizeof(ChunkStatus) * kStatusRing);
     if (cancel_h) *cancel_h = 0;
     enq_steps = 0;
+    sdone = 0;
+    soff = 0;
     ORF_CUDA(cudaMemcpyAsync(d_st, &js, sizeof js, cudaMemcpyHostToDevice, ctx->stream));
     ORF_CUDA(cudaStreamSynchronize(ctx->stream));
     pl = ProgressLoop{};
@@ -585,6 +641,8 @@ uint64_t Job3D<R>::state_key() const {
 template <class R>
 void Job3D<R>::resume_host(const JobState& js) {
     enq_steps = js.chunk * kChunk;
+    sdone = js.step;
+    soff = 0;
     pl = ProgressLoop{};
     pl.ring = ring_h;
     pl.cancel = cancel_h;
@@ -605,6 +663,11 @@ int Job3D<R>::advance(int64_t nsteps, orf_progress_fn progress, void* user) {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev != ctx->device) ORF_CUDA(cudaSetDevice(ctx->device));
+    if (soff != 0) {
+        set_error("advance: a chunk begun by orf_job3d_step is unfinished (%d of %d steps)", soff, kChunk);
+        return ORF_EINVAL;
+    }
+    enq_steps = std::max(enq_steps, sdone);
     const int64_t left = std::max<int64_t>(0, nmax - enq_steps);
     const int64_t chunks = (std::min(nsteps, left) + kChunk - 1) / kChunk;
     enq_steps += chunks * kChunk;
@@ -613,6 +676,43 @@ int Job3D<R>::advance(int64_t nsteps, orf_progress_fn progress, void* user) {
     eng.collect_timing();
     ctx->stats.cell_updates += (pl.last_step - steps0) * (int64_t)N();
     return pl.cancelled ? ORF_ECANCELLED : ORF_OK;
+}
+
+// One launch pair per step, as in a chunk of advance(), with the sample slot
+// of the step in its chunk; the chunk's DFT flush and check follow its last
+// step, or the run's last one.  The host does not wait.
+template <class R>
+int Job3D<R>::step_async(int64_t nsteps) {
+    if (nsteps < 0) return ORF_EINVAL;
+    if (soff == 0) sdone = std::max(sdone, enq_steps);   // continue after whole chunks of advance()
+    cudaStream_t st = ctx->stream;
+    for (int64_t q = 0; q < nsteps && sdone < nmax; ++q) {
+        const int we = soff == kChunk - 1 ? 1 : 0;
+        ORF_CUDA(eng.step(soff, 1, eng.par, we, st, nullptr));
+        eng.par ^= 1;
+        ++soff;
+        ++sdone;
+        ctx->stats.cell_updates += (int64_t)N();
+        if (soff == kChunk || sdone == nmax) {
+            ORF_CUDA(launch_flush(sizeof(R) == 8, d_streams, d_items, nitems, st));
+            ORF_CUDA(launch_check(d_states, 1, st));
+            soff = 0;
+        }
+    }
+    enq_steps = std::max(enq_steps, sdone - soff);
+    return ORF_OK;
+}
+
+template <class R>
+int Job3D<R>::plane_ptr(int b, int f, int k, void** dev, size_t* bytes) {
+    if (b < 0 || b > 1 || f < 0 || f > 5 || k < 0 || k >= n[2] || !dev || !bytes) {
+        set_error("plane: buffer 0/1, field 0..5 (Ex Ey Ez Hx Hy Hz), plane 0..%d", n[2] - 1);
+        return ORF_EINVAL;
+    }
+    R* base = f < 3 ? h.E[b][f] : h.H[b][f - 3];
+    *dev = base + (size_t)k * n[1] * pitch;
+    *bytes = (size_t)n[1] * pitch * sizeof(R);
+    return ORF_OK;
 }
 
 template <class R>
@@ -699,6 +799,47 @@ int make_job3d(orf_ctx* ctx, const orf_sim3d* sim, orf_job** out) {
         auto j = std::make_unique<Job3D<double>>();
         j->ctx = ctx;
         ORF_TRY(j->create(sim));
+        *out = j.release();
+    }
+    return ORF_OK;
+}
+
+int make_job3d_slab(orf_ctx* ctx, const orf_sim3d* sim, int z_off, int nz_glob, orf_job** out) {
+    *out = nullptr;
+    ORF_TRY(validate3d(sim, true));
+    if (z_off < 0 || nz_glob < sim->nz || z_off + sim->nz > nz_glob) {
+        set_error("z slab [%d, %d) outside the %d planes of the grid", z_off, z_off + sim->nz, nz_glob);
+        return ORF_EINVAL;
+    }
+    if (sim->periodic[2]) {
+        set_error("a z slab needs a non-periodic z axis");
+        return ORF_EINVAL;
+    }
+    if (sim->shutoff != 0.0) {
+        set_error("z slabs run a fixed step count: shutoff must be 0 (the energy of one slab is not the run's)");
+        return ORF_EINVAL;
+    }
+    if (sim->src_axis == 2) {   // a z-normal source plane: outside the grid's CPML
+        const int g = z_off + sim->src_index, np = sim->npml[2];
+        if (g < np || g >= nz_glob - np) {
+            set_error("source.index lies inside the CPML of the grid");
+            return ORF_EINVAL;
+        }
+    }
+    auto build = [&](auto* j) -> int {
+        j->ctx = ctx;
+        j->slab = true;
+        j->z_off = z_off;
+        j->nz_glob = nz_glob;
+        return j->create(sim);
+    };
+    if (sim->precision == ORF_SINGLE) {
+        auto j = std::make_unique<Job3D<float>>();
+        ORF_TRY(build(j.get()));
+        *out = j.release();
+    } else {
+        auto j = std::make_unique<Job3D<double>>();
+        ORF_TRY(build(j.get()));
         *out = j.release();
     }
     return ORF_OK;

@@ -7,7 +7,10 @@
 namespace orf {
 
 // Host-only tile plan of a 3D run (job3d.cu): interior tiles and CPML tiles.
-void plan3d(const orf_sim3d* s, std::vector<Tile3D>& tiles, std::vector<Tile3D>& tiles_pml);
+// zlo / zhi: the low / high z end has its CPML layer (false: the end of a z
+// slab that borders another slab, whose planes run as interior tiles)
+void plan3d(const orf_sim3d* s, std::vector<Tile3D>& tiles, std::vector<Tile3D>& tiles_pml, bool zlo = true,
+            bool zhi = true);
 
 template <class R>
 struct Job3D : orf_job {
@@ -16,6 +19,14 @@ struct Job3D : orf_job {
     int pitch = 0, nM = 0, nL = 0, idxw = 1, zc = 4;
     double d = 0, Cc = 0, S = 0, src_end = 0, shutoff = 0;
     int64_t nmax = 0, nsrc = 0, enq_steps = 0;
+    // z slab of a larger grid (orf_job3d_create_slab): global index of local
+    // plane 0 and the global plane count (the z CPML profile is the global one)
+    bool slab = false;
+    int z_off = 0, nz_glob = 0;
+    // step-by-step enqueueing (orf_job3d_step): steps enqueued and the
+    // sample slot of the next step in its chunk
+    int64_t sdone = 0;
+    int soff = 0;
     Arena arena;
     Inst3D<R> h{};
     Inst3D<R>* d_inst = nullptr;
@@ -58,6 +69,8 @@ struct Job3D : orf_job {
     int64_t step_budget() const override { return nmax; }
 
     int create(const orf_sim3d* s);
+    int step_async(int64_t nsteps) override;
+    int plane_ptr(int buffer, int field, int k, void** dev, size_t* bytes) override;
     static constexpr int kTmaps3 = 23;   // E[2][3], H[2][3], index[3], z psi H[2][2], z psi E[2][2]
     // rows_pitch / nplanes: row length and plane count of the array (the
     // field pitch and nz unless given)

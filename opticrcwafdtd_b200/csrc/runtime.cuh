@@ -266,6 +266,10 @@ struct orf_job {
     virtual int get_fields(double* const* f, int nf) = 0;
     virtual int finish2d(orf_out2d*) { return ORF_EINVAL; }
     virtual int finish3d(orf_out3d*) { return ORF_EINVAL; }
+    // 3D: enqueue exactly nsteps steps without waiting (orf_job3d_step), and
+    // the device address of plane k of a field in a buffer (orf_job3d_plane)
+    virtual int step_async(int64_t) { return ORF_EINVAL; }
+    virtual int plane_ptr(int, int, int, void**, size_t*) { return ORF_EINVAL; }
     // checkpoint / resume (checkpoint.cu): the device regions of field
     // buffer b holding the run's state (fields, CPML psi, then the DFT sums,
     // which have one copy), a key of the grid and run options, the device
@@ -284,9 +288,13 @@ int job_checkpoint(orf_job* job, void* buf, size_t bytes);
 int job_restore(orf_job* job, const void* buf, size_t bytes, int into);
 int make_job2d(orf_ctx* ctx, const orf_sim2d* sim, orf_job** out);
 int make_job3d(orf_ctx* ctx, const orf_sim3d* sim, orf_job** out);
+// a z slab of a larger 3D grid: local plane 0 is global plane z_off of nz_glob
+int make_job3d_slab(orf_ctx* ctx, const orf_sim3d* sim, int z_off, int nz_glob, orf_job** out);
 int batch2d_run(orf_ctx* ctx, int n, const orf_sim2d* sims, orf_out2d* outs, orf_progress_fn progress,
                 void* user);
 int validate2d(const orf_sim2d* s);
-int validate3d(const orf_sim3d* s);
+// slab: the z position of a z-normal source is checked by the caller
+// against the global grid
+int validate3d(const orf_sim3d* s, bool slab = false);
 orf_ctx* default_ctx(int* status);
 }  // namespace orf

@@ -27,6 +27,7 @@ class Context:
         _lib.check(self._lib.orf_ctx_create(device, C.c_void_p(stream) if stream else None, C.byref(h)),
                    "orf_ctx_create")
         self.handle = h
+        self.device = device
 
     def set_tuning(self, tsteps: int = 0, variant: int = 0, use_graph: bool = True) -> None:
         t = _abi.OrfTuning(tsteps, variant, 1 if use_graph else 0, 0)
