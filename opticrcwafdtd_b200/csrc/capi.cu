@@ -144,15 +144,17 @@ int32_t orf_out2d_sizes(const orf_sim2d* s, int64_t* n_flux, int64_t* n_flux_z, 
     return ORF_OK;
 }
 
-int32_t orf_fdtd2d_run_ctx(orf_ctx* ctx, const orf_sim2d* sim, orf_out2d* out, orf_progress_fn progress,
-                           void* user) {
+namespace {
+// scanned: the caller validated the sim with its permittivity scan already
+int run2d_ctx(orf_ctx* ctx, const orf_sim2d* sim, orf_out2d* out, orf_progress_fn progress, void* user,
+              bool scanned) {
     if (!ctx || !sim || !out) { set_error("NULL argument"); return ORF_EINVAL; }
     ORF_ON_DEVICE(ctx->device);
     // host phases into the context's counters: set-up (tables, device
     // block, uploads), the time loop, results and release
     const double t0 = now_s();
     orf_job* job = nullptr;
-    ORF_TRY(make_job2d(ctx, sim, &job));
+    ORF_TRY(make_job2d(ctx, sim, &job, !scanned));
     std::unique_ptr<orf_job> guard(job);
     const double t1 = now_s();
     ORF_TRY(job->advance(job->step_budget(), progress, user));
@@ -166,14 +168,20 @@ int32_t orf_fdtd2d_run_ctx(orf_ctx* ctx, const orf_sim2d* sim, orf_out2d* out, o
     out->wall_time = t3 - t0;
     return ORF_OK;
 }
+}  // namespace
+
+int32_t orf_fdtd2d_run_ctx(orf_ctx* ctx, const orf_sim2d* sim, orf_out2d* out, orf_progress_fn progress,
+                           void* user) {
+    return run2d_ctx(ctx, sim, out, progress, user, false);
+}
 
 int32_t orf_fdtd2d_run(const orf_sim2d* sim, orf_out2d* out, orf_progress_fn progress, void* user) {
     if (!out) { set_error("out is NULL"); return ORF_EINVAL; }
-    ORF_TRY(validate2d(sim));
+    ORF_TRY(validate2d(sim));   // before any device work; the job does not scan again
     int st = ORF_OK;
     orf_ctx* c = default_ctx(&st);
     if (!c) return st;
-    return orf_fdtd2d_run_ctx(c, sim, out, progress, user);
+    return run2d_ctx(c, sim, out, progress, user, true);
 }
 
 int32_t orf_job2d_create(orf_ctx* ctx, const orf_sim2d* sim, orf_job** job) {
@@ -274,15 +282,16 @@ int32_t orf_out3d_sizes(const orf_sim3d* s, int32_t* na, int32_t* nb) {
     return ORF_OK;
 }
 
-int32_t orf_fdtd3d_run_ctx(orf_ctx* ctx, const orf_sim3d* sim, orf_out3d* out, orf_progress_fn progress,
-                           void* user) {
+namespace {
+int run3d_ctx(orf_ctx* ctx, const orf_sim3d* sim, orf_out3d* out, orf_progress_fn progress, void* user,
+              bool scanned) {
     if (!ctx || !sim || !out) { set_error("NULL argument"); return ORF_EINVAL; }
     ORF_ON_DEVICE(ctx->device);
     // host phases into the context's counters: set-up (tables, device
     // block, uploads), the time loop, results and release
     const double t0 = now_s();
     orf_job* job = nullptr;
-    ORF_TRY(make_job3d(ctx, sim, &job));
+    ORF_TRY(make_job3d(ctx, sim, &job, !scanned));
     std::unique_ptr<orf_job> guard(job);
     const double t1 = now_s();
     ORF_TRY(job->advance(job->step_budget(), progress, user));
@@ -296,14 +305,20 @@ int32_t orf_fdtd3d_run_ctx(orf_ctx* ctx, const orf_sim3d* sim, orf_out3d* out, o
     out->wall_time = t3 - t0;
     return ORF_OK;
 }
+}  // namespace
+
+int32_t orf_fdtd3d_run_ctx(orf_ctx* ctx, const orf_sim3d* sim, orf_out3d* out, orf_progress_fn progress,
+                           void* user) {
+    return run3d_ctx(ctx, sim, out, progress, user, false);
+}
 
 int32_t orf_fdtd3d_run(const orf_sim3d* sim, orf_out3d* out, orf_progress_fn progress, void* user) {
     if (!out) { set_error("out is NULL"); return ORF_EINVAL; }
-    ORF_TRY(validate3d(sim));
+    ORF_TRY(validate3d(sim));   // before any device work; the job does not scan again
     int st = ORF_OK;
     orf_ctx* c = default_ctx(&st);
     if (!c) return st;
-    return orf_fdtd3d_run_ctx(c, sim, out, progress, user);
+    return run3d_ctx(c, sim, out, progress, user, true);
 }
 
 int32_t orf_plan2d(const orf_sim2d* sim, const orf_tuning* tuning, orf_tile2d* tiles, int32_t cap,

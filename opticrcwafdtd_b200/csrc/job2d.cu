@@ -14,7 +14,7 @@
 
 namespace orf {
 
-int validate2d(const orf_sim2d* s) {
+int validate2d(const orf_sim2d* s, bool scan_eps) {
     if (!s) { set_error("sim is NULL"); return ORF_EINVAL; }
     if (s->pol != ORF_TE && s->pol != ORF_TM) { set_error("sim.pol must be TE or TM"); return ORF_EINVAL; }
     if (s->nx < 3 || s->nz < 2) { set_error("grid must be at least 3 x 2 cells"); return ORF_EINVAL; }
@@ -29,15 +29,16 @@ int validate2d(const orf_sim2d* s) {
     if (s->pol == ORF_TE && !s->eps) { set_error("sim.eps is required for TE"); return ORF_EINVAL; }
     if (s->pol == ORF_TM && (!s->eps_x || !s->eps_z)) { set_error("sim.epsX and sim.epsZ are required for TM"); return ORF_EINVAL; }
     auto chk = [&](const double* e, size_t n, const char* nm) {
-        for (size_t q = 0; q < n; ++q)
-            if (!(e[q] > 0) || !std::isfinite(e[q])) {
-                set_error("%s(%zu) = %g: permittivity must be positive and finite", nm, q + 1, e[q]);
-                return false;
-            }
+        const size_t q = first_bad_positive(e, n);
+        if (q < n) {
+            set_error("%s(%zu) = %g: permittivity must be positive and finite", nm, q + 1, e[q]);
+            return false;
+        }
         return true;
     };
-    if (s->pol == ORF_TE && !chk(s->eps, (size_t)nx * nz, "sim.eps")) return ORF_EINVAL;
-    if (s->pol == ORF_TM && (!chk(s->eps_x, (size_t)nx * nzA, "sim.epsX") || !chk(s->eps_z, (size_t)(nx - 1) * nz, "sim.epsZ")))
+    if (scan_eps && s->pol == ORF_TE && !chk(s->eps, (size_t)nx * nz, "sim.eps")) return ORF_EINVAL;
+    if (scan_eps && s->pol == ORF_TM &&
+        (!chk(s->eps_x, (size_t)nx * nzA, "sim.epsX") || !chk(s->eps_z, (size_t)(nx - 1) * nz, "sim.epsZ")))
         return ORF_EINVAL;
     const int npz = per ? 0 : s->npml_z;
     if (s->npml_x < 0 || 2 * s->npml_x >= nx - 1) { set_error("npml(1) = %d does not fit numel(x) = %d", s->npml_x, nx); return ORF_EINVAL; }
@@ -206,7 +207,7 @@ int plan2d(const orf_sim2d* s, const orf_tuning& tuning, Plan2D* plan) {
 
 template <class R>
 int Job2D<R>::create(const orf_sim2d* s) {
-    ORF_TRY(validate2d(s));
+    ORF_TRY(validate2d(s, false));   // every caller scanned the permittivity already
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev != ctx->device) ORF_CUDA(cudaSetDevice(ctx->device));
@@ -773,9 +774,9 @@ int Job2D<R>::get_fields(double* const* f, int nf) {
 template struct Job2D<float>;
 template struct Job2D<double>;
 
-int make_job2d(orf_ctx* ctx, const orf_sim2d* sim, orf_job** out) {
+int make_job2d(orf_ctx* ctx, const orf_sim2d* sim, orf_job** out, bool scan_eps) {
     *out = nullptr;
-    ORF_TRY(validate2d(sim));
+    ORF_TRY(validate2d(sim, scan_eps));
     if (sim->precision == ORF_SINGLE) {
         auto j = std::make_unique<Job2D<float>>();
         j->ctx = ctx;

@@ -17,7 +17,7 @@
 
 namespace orf {
 
-int validate3d(const orf_sim3d* s, bool slab) {
+int validate3d(const orf_sim3d* s, bool slab, bool scan_eps) {
     if (!s) { set_error("sim is NULL"); return ORF_EINVAL; }
     const int n[3] = {s->nx, s->ny, s->nz};
     for (int q = 0; q < 3; ++q)
@@ -31,12 +31,13 @@ int validate3d(const orf_sim3d* s, bool slab) {
     if (!s->eps_x || !s->eps_y || !s->eps_z) { set_error("sim.eps.x/.y/.z are required"); return ORF_EINVAL; }
     const size_t N = (size_t)n[0] * n[1] * n[2];
     const double* e[3] = {s->eps_x, s->eps_y, s->eps_z};
-    for (int c = 0; c < 3; ++c)
-        for (size_t q = 0; q < N; ++q)
-            if (!(e[c][q] > 0) || !std::isfinite(e[c][q])) {
-                set_error("sim.eps.%c(%zu) = %g: permittivity must be positive and finite", "xyz"[c], q + 1, e[c][q]);
-                return ORF_EINVAL;
-            }
+    for (int c = 0; c < 3 && scan_eps; ++c) {
+        const size_t q = first_bad_positive(e[c], N);
+        if (q < N) {
+            set_error("sim.eps.%c(%zu) = %g: permittivity must be positive and finite", "xyz"[c], q + 1, e[c][q]);
+            return ORF_EINVAL;
+        }
+    }
     for (int q = 0; q < 3; ++q) {
         const int np = s->periodic[q] ? 0 : s->npml[q];
         if (np < 0 || 2 * np >= n[q] - 1) { set_error("npml(%d) = %d does not fit the grid", q + 1, np); return ORF_EINVAL; }
@@ -166,7 +167,7 @@ void plan3d(const orf_sim3d* s, std::vector<Tile3D>& tiles, std::vector<Tile3D>&
 
 template <class R>
 int Job3D<R>::create(const orf_sim3d* s) {
-    ORF_TRY(validate3d(s, slab));
+    ORF_TRY(validate3d(s, slab, false));   // every caller scanned the permittivity already
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev != ctx->device) ORF_CUDA(cudaSetDevice(ctx->device));
@@ -787,9 +788,9 @@ int Job3D<R>::get_fields(double* const* f, int nf) {
 template struct Job3D<float>;
 template struct Job3D<double>;
 
-int make_job3d(orf_ctx* ctx, const orf_sim3d* sim, orf_job** out) {
+int make_job3d(orf_ctx* ctx, const orf_sim3d* sim, orf_job** out, bool scan_eps) {
     *out = nullptr;
-    ORF_TRY(validate3d(sim));
+    ORF_TRY(validate3d(sim, false, scan_eps));
     if (sim->precision == ORF_SINGLE) {
         auto j = std::make_unique<Job3D<float>>();
         j->ctx = ctx;

@@ -3,6 +3,7 @@
 #include <atomic>
 #include <map>
 #include <mutex>
+#include <cfloat>
 #include <thread>
 #include <unordered_map>
 
@@ -353,6 +354,32 @@ void parallel_rows_n(int n, size_t cells_per_row, const std::function<void(int, 
         pool.emplace_back([&fn, a, b] { fn(a, b); });
     }
     for (auto& th : pool) th.join();
+}
+
+size_t first_bad_positive(const double* v, size_t n) {
+    // blocks of 4096 values: a branch-free test of the whole block (positive
+    // and at most the largest finite double: NaN fails both), then the exact
+    // position inside the first block that fails
+    constexpr size_t kBlock = 4096;
+    const size_t nb = (n + kBlock - 1) / kBlock;
+    std::atomic<size_t> bad{n};
+    parallel_rows_n((int)nb, kBlock, [&](int b0, int b1) {
+        for (int b = b0; b < b1; ++b) {
+            const size_t a = (size_t)b * kBlock, e = std::min(n, a + kBlock);
+            if (a >= bad.load(std::memory_order_relaxed)) return;
+            bool ok = true;
+            for (size_t q = a; q < e; ++q) ok &= (v[q] > 0.0) & (v[q] <= DBL_MAX);
+            if (ok) continue;
+            for (size_t q = a; q < e; ++q)
+                if (!(v[q] > 0.0 && v[q] <= DBL_MAX)) {
+                    size_t cur = bad.load();
+                    while (q < cur && !bad.compare_exchange_weak(cur, q)) {
+                    }
+                    return;   // the rest of this range lies after q
+                }
+        }
+    });
+    return bad.load();
 }
 
 void set_error(const char* fmt, ...) {

@@ -156,6 +156,10 @@ struct IndexRow {
 };
 void index_values(const std::vector<IndexRow>& rows, std::vector<double>& vals);
 
+// Index of the first of the n values that is not positive and finite (n if
+// there is none), scanned by up to 16 host threads for long arrays.
+size_t first_bad_positive(const double* v, size_t n);
+
 // fn(r0, r1) over rows [0, n) split into contiguous ranges, on up to 16
 // host threads when the n rows of cells_per_row cells hold a million or more
 void parallel_rows_n(int n, size_t cells_per_row, const std::function<void(int, int)>& fn);
@@ -286,15 +290,18 @@ namespace orf {
 int job_checkpoint_size(orf_job* job, size_t* bytes);
 int job_checkpoint(orf_job* job, void* buf, size_t bytes);
 int job_restore(orf_job* job, const void* buf, size_t bytes, int into);
-int make_job2d(orf_ctx* ctx, const orf_sim2d* sim, orf_job** out);
-int make_job3d(orf_ctx* ctx, const orf_sim3d* sim, orf_job** out);
+// scan_eps = false: the caller validated the sim, permittivity included
+int make_job2d(orf_ctx* ctx, const orf_sim2d* sim, orf_job** out, bool scan_eps = true);
+int make_job3d(orf_ctx* ctx, const orf_sim3d* sim, orf_job** out, bool scan_eps = true);
 // a z slab of a larger 3D grid: local plane 0 is global plane z_off of nz_glob
 int make_job3d_slab(orf_ctx* ctx, const orf_sim3d* sim, int z_off, int nz_glob, orf_job** out);
 int batch2d_run(orf_ctx* ctx, int n, const orf_sim2d* sims, orf_out2d* outs, orf_progress_fn progress,
                 void* user);
-int validate2d(const orf_sim2d* s);
+// scan_eps = false skips the per-cell permittivity scan (for callers that
+// ran it already: a job's create() after make_job*, batch or serve checks)
+int validate2d(const orf_sim2d* s, bool scan_eps = true);
 // slab: the z position of a z-normal source is checked by the caller
 // against the global grid
-int validate3d(const orf_sim3d* s, bool slab = false);
+int validate3d(const orf_sim3d* s, bool slab = false, bool scan_eps = true);
 orf_ctx* default_ctx(int* status);
 }  // namespace orf
