@@ -52,6 +52,29 @@ def test_host_validation_rejects_bad_sims(bad, frag):
     assert frag in _lib.last_error()
 
 
+def test_permittivity_scan_reports_the_first_bad_cell_of_long_arrays():
+    """Arrays of millions of values are scanned by several host threads in
+    blocks: the message names the first bad cell in column-major order, even
+    when later blocks (scanned by other threads) fail too."""
+    lib = _lib.load()
+    nx, nz = 2000, 1100
+    for bad_at, vals in (((1_650_000, 700_001, 2_100_000), (np.nan, -2.0, np.inf)),
+                         ((4095, 4096), (0.0, np.nan)),
+                         ((nx * nz - 1,), (np.inf,))):
+        eps = np.ones((nx, nz), order="F")
+        flat = eps.reshape(-1, order="F")   # a view: column-major cell order
+        for q, v in zip(bad_at, vals):
+            flat[q] = v
+        s = dict(x=np.arange(nx) * 0.02, z=np.arange(nz) * 0.02, eps=eps, npml=[5, 5],
+                 source=dict(ix=10, profile=np.ones(nz), neff=1, lambda0=1.5), lambdas=[1.5], monitors=[8])
+        m = _abi.marshal_sim2d(s)
+        o, _ = _abi.alloc_out2d(m)
+        st = lib.orf_fdtd2d_run(C.byref(m.struct), C.byref(o), _abi.PROGRESS_FN(0), None)
+        assert st == 1
+        first = min(bad_at)
+        assert f"sim.eps({first + 1})" in _lib.last_error(), _lib.last_error()
+
+
 def test_marshal_rejects_wrong_shapes():
     with pytest.raises(_abi.OrfError) as e:
         _abi.marshal_sim2d(_sim(eps=np.ones((39, 20))))
