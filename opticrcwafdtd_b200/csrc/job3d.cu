@@ -184,16 +184,19 @@ int Job3D<R>::create(const orf_sim3d* s) {
     // ---- material indices (exact table of distinct eps values)
     // component by component, row by row (index_values: several host
     // threads for large grids, the indices of one sequential scan)
+    // (uninitialised scratch: index_values writes the nx cells of every
+    // row, the narrowing below the padding columns, both on several host
+    // threads for large grids)
     const double* eps[3] = {s->eps_x, s->eps_y, s->eps_z};
-    std::vector<uint32_t> ix[3];
+    std::unique_ptr<uint32_t[]> ix[3];
     std::vector<IndexRow> irows;
     irows.reserve((size_t)3 * n[1] * n[2]);
     for (int c = 0; c < 3; ++c) {
-        ix[c].assign(NP(), 0);
+        ix[c].reset(new uint32_t[NP()]);
         for (int k = 0; k < n[2]; ++k)
             for (int j = 0; j < n[1]; ++j)
                 irows.push_back({eps[c] + (size_t)n[0] * ((size_t)j + (size_t)n[1] * k),
-                                 ix[c].data() + ((size_t)k * n[1] + j) * pitch, n[0]});
+                                 ix[c].get() + ((size_t)k * n[1] + j) * pitch, n[0]});
     }
     std::vector<double> lvals;
     index_values(irows, lvals);
@@ -397,17 +400,33 @@ int Job3D<R>::create(const orf_sim3d* s) {
         ctx->stats.h2d_bytes += (int64_t)bytes;
         return ORF_OK;
     };
+    // the device index of a component: idxw-byte table indices in rows of
+    // `pitch`, zero in the padding columns (the TMA boxes read them)
+    std::unique_ptr<unsigned char[]> ib(new unsigned char[NP() * idxw]);
     for (int c = 0; c < 3; ++c) {
-        if (idxw == 4) {
-            ORF_TRY(up(d_ix[c], ix[c].data(), NP() * 4));
-        } else if (idxw == 2) {
-            std::vector<uint16_t> t(ix[c].begin(), ix[c].end());
-            ORF_TRY(up(d_ix[c], t.data(), NP() * 2));
-        } else {
-            std::vector<uint8_t> t(ix[c].begin(), ix[c].end());
-            ORF_TRY(up(d_ix[c], t.data(), NP()));
-        }
-        std::vector<uint32_t>().swap(ix[c]);
+        const uint32_t* v = ix[c].get();
+        unsigned char* dst = ib.get();
+        const int w = n[0], iw = idxw;
+        parallel_rows_n(n[1] * n[2], (size_t)pitch, [&](int r0, int r1) {
+            for (int r = r0; r < r1; ++r) {
+                const size_t o = (size_t)r * pitch;
+                if (iw == 4) {
+                    uint32_t* d = reinterpret_cast<uint32_t*>(dst) + o;
+                    for (int i = 0; i < w; ++i) d[i] = v[o + i];
+                    for (int i = w; i < pitch; ++i) d[i] = 0;
+                } else if (iw == 2) {
+                    uint16_t* d = reinterpret_cast<uint16_t*>(dst) + o;
+                    for (int i = 0; i < w; ++i) d[i] = (uint16_t)v[o + i];
+                    for (int i = w; i < pitch; ++i) d[i] = 0;
+                } else {
+                    unsigned char* d = dst + o;
+                    for (int i = 0; i < w; ++i) d[i] = (unsigned char)v[o + i];
+                    for (int i = w; i < pitch; ++i) d[i] = 0;
+                }
+            }
+        });
+        ix[c].reset();
+        ORF_TRY(up(d_ix[c], ib.get(), NP() * idxw));
     }
     ORF_TRY(up(d_lutc, hlutc.data(), nlut * sizeof(R)));
     ORF_TRY(up(d_lute, lvals.data(), nlut * sizeof(double)));
