@@ -486,14 +486,16 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
                             B[j] = fma(-cb, dx, B[j]);
                         }
                     }
+                    // (an interior tile has no row masks, and its loaded rows
+                    // may run past the grid's last row: the source profile is
+                    // read for grid rows only)
                     if (hs && i == six - 1) {   // TF/SF: the B column left of the plane is scattered field
                         const R ge = (R)sg[0][s];
     #pragma unroll
                         for (int j = 0; j < KS; ++j) {
-                            if ((mB >> j) & 1u) {
-                                const int kk = d.periodic ? pmod(kb + j, nz) : kb + j;
-                                if (ORF_IN(kk, nz)) B[j] = fma(__ldg(I->srcB + kk), ge, B[j]);
-                            }
+                            const int kk = d.periodic ? pmod(kb + j, nz) : kb + j;
+                            if (((mB >> j) & 1u) && kk >= 0 && kk < nz && ORF_IN(kk, nz))
+                                B[j] = fma(__ldg(I->srcB + kk), ge, B[j]);
                         }
                     }
                     // ----- E half step: P (branch-free stencil loop)
@@ -536,10 +538,9 @@ k_step2d_fast(const FastTile2D* __restrict__ tiles, int ntiles, int launch_off, 
                         const R gh = (R)sg[1][s];
     #pragma unroll
                         for (int j = 0; j < KS; ++j) {
-                            if ((mP >> j) & 1u) {
-                                const int kk = d.periodic ? pmod(kb + j, nz) : kb + j;
-                                if (ORF_IN(kk, nz)) P[j] = fma(__ldg(I->srcP + kk), gh, P[j]);
-                            }
+                            const int kk = d.periodic ? pmod(kb + j, nz) : kb + j;
+                            if (((mP >> j) & 1u) && kk >= 0 && kk < nz && ORF_IN(kk, nz))
+                                P[j] = fma(__ldg(I->srcP + kk), gh, P[j]);
                         }
                     }
                     if (d.flags & 6) {      // DFT monitor samples of this step

@@ -2,8 +2,9 @@
 for a device-side memory checker: its 2D step kernels test every global
 access against the extent of its buffer and every stored cell against the
 grid, count what fails and skip it.  Small runs over TE/TM, periodic z, FP32
-and FP64, fused depths 3-10 with both interior variants, a 16-bit material
-index and an uneven batch go through it (in a process of their own, which
+and FP64, fused depths 3-10 with both interior variants, a source column in
+an interior tile whose rows run past the grid, a 16-bit material index and an
+uneven batch go through it (in a process of their own, which
 loads that library); the test requires no violation and the oracle's
 fields (1e-10 FP64, 1e-4 FP32)."""
 import json
@@ -29,7 +30,7 @@ def test_checked_build_counts_no_out_of_bounds_access():
     res = json.loads(r.stdout.strip().splitlines()[-1])
     assert res["violations"] == 0, res
     assert res["worst_fp64"] <= 1e-10 and res["worst_fp32"] <= 1e-4, res
-    assert res["batch_finite"] and res["runs"] >= 34
+    assert res["batch_finite"] and res["runs"] >= 36
 
 
 def test_normal_build_has_no_check_counter():
