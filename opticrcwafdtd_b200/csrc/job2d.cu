@@ -346,7 +346,7 @@ int Job2D<R>::create(const orf_sim2d* s) {
     ar.add(&d_samples, (size_t)kChunk * sstride + 1);
     size_t acc_elems = 0;
     for (auto& q : sd) acc_elems += (size_t)q.len * nL;
-    ar.add(&d_acc, acc_elems * 16 + 16);
+    ar.add_bytes(&d_acc, acc_elems * 16 + 16);
     ar.add(&d_omega, nL);
     ar.add(&d_flux, (size_t)(nM + nMZ) * nL + 1);
     ar.add(&d_stage, (size_t)std::max(nx, nz) * nL);
@@ -616,9 +616,16 @@ int Job2D<R>::reset() {
 
 template <class R>
 void Job2D<R>::state_regions(int b, std::vector<std::pair<void*, size_t>>& out) {
-    const size_t f = sizeof(R) * pitch * nz;
+    const size_t fb = sizeof(R) * pitch * nz;
     const size_t px = sizeof(R) * ((size_t)nz * 2 * h.npx + 1), pz = sizeof(R) * ((size_t)2 * h.npz * nx + 1);
-    out = {{h.P[b], f}, {h.A[b], f}, {h.B[b], f}, {h.psiB[b], px}, {h.psiPx[b], px}, {h.psiA[b], pz}, {h.psiPz[b], pz}};
+    out.clear();
+    out.push_back({h.P[b], fb});
+    out.push_back({h.A[b], fb});
+    out.push_back({h.B[b], fb});
+    out.push_back({h.psiB[b], px});
+    out.push_back({h.psiPx[b], px});
+    out.push_back({h.psiA[b], pz});
+    out.push_back({h.psiPz[b], pz});
     size_t acc_elems = 0;
     for (auto& q : host_streams) acc_elems += (size_t)q.len * nL;
     out.push_back({d_acc, acc_elems * 16});

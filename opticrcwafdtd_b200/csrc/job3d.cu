@@ -368,7 +368,7 @@ int Job3D<R>::create(const orf_sim3d* s) {
         acc_elems += (size_t)q.len * nL;
         stage_elems = std::max(stage_elems, (size_t)q.len * nL);
     }
-    ar.add(&d_acc, acc_elems * 16 + 16);
+    ar.add_bytes(&d_acc, acc_elems * 16 + 16);
     ar.add(&d_omega, nL);
     ar.add(&d_flux, (size_t)nM * nL + 1);
     ar.add(&d_stage, stage_elems);

@@ -173,6 +173,7 @@ struct Arena {
     void add(T** p, size_t n) {
         req.push_back({reinterpret_cast<void**>(p), n * sizeof(T)});
     }
+    void add_bytes(void** p, size_t bytes) { req.push_back({p, bytes}); }   // an untyped block
     size_t bytes() const {
         size_t s = 0;
         for (auto& r : req) s += (r.second + 255) & ~size_t(255);
