@@ -158,3 +158,24 @@ def test_host_validation_rejects_bad_3d_sims(change, frag):
     st = lib.orf_fdtd3d_run(C.byref(m.struct), C.byref(o), _abi.PROGRESS_FN(0), None)
     assert st == 1, _lib.last_error()
     assert frag in _lib.last_error()
+
+
+def test_3d_permittivity_scan_reports_the_first_bad_cell():
+    """The 3D scan (three components of over a million cells each, threaded
+    in blocks) names the component and the first bad cell of it."""
+    lib = _lib.load()
+    s = _sim3d()
+    n = (110, 100, 96)
+    d = 0.04
+    s.update(x=np.arange(n[0]) * d, y=np.arange(n[1]) * d, z=np.arange(n[2]) * d)
+    s["eps"] = {c: np.ones(n, order="F") for c in "xyz"}
+    s["source"] = dict(s["source"], Ea=1.0, Eb=0.0, Ha=0.0, Hb=1.0, index=20)
+    s["monitors"] = [dict(axis=3, index=30)]
+    flat = s["eps"]["y"].reshape(-1, order="F")
+    flat[900_001] = np.nan
+    flat[300_000] = -1.0
+    m = _abi.marshal_sim3d(s)
+    o, _ = _abi.alloc_out3d(m)
+    st = lib.orf_fdtd3d_run(C.byref(m.struct), C.byref(o), _abi.PROGRESS_FN(0), None)
+    assert st == 1
+    assert "sim.eps.y(300001)" in _lib.last_error(), _lib.last_error()
