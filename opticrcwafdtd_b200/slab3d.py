@@ -415,6 +415,55 @@ def fdtd3D_slabs(sim, nslabs: int, device: int = 0, return_jobs: bool = False):
     return out
 
 
+def sim_signature(sim) -> str:
+    """A digest of everything a slab run's ranks must agree on: the grid,
+    its permittivity, the source, monitors, wavelengths and step count."""
+    import hashlib
+
+    g = _abi._get
+    h = hashlib.sha256()
+
+    def put(v):
+        a = np.ascontiguousarray(np.asarray(v, dtype=np.float64))
+        h.update(str(a.shape).encode())
+        h.update(a.tobytes())
+
+    for k in ("x", "y", "z", "lambdas"):
+        put(g(sim, k))
+    eps = g(sim, "eps")
+    for c in "xyz":
+        put(g(eps, c))
+    src = g(sim, "source")
+    for k in ("axis", "index", "Ea", "Eb", "Ha", "Hb", "neff", "lambda0", "bw"):
+        v = g(src, k)
+        put(0.0 if v is None else np.real(v))
+    mons = g(sim, "monitors", [])
+    if isinstance(mons, dict):
+        mons = [mons]
+    put([[int(g(m, "axis")), int(g(m, "index"))] for m in mons] or [[0, 0]])
+    put(np.atleast_1d(np.asarray(g(sim, "npml", [0, 0, 0]), dtype=np.float64)))
+    put(np.atleast_1d(np.asarray(g(sim, "periodic", [False] * 3), dtype=np.float64)))
+    put([_n_steps(sim), float(g(sim, "courant", 0.99 / math.sqrt(3.0))),
+         1.0 if str(g(sim, "precision", "double")).lower() == "single" else 0.0])
+    return h.hexdigest()
+
+
+def check_same_sim(sim, group=None) -> None:
+    """Every rank of the group must hold the same sim before the slabs are
+    cut: one all_gather_object of a digest, on the host, before any device
+    work (a mismatch would swap planes of different runs)."""
+    import torch.distributed as dist
+
+    sig = sim_signature(sim)
+    sigs = [None] * dist.get_world_size(group)
+    dist.all_gather_object(sigs, sig, group=group)
+    bad = [r for r, v in enumerate(sigs) if v != sigs[0]]
+    if bad:
+        raise _abi.OrfError("orf:invalidInput",
+                            f"the ranks hold different sims (ranks {bad} differ from rank 0): every rank of a z-slab "
+                            "run must pass the same sim")
+
+
 def fdtd3D_distributed(sim, group=None, device: int | None = None, return_job: bool = False):
     """out = fdtd3D_distributed(sim): fdtd3D(sim) on the ranks of a
     torch.distributed group (NCCL), rank r running z slab r on its GPU.
@@ -425,6 +474,7 @@ def fdtd3D_distributed(sim, group=None, device: int | None = None, return_job: b
 
     _check_shutoff(sim)
     tr = DistTransport(group)
+    check_same_sim(sim, group)
     nz = np.asarray(_abi._get(sim, "z")).size
     slabs = split_z(nz, tr.world, _npml_z(sim))
     s = slabs[tr.rank]

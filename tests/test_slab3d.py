@@ -1,6 +1,6 @@
 """Host side of the z-slab split of one 3D run (opticrcwafdtd_b200.slab3d):
-slab planes, the slabs' sims, the put-together out struct, and the halo swap
-between ranks, on CPU (three gloo ranks)."""
+slab planes, the slabs' sims, the put-together out struct, the halo swap
+between ranks and the ranks' sim check, on CPU (gloo ranks)."""
 import os
 
 import numpy as np
@@ -214,3 +214,58 @@ def test_dist_transport_swaps_ghost_planes_between_ranks():
             else:                        # the rank below's last own plane
                 assert val == 100.0 * r + f
     assert set(res[1]) == {("recv_above", f) for f in slab3d.SEND_DOWN} | {("recv_below", f) for f in slab3d.SEND_UP}
+
+
+def _same_sim_worker(rank, world, port, q):
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        res = {}
+        sim = _sim()
+        slab3d.check_same_sim(sim)           # identical sims: no error
+        res["same"] = "ok"
+        other = _sim()
+        if rank == 1:
+            other["eps"]["x"][3, 2, 17] += 1e-12   # one cell differs on one rank
+        try:
+            slab3d.fdtd3D_distributed(other)      # refused on the host, before any device work
+            res["diff"] = "ran"
+        except OrfError as e:
+            res["diff"] = "refused" if "different sims" in str(e) else f"other: {e}"
+        q.put((rank, res))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.timeout(120)
+def test_ranks_with_different_sims_are_refused_before_device_work():
+    import multiprocessing as mp
+    import socket
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    ps = [ctx.Process(target=_same_sim_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    res = dict(q.get(timeout=100) for _ in ps)
+    for p in ps:
+        p.join(timeout=30)
+        assert p.exitcode == 0
+    assert res[0] == res[1] == {"same": "ok", "diff": "refused"}
+
+
+def test_sim_signature_sees_every_input():
+    base = slab3d.sim_signature(_sim())
+    assert slab3d.sim_signature(_sim()) == base
+    for change in (lambda s: s["eps"]["z"].__setitem__((0, 0, 0), 2.0),
+                   lambda s: s["source"].update(index=13),
+                   lambda s: s.update(lambdas=[0.5, 0.61]),
+                   lambda s: s.update(maxTime=2.0),
+                   lambda s: s["monitors"].append(dict(axis=3, index=7)),
+                   lambda s: s.update(precision="single")):
+        s = _sim()
+        change(s)
+        assert slab3d.sim_signature(s) != base
